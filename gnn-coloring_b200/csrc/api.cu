@@ -1,0 +1,501 @@
+// Native C ABI (include/gnn_coloring.h): contexts, device-resident graphs and models, and the
+// hot-path entry points.  Every call returns a status; nothing falls back to the CPU.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+#include "gc_internal.h"
+#include "host_graph.h"
+
+gc_status gc_sort_order_bits(gc_graph *g, int key_bits);
+
+// ---- errors ------------------------------------------------------------------------------------
+
+gc_status gc_fail(gc_ctx *ctx, gc_status s, const std::string &msg) {
+    if (ctx) ctx->last_error = msg;
+    return s;
+}
+
+gc_status gc_check_cuda(gc_ctx *ctx, cudaError_t e, const char *what) {
+    if (e == cudaSuccess) return GC_OK;
+    std::string m = std::string(what) + ": " + cudaGetErrorString(e);
+    if (e == cudaErrorMemoryAllocation) return gc_fail(ctx, GC_ERR_NOMEM, m);
+    return gc_fail(ctx, GC_ERR_CUDA, m);
+}
+
+gc_status gc_check_launch(gc_ctx *ctx, const char *what) { return gc_check_cuda(ctx, cudaGetLastError(), what); }
+
+gc_status gc_reset_state(gc_ctx *ctx) {
+    return gc_check_cuda(ctx, cudaMemsetAsync(ctx->dstate, 0, sizeof(gc::DevState), ctx->stream), "reset device state");
+}
+
+gc_status gc_read_state(gc_ctx *ctx) {
+    gc_status s = gc_check_cuda(
+        ctx, cudaMemcpyAsync(ctx->hstate, ctx->dstate, sizeof(gc::DevState), cudaMemcpyDeviceToHost, ctx->stream),
+        "read device state");
+    if (s != GC_OK) return s;
+    if ((s = gc_check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "kernel execution")) != GC_OK) return s;
+    unsigned int err = ctx->hstate->err;
+    if (err) {
+        char buf[160];
+        snprintf(buf, sizeof buf, "device error 0x%x at index %u (%s)", err, ctx->hstate->err_info,
+                 (err & gc::ERR_WAIT_EXPIRED) ? "wait for a predecessor color expired"
+                 : (err & gc::ERR_BOUND)      ? "bound exceeded"
+                                              : "ordering invariant");
+        return gc_fail(ctx, GC_ERR_DEVICE, buf);
+    }
+    return GC_OK;
+}
+
+namespace {
+
+struct DeviceGuard {
+    explicit DeviceGuard(const gc_ctx *ctx) {
+        if (ctx) cudaSetDevice(ctx->device);
+    }
+};
+
+__global__ void k_check_csr(const uint32_t *__restrict__ V, const uint32_t *__restrict__ E, uint32_t N, uint32_t M,
+                            gc::DevState *st) {
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < N; u += stride) {
+        uint32_t a = V[u], b = V[u + 1];
+        if (b < a || b > M) gc::raise_error(st, gc::ERR_BOUND, u);
+    }
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < M; i += stride)
+        if (E[i] >= N) gc::raise_error(st, gc::ERR_BOUND, i);
+}
+
+void free_graph_buffers(gc_graph *g) {
+    if (g->owns_csr) {
+        cudaFree(g->V);
+        cudaFree(g->E);
+    }
+    void *bufs[] = {g->key,     g->color,    g->P,       g->pc,      g->order,    g->sort_buf, g->sort_hist,
+                    g->big,     g->hubs,     g->x,       g->y,       g->t01,      g->deg_rem,  g->frontier,
+                    g->frontier2, g->removed};
+    for (void *p : bufs)
+        if (p) cudaFree(p);
+}
+
+gc_status alloc_graph(gc_ctx *ctx, gc_graph *g, uint32_t N, uint32_t M, bool csr) {
+    gc_status s;
+    g->cap_N = N;
+    g->cap_M = M;
+    if (csr) {
+        if ((s = gc_alloc(ctx, &g->V, (size_t)N + 1, "graph V")) != GC_OK) return s;
+        if ((s = gc_alloc(ctx, &g->E, (size_t)M, "graph E")) != GC_OK) return s;
+    }
+    if ((s = gc_alloc(ctx, &g->key, (size_t)N, "keys")) != GC_OK) return s;
+    if ((s = gc_alloc(ctx, &g->color, (size_t)N, "colors")) != GC_OK) return s;
+    return GC_OK;
+}
+
+gc_status check_host_csr(gc_ctx *ctx, uint32_t N, const uint32_t *V, const uint32_t *E) {
+    if (!V) return gc_fail(ctx, GC_ERR_INVALID, "V is NULL");
+    if (V[0] != 0) return gc_fail(ctx, GC_ERR_INVALID, "V[0] must be 0");
+    if (V[N] > 0 && !E) return gc_fail(ctx, GC_ERR_INVALID, "E is NULL");
+    return GC_OK;
+}
+
+gc_status finish_upload(gc_graph *g) {
+    gc_ctx *ctx = g->ctx;
+    gc_status s;
+    g->has_keys = g->has_colors = false;
+    g->key_kind = -1;
+    if (g->N == 0) return gc_graph_prepare(g);
+    if ((s = gc_reset_state(ctx)) != GC_OK) return s;
+    k_check_csr<<<ctx->num_sms * 4, 256, 0, ctx->stream>>>(g->V, g->E, g->N, g->M, ctx->dstate);
+    ctx->launches++;
+    if ((s = gc_check_launch(ctx, "csr check")) != GC_OK) return s;
+    if ((s = gc_read_state(ctx)) != GC_OK)
+        return s == GC_ERR_DEVICE ? gc_fail(ctx, GC_ERR_INVALID, "malformed CSR: V not monotone or E out of range") : s;
+    return gc_graph_prepare(g);
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *gc_status_string(gc_status s) {
+    switch (s) {
+        case GC_OK: return "ok";
+        case GC_ERR_INVALID: return "invalid argument";
+        case GC_ERR_NOMEM: return "out of memory";
+        case GC_ERR_CUDA: return "CUDA error";
+        case GC_ERR_DEVICE: return "device-side error";
+        case GC_ERR_IO: return "I/O error";
+        case GC_ERR_FORMAT: return "format error";
+        case GC_ERR_BUDGET: return "HBM budget exceeded";
+        case GC_ERR_NODEV: return "no CUDA device";
+        case GC_ERR_STATE: return "call out of order";
+    }
+    return "unknown status";
+}
+
+gc_status gc_ctx_create(int device, gc_ctx **out) {
+    if (!out) return GC_ERR_INVALID;
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        return GC_ERR_NODEV;
+    }
+    if (device < 0 || device >= n) return GC_ERR_INVALID;
+    gc_ctx *ctx = new gc_ctx();
+    ctx->device = device;
+    gc_status s = gc_check_cuda(ctx, cudaSetDevice(device), "set device");
+    if (s == GC_OK) s = gc_check_cuda(ctx, cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device), "sm count");
+    if (s == GC_OK) s = gc_check_cuda(ctx, cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking), "stream");
+    if (s == GC_OK) s = gc_check_cuda(ctx, cudaMalloc((void **)&ctx->dstate, sizeof(gc::DevState)), "device state");
+    if (s == GC_OK) s = gc_check_cuda(ctx, cudaMallocHost((void **)&ctx->hstate, sizeof(gc::DevState)), "host state");
+    if (s == GC_OK) s = gc_reset_state(ctx);
+    if (const char *lim = getenv("GC_SPIN_LIMIT")) ctx->spin_limit = (unsigned int)strtoul(lim, nullptr, 10);
+    if (s != GC_OK) {
+        gc_ctx_destroy(ctx);
+        return s;
+    }
+    *out = ctx;
+    return GC_OK;
+}
+
+void gc_ctx_destroy(gc_ctx *ctx) {
+    if (!ctx) return;
+    DeviceGuard dg(ctx);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    if (ctx->side_stream) {
+        cudaStreamSynchronize(ctx->side_stream);
+        cudaStreamDestroy(ctx->side_stream);
+    }
+    if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
+    if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
+    if (ctx->dstate) cudaFree(ctx->dstate);
+    if (ctx->hstate) cudaFreeHost(ctx->hstate);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+const char *gc_last_error(const gc_ctx *ctx) { return ctx ? ctx->last_error.c_str() : "no context"; }
+void *gc_ctx_stream(gc_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
+uint64_t gc_ctx_launches(const gc_ctx *ctx) { return ctx ? ctx->launches : 0; }
+
+gc_status gc_sync(gc_ctx *ctx) {
+    if (!ctx) return GC_ERR_INVALID;
+    DeviceGuard dg(ctx);
+    return gc_check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "synchronize");
+}
+
+// ---- graphs ---------------------------------------------------------------------------------
+
+gc_status gc_graph_upload(gc_ctx *ctx, uint32_t N, const uint32_t *V, const uint32_t *E, gc_graph **out) {
+    if (!ctx || !out) return GC_ERR_INVALID;
+    DeviceGuard dg(ctx);
+    *out = nullptr;
+    gc_status s = check_host_csr(ctx, N, V, E);
+    if (s != GC_OK) return s;
+    gc_graph *g = new gc_graph();
+    g->ctx = ctx;
+    if ((s = alloc_graph(ctx, g, N, V[N], true)) != GC_OK) {
+        gc_graph_free(g);
+        return s;
+    }
+    if ((s = gc_graph_reupload(ctx, g, N, V, E)) != GC_OK) {
+        gc_graph_free(g);
+        return s;
+    }
+    *out = g;
+    return GC_OK;
+}
+
+gc_status gc_graph_create(gc_ctx *ctx, uint32_t cap_N, uint32_t cap_M, gc_graph **out) {
+    if (!ctx || !out) return GC_ERR_INVALID;
+    DeviceGuard dg(ctx);
+    *out = nullptr;
+    gc_graph *g = new gc_graph();
+    g->ctx = ctx;
+    gc_status s = alloc_graph(ctx, g, cap_N, cap_M, true);
+    if (s != GC_OK) {
+        gc_graph_free(g);
+        return s;
+    }
+    *out = g;
+    return GC_OK;
+}
+
+gc_status gc_graph_reupload(gc_ctx *ctx, gc_graph *g, uint32_t N, const uint32_t *V, const uint32_t *E) {
+    if (!ctx || !g || !g->owns_csr) return GC_ERR_INVALID;
+    DeviceGuard dg(ctx);
+    gc_status s = check_host_csr(ctx, N, V, E);
+    if (s != GC_OK) return s;
+    const uint32_t M = V[N];
+    if (N > g->cap_N || M > g->cap_M) return gc_fail(ctx, GC_ERR_INVALID, "graph exceeds the allocated capacity");
+    g->N = N;
+    g->M = M;
+    if ((s = gc_check_cuda(ctx, cudaMemcpyAsync(g->V, V, sizeof(uint32_t) * ((size_t)N + 1), cudaMemcpyHostToDevice,
+                                                ctx->stream), "upload V")) != GC_OK)
+        return s;
+    if (M && (s = gc_check_cuda(ctx, cudaMemcpyAsync(g->E, E, sizeof(uint32_t) * (size_t)M, cudaMemcpyHostToDevice,
+                                                     ctx->stream), "upload E")) != GC_OK)
+        return s;
+    return finish_upload(g);
+}
+
+gc_status gc_graph_wrap_device(gc_ctx *ctx, uint32_t N, uint32_t M, const uint32_t *dV, const uint32_t *dE,
+                               gc_graph **out) {
+    if (!ctx || !out || !dV || (M && !dE)) return GC_ERR_INVALID;
+    DeviceGuard dg(ctx);
+    *out = nullptr;
+    gc_graph *g = new gc_graph();
+    g->ctx = ctx;
+    g->owns_csr = false;
+    g->V = const_cast<uint32_t *>(dV);
+    g->E = const_cast<uint32_t *>(dE);
+    gc_status s = alloc_graph(ctx, g, N, M, false);
+    if (s == GC_OK) {
+        g->N = N;
+        g->M = M;
+        s = finish_upload(g);
+    }
+    if (s != GC_OK) {
+        gc_graph_free(g);
+        return s;
+    }
+    *out = g;
+    return GC_OK;
+}
+
+void gc_graph_free(gc_graph *g) {
+    if (!g) return;
+    DeviceGuard dg(g->ctx);
+    if (g->ctx) cudaStreamSynchronize(g->ctx->stream);
+    free_graph_buffers(g);
+    delete g;
+}
+
+uint32_t gc_graph_num_vertices(const gc_graph *g) { return g ? g->N : 0; }
+uint32_t gc_graph_num_edges(const gc_graph *g) { return g ? g->M : 0; }
+uint32_t gc_graph_max_degree(const gc_graph *g) { return g ? g->max_deg : 0; }
+const uint32_t *gc_graph_device_keys(const gc_graph *g) { return g ? g->key : nullptr; }
+const int32_t *gc_graph_device_colors(const gc_graph *g) { return g ? g->color : nullptr; }
+
+// ---- models ---------------------------------------------------------------------------------
+
+gc_status gc_model_create(gc_ctx *ctx, int params, int md, const float *param, gc_model **out) {
+    if (!ctx || !out || !param) return GC_ERR_INVALID;
+    DeviceGuard dg(ctx);
+    *out = nullptr;
+    if (params / gc::LAYER_PARAMS < 2)
+        return gc_fail(ctx, GC_ERR_INVALID, "a GraphSAGE-16 model needs at least 2 layers (1056 parameters)");
+    gc_model *m = new gc_model();
+    m->ctx = ctx;
+    m->params = params;
+    m->md = md;
+    m->layers = params / gc::LAYER_PARAMS;
+    m->h_param = (float *)malloc(sizeof(float) * params);
+    if (!m->h_param) {
+        delete m;
+        return gc_fail(ctx, GC_ERR_NOMEM, "model host copy");
+    }
+    memcpy(m->h_param, param, sizeof(float) * params);
+    gc_status s = gc_alloc(ctx, &m->d_param, (size_t)params, "model parameters");
+    if (s == GC_OK)
+        s = gc_check_cuda(ctx, cudaMemcpyAsync(m->d_param, param, sizeof(float) * params, cudaMemcpyHostToDevice, ctx->stream),
+                          "upload model");
+    if (s == GC_OK) s = gc_check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "upload model");
+    if (s != GC_OK) {
+        gc_model_free(m);
+        return s;
+    }
+    *out = m;
+    return GC_OK;
+}
+
+gc_status gc_model_load(gc_ctx *ctx, const char *path, gc_model **out) {
+    if (!ctx || !path || !out) return GC_ERR_INVALID;
+    int params = 0, md = 0;
+    float *param = nullptr;
+    gc_status s = gc_model_read(path, &params, &md, &param);
+    if (s != GC_OK) return gc_fail(ctx, s, std::string("cannot read model file ") + path);
+    s = gc_model_create(ctx, params, md, param, out);
+    free(param);
+    return s;
+}
+
+void gc_model_free(gc_model *m) {
+    if (!m) return;
+    DeviceGuard dg(m->ctx);
+    if (m->d_param) cudaFree(m->d_param);
+    free(m->h_param);
+    delete m;
+}
+
+int gc_model_layers(const gc_model *m) { return m ? m->layers : 0; }
+
+// ---- hot path -------------------------------------------------------------------------------
+
+gc_status gc_priority(gc_ctx *ctx, gc_graph *g, gc_heuristic h, const gc_model *model) {
+    if (!ctx || !g || g->ctx != ctx) return GC_ERR_INVALID;
+    DeviceGuard dg(ctx);
+    gc_status s;
+    switch (h) {
+        case GC_FF:
+        case GC_LF:
+        case GC_LLF: s = gc_priority_simple(g, h); break;
+        case GC_SL: s = gc_priority_peel(g, false); break;
+        case GC_SLL: s = gc_priority_peel(g, true); break;
+        case GC_GNN:
+            if (!model) return gc_fail(ctx, GC_ERR_INVALID, "GNN priorities need a model");
+            s = gc_priority_gnn(g, model);
+            break;
+        default: return gc_fail(ctx, GC_ERR_INVALID, "unknown heuristic");
+    }
+    if (s != GC_OK) return s;
+    g->key_kind = (int)h;
+    g->has_keys = true;
+    g->has_colors = false;
+    return GC_OK;
+}
+
+gc_status gc_priority_set(gc_ctx *ctx, gc_graph *g, const double *p) {
+    if (!ctx || !g || (g->N && !p)) return GC_ERR_INVALID;
+    DeviceGuard dg(ctx);
+    const uint32_t N = g->N;
+    std::vector<uint32_t> k(N);
+    // Exact order-preserving keys: integers in [0, 2^32) map to themselves; otherwise values are
+    // ranked (equal values share a rank).  -0.0 == +0.0 as in the reference's comparisons.
+    bool integral = true;
+    for (uint32_t u = 0; u < N; u++) {
+        double v = p[u];
+        if (std::isnan(v)) return gc_fail(ctx, GC_ERR_INVALID, "NaN priority");
+        if (!(v >= 0.0 && v <= 4294967295.0 && v == std::floor(v))) integral = false;
+    }
+    if (integral) {
+        for (uint32_t u = 0; u < N; u++) k[u] = (uint32_t)p[u];
+    } else {
+        std::vector<double> vals(p, p + N);
+        for (double &v : vals)
+            if (v == 0.0) v = 0.0;
+        std::sort(vals.begin(), vals.end());
+        vals.erase(std::unique(vals.begin(), vals.end()), vals.end());
+        for (uint32_t u = 0; u < N; u++) {
+            double v = p[u] == 0.0 ? 0.0 : p[u];
+            k[u] = (uint32_t)(std::lower_bound(vals.begin(), vals.end(), v) - vals.begin());
+        }
+    }
+    gc_status s;
+    if (N) {
+        if ((s = gc_check_cuda(ctx, cudaMemcpyAsync(g->key, k.data(), sizeof(uint32_t) * N, cudaMemcpyHostToDevice,
+                                                    ctx->stream), "upload priorities")) != GC_OK)
+            return s;
+        if ((s = gc_check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "upload priorities")) != GC_OK) return s;
+    }
+    g->user_p.assign(p, p + N);
+    g->key_kind = 200;
+    g->has_keys = true;
+    g->has_colors = false;
+    return GC_OK;
+}
+
+gc_status gc_color(gc_ctx *ctx, gc_graph *g, int recolor, int *colors_used) {
+    if (!ctx || !g || g->ctx != ctx || recolor < 0) return GC_ERR_INVALID;
+    if (!g->has_keys) return gc_fail(ctx, GC_ERR_STATE, "no priorities: call gc_priority or gc_priority_set first");
+    DeviceGuard dg(ctx);
+    gc_status s;
+    if ((s = gc_reset_state(ctx)) != GC_OK) return s;
+    if ((s = gc_jp_color(g)) != GC_OK) return s;
+    for (int it = 0; it < recolor; it++) {
+        if ((s = gc_keys_from_colors(g)) != GC_OK) return s;
+        if ((s = gc_jp_color(g)) != GC_OK) return s;
+    }
+    if ((s = gc_read_state(ctx)) != GC_OK) return s;
+    if (colors_used) {
+        int C = 0;
+        if ((s = gc_validate_device(g, &C)) != GC_OK) return s;
+        *colors_used = C;
+        g->colors_used = C;
+    }
+    return GC_OK;
+}
+
+gc_status gc_recolor(gc_ctx *ctx, gc_graph *g, int iters, int *colors_used) {
+    if (!ctx || !g || g->ctx != ctx || iters < 0) return GC_ERR_INVALID;
+    if (!g->has_colors) return gc_fail(ctx, GC_ERR_STATE, "no coloring to recolor");
+    DeviceGuard dg(ctx);
+    gc_status s;
+    if ((s = gc_reset_state(ctx)) != GC_OK) return s;
+    for (int it = 0; it < iters; it++) {
+        if ((s = gc_keys_from_colors(g)) != GC_OK) return s;
+        g->has_keys = true;
+        if ((s = gc_jp_color(g)) != GC_OK) return s;
+    }
+    if ((s = gc_read_state(ctx)) != GC_OK) return s;
+    if (colors_used) {
+        int C = 0;
+        if ((s = gc_validate_device(g, &C)) != GC_OK) return s;
+        *colors_used = C;
+        g->colors_used = C;
+    }
+    return GC_OK;
+}
+
+gc_status gc_validate(gc_ctx *ctx, gc_graph *g, int *max_color) {
+    if (!ctx || !g || !max_color) return GC_ERR_INVALID;
+    if (!g->has_colors) return gc_fail(ctx, GC_ERR_STATE, "no coloring to validate");
+    DeviceGuard dg(ctx);
+    return gc_validate_device(g, max_color);
+}
+
+gc_status gc_upload_colors(gc_ctx *ctx, gc_graph *g, const int32_t *color) {
+    if (!ctx || !g || (g->N && !color)) return GC_ERR_INVALID;
+    DeviceGuard dg(ctx);
+    gc_status s;
+    if (g->N && (s = gc_check_cuda(ctx, cudaMemcpyAsync(g->color, color, sizeof(int32_t) * g->N, cudaMemcpyHostToDevice,
+                                                        ctx->stream), "upload colors")) != GC_OK)
+        return s;
+    if ((s = gc_check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "upload colors")) != GC_OK) return s;
+    g->has_colors = true;
+    return GC_OK;
+}
+
+gc_status gc_download_colors(gc_ctx *ctx, gc_graph *g, int32_t *color) {
+    if (!ctx || !g || (g->N && !color)) return GC_ERR_INVALID;
+    if (!g->has_colors) return gc_fail(ctx, GC_ERR_STATE, "no coloring computed");
+    DeviceGuard dg(ctx);
+    gc_status s;
+    if (g->N && (s = gc_check_cuda(ctx, cudaMemcpyAsync(color, g->color, sizeof(int32_t) * g->N, cudaMemcpyDeviceToHost,
+                                                        ctx->stream), "download colors")) != GC_OK)
+        return s;
+    return gc_check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "download colors");
+}
+
+gc_status gc_download_priority(gc_ctx *ctx, gc_graph *g, double *p) {
+    if (!ctx || !g || (g->N && !p)) return GC_ERR_INVALID;
+    if (!g->has_keys) return gc_fail(ctx, GC_ERR_STATE, "no priorities computed");
+    DeviceGuard dg(ctx);
+    const uint32_t N = g->N;
+    if (g->key_kind == 200) {
+        memcpy(p, g->user_p.data(), sizeof(double) * N);
+        return GC_OK;
+    }
+    std::vector<uint32_t> k(N);
+    gc_status s;
+    if (N && (s = gc_check_cuda(ctx, cudaMemcpyAsync(k.data(), g->key, sizeof(uint32_t) * N, cudaMemcpyDeviceToHost,
+                                                     ctx->stream), "download priorities")) != GC_OK)
+        return s;
+    if ((s = gc_check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "download priorities")) != GC_OK) return s;
+    if (g->key_kind == GC_GNN) {
+        for (uint32_t u = 0; u < N; u++) {
+            float f;
+            memcpy(&f, &k[u], sizeof f);
+            p[u] = (double)f;
+        }
+    } else {
+        for (uint32_t u = 0; u < N; u++) p[u] = (double)k[u];
+    }
+    return GC_OK;
+}
+
+}  // extern "C"

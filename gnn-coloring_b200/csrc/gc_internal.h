@@ -1,0 +1,99 @@
+// Internal objects of the device library: contexts, device-resident graphs and models, and the
+// host-side drivers of each kernel family.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "gc_device.cuh"
+#include "gnn_coloring.h"
+
+struct gc_ctx {
+    int device = 0;
+    int num_sms = 0;
+    cudaStream_t stream = nullptr;
+    cudaStream_t side_stream = nullptr;  // GNN hub CTAs run here, overlapping the bulk of a layer
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    int color_blocks_per_sm = 0;         // resident CTAs of the coloring kernel (occupancy query)
+    gc::DevState *dstate = nullptr;      // device status block
+    gc::DevState *hstate = nullptr;      // pinned host mirror for read-back
+    uint64_t launches = 0;
+    std::string last_error;
+    unsigned int spin_limit = 1u << 22;  // iterations a kernel waits on a predecessor before giving up
+};
+
+// Vertices with more neighbours than this are handled by a whole CTA in the GNN layers.
+constexpr uint32_t GC_GNN_HUB_DEGREE = 1024;
+// Vertices with more neighbours than this are split across several warps in the JP split pass.
+constexpr uint32_t GC_SPLIT_BIG_DEGREE = 32;
+constexpr uint32_t GC_SPLIT_CHUNK = 2048;
+
+struct gc_graph {
+    gc_ctx *ctx = nullptr;
+    uint32_t N = 0, M = 0;          // current graph
+    uint32_t cap_N = 0, cap_M = 0;  // allocated capacity
+    uint32_t max_deg = 0;
+    bool owns_csr = true;
+    uint32_t *V = nullptr, *E = nullptr;
+    // priorities and colors
+    uint32_t *key = nullptr;   // uint32 priority keys (float bits for GNN)
+    int32_t *color = nullptr;  // 1-based colors
+    int key_kind = -1;         // gc_heuristic that produced the keys, 100 = colors (Culberson), 200 = user
+    bool has_keys = false, has_colors = false;
+    // JP workspace
+    uint32_t *P = nullptr;      // predecessor lists, packed at the front of each CSR segment
+    uint32_t *pc = nullptr;     // predecessor counts
+    uint32_t *order = nullptr;  // vertices by descending key, ascending id on ties: the ticket order
+    uint32_t *sort_buf = nullptr;  // radix sort ping-pong (keys and values), 4 * cap_N words
+    uint32_t *sort_hist = nullptr;
+    uint32_t sort_hist_cap = 0;
+    // degree classes (depend on the graph only; rebuilt on upload)
+    uint32_t *big = nullptr;         // split tasks: (vertex, first edge) pairs for deg > GC_SPLIT_BIG_DEGREE
+    uint32_t n_big_tasks = 0;
+    uint32_t *hubs = nullptr;        // vertices with deg > GC_GNN_HUB_DEGREE
+    uint32_t n_hubs = 0;
+    // GNN scratch (allocated on first use)
+    float *x = nullptr, *y = nullptr;
+    float2 *t01 = nullptr;
+    // SL/SLL scratch (allocated on first use)
+    uint32_t *deg_rem = nullptr, *frontier = nullptr, *frontier2 = nullptr, *removed = nullptr;
+    // stats of the last coloring
+    int colors_used = 0;
+    std::vector<double> user_p;  // priorities given by gc_priority_set, returned unchanged
+};
+
+struct gc_model {
+    gc_ctx *ctx = nullptr;
+    int params = 0, md = 0, layers = 0;
+    float *d_param = nullptr;  // device copy
+    float *h_param = nullptr;  // host copy
+};
+
+// ---- helpers (api.cu) ----
+gc_status gc_fail(gc_ctx *ctx, gc_status s, const std::string &msg);
+gc_status gc_check_cuda(gc_ctx *ctx, cudaError_t e, const char *what);
+gc_status gc_check_launch(gc_ctx *ctx, const char *what);
+gc_status gc_read_state(gc_ctx *ctx);  // syncs, copies DevState, reports device errors
+gc_status gc_reset_state(gc_ctx *ctx);
+template <typename T>
+gc_status gc_alloc(gc_ctx *ctx, T **p, size_t count, const char *what) {
+    if (*p) return GC_OK;
+    cudaError_t e = cudaMalloc((void **)p, sizeof(T) * (count ? count : 1));
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        return gc_check_cuda(ctx, e, what);
+    }
+    return GC_OK;
+}
+
+// ---- kernel drivers ----
+gc_status gc_graph_prepare(gc_graph *g);  // degree classes, max degree (k_graph.cu)
+gc_status gc_priority_simple(gc_graph *g, gc_heuristic h);         // FF / LF / LLF (k_priority.cu)
+gc_status gc_priority_peel(gc_graph *g, bool log_thresholds);      // SL / SLL (k_priority.cu)
+gc_status gc_priority_gnn(gc_graph *g, const gc_model *m);         // GraphSAGE (k_gnn.cu)
+gc_status gc_jp_color(gc_graph *g);                                // JP by current keys (k_jp.cu)
+gc_status gc_keys_from_colors(gc_graph *g);                        // Culberson step (k_jp.cu)
+gc_status gc_validate_device(gc_graph *g, int *max_color);         // (k_jp.cu)
+gc_status gc_sort_order(gc_graph *g);                              // ticket order (k_sort.cu)

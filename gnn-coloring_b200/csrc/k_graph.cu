@@ -1,0 +1,101 @@
+// Per-graph preparation on the device: maximum degree and the degree classes that the
+// split and GNN kernels schedule separately.  Depends only on the CSR, so it runs once per
+// upload (the reference likewise prepares its CSR before any timed call, src/main.c:106-133).
+#include <algorithm>
+#include <vector>
+
+#include "gc_internal.h"
+
+namespace {
+
+__global__ void k_degree_classes(const uint32_t *__restrict__ V, uint32_t N, uint32_t big_deg,
+                                 uint32_t chunk, uint32_t hub_deg, gc::DevState *st,
+                                 uint32_t *__restrict__ tasks, uint32_t task_cap,
+                                 uint32_t *__restrict__ hubs, uint32_t hub_cap) {
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < N; base += stride) {
+        uint32_t u = base + threadIdx.x;
+        uint32_t beg = 0, d = 0;
+        if (u < N) {
+            beg = V[u];
+            d = V[u + 1] - beg;
+        }
+        uint32_t wmax = __reduce_max_sync(0xffffffffu, d);
+        if ((threadIdx.x & 31) == 0 && wmax) atomicMax(&st->max_color, wmax);
+        if (u >= N) continue;
+        if (d > big_deg) {
+            uint32_t nt = (d + chunk - 1) / chunk;
+            uint32_t at = atomicAdd(&st->count, nt);
+            if (tasks)
+                for (uint32_t k = 0; k < nt; k++)
+                    if (at + k < task_cap) {
+                        tasks[2 * (at + k)] = u;
+                        tasks[2 * (at + k) + 1] = beg + k * chunk;
+                    }
+        }
+        if (d > hub_deg) {
+            uint32_t at = atomicAdd(&st->count2, 1u);
+            if (hubs && at < hub_cap) hubs[at] = u;
+        }
+    }
+}
+
+}  // namespace
+
+gc_status gc_graph_prepare(gc_graph *g) {
+    gc_ctx *ctx = g->ctx;
+    gc_status s;
+    if (g->N == 0) {
+        g->max_deg = 0;
+        g->n_big_tasks = 0;
+        g->n_hubs = 0;
+        return GC_OK;
+    }
+    int grid = ctx->num_sms * 8;
+    // pass 1: counts
+    if ((s = gc_reset_state(ctx)) != GC_OK) return s;
+    k_degree_classes<<<grid, 256, 0, ctx->stream>>>(g->V, g->N, GC_SPLIT_BIG_DEGREE, GC_SPLIT_CHUNK,
+                                                    GC_GNN_HUB_DEGREE, ctx->dstate, nullptr, 0, nullptr, 0);
+    ctx->launches++;
+    if ((s = gc_check_launch(ctx, "degree classes")) != GC_OK) return s;
+    if ((s = gc_read_state(ctx)) != GC_OK) return s;
+    g->max_deg = ctx->hstate->max_color;
+    uint32_t n_tasks = ctx->hstate->count, n_hubs = ctx->hstate->count2;
+    // (re)allocate lists
+    if (g->big) cudaFree(g->big);
+    if (g->hubs) cudaFree(g->hubs);
+    g->big = nullptr;
+    g->hubs = nullptr;
+    if ((s = gc_alloc(ctx, &g->big, 2 * (size_t)n_tasks, "split task list")) != GC_OK) return s;
+    if ((s = gc_alloc(ctx, &g->hubs, (size_t)n_hubs, "hub list")) != GC_OK) return s;
+    // pass 2: fill
+    if ((s = gc_reset_state(ctx)) != GC_OK) return s;
+    k_degree_classes<<<grid, 256, 0, ctx->stream>>>(g->V, g->N, GC_SPLIT_BIG_DEGREE, GC_SPLIT_CHUNK,
+                                                    GC_GNN_HUB_DEGREE, ctx->dstate, g->big, n_tasks,
+                                                    g->hubs, n_hubs);
+    ctx->launches++;
+    if ((s = gc_check_launch(ctx, "degree classes")) != GC_OK) return s;
+    if ((s = gc_read_state(ctx)) != GC_OK) return s;
+    g->n_big_tasks = n_tasks;
+    g->n_hubs = n_hubs;
+    // hubs by descending degree, so the longest FP32 add chains start first
+    if (n_hubs > 1) {
+        std::vector<uint32_t> h(n_hubs), Vh((size_t)g->N + 1);
+        if ((s = gc_check_cuda(ctx, cudaMemcpyAsync(h.data(), g->hubs, 4 * (size_t)n_hubs,
+                                                    cudaMemcpyDeviceToHost, ctx->stream), "hub list")) != GC_OK)
+            return s;
+        if ((s = gc_check_cuda(ctx, cudaMemcpyAsync(Vh.data(), g->V, 4 * ((size_t)g->N + 1),
+                                                    cudaMemcpyDeviceToHost, ctx->stream), "V")) != GC_OK)
+            return s;
+        if ((s = gc_check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "hub list")) != GC_OK) return s;
+        std::sort(h.begin(), h.end(), [&](uint32_t a, uint32_t b) {
+            uint32_t da = Vh[a + 1] - Vh[a], db = Vh[b + 1] - Vh[b];
+            return da != db ? da > db : a < b;
+        });
+        if ((s = gc_check_cuda(ctx, cudaMemcpyAsync(g->hubs, h.data(), 4 * (size_t)n_hubs,
+                                                    cudaMemcpyHostToDevice, ctx->stream), "hub list")) != GC_OK)
+            return s;
+        if ((s = gc_check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "hub list")) != GC_OK) return s;
+    }
+    return GC_OK;
+}

@@ -1,0 +1,176 @@
+// Ticket order for the coloring kernel: all vertices by descending key, ties by ascending id,
+// i.e. a topological order of the reference's priority DAG (src/coloring.c:72 and :249: v
+// precedes u when p[v] > p[u], or p[v] == p[u] and v < u).  Any topological order would do; this
+// is the one every heuristic shares.
+//
+// LSD radix sort with 8-bit digits over the complemented key (ascending ~key = descending key).
+// The input sequence lists vertices by ascending id and every pass is stable, so equal keys end
+// up by ascending id.  Passes over digits that no key can have set are skipped: the caller
+// passes the key's bit width (known per heuristic: degree bound, color bound, 32 for floats).
+//
+// Per pass: tile histograms -> one exclusive scan in digit-major order -> stable scatter.
+// Stability inside a tile: each warp walks its own contiguous run of the tile in order, ranking
+// equal digits with __match_any_sync; per-digit warp totals are then prefixed across warps.
+#include "gc_internal.h"
+
+namespace {
+using namespace gc;
+
+constexpr int SORT_WARPS = 8;
+constexpr int SORT_THREADS = SORT_WARPS * 32;
+constexpr int SORT_ITEMS = 32;                               // per lane
+constexpr int SORT_TILE = SORT_THREADS * SORT_ITEMS;          // 8192 elements per CTA
+constexpr int RADIX = 256;
+
+__device__ __forceinline__ uint32_t load_key(const uint32_t *kin, const uint32_t *key, uint32_t n, uint32_t j, bool first) {
+    return first ? key[j] : kin[j];
+}
+__device__ __forceinline__ uint32_t digit_of(uint32_t k, int shift) { return ((~k) >> shift) & (RADIX - 1); }
+
+__global__ void __launch_bounds__(SORT_THREADS) k_sort_hist(const uint32_t *__restrict__ kin, const uint32_t *__restrict__ key,
+                                                            uint32_t n, int shift, int first,
+                                                            uint32_t *__restrict__ counts, uint32_t ntiles) {
+    __shared__ uint32_t hist[RADIX];
+    for (int i = threadIdx.x; i < RADIX; i += SORT_THREADS) hist[i] = 0;
+    __syncthreads();
+    const uint32_t tile = blockIdx.x;
+    const uint32_t base = tile * SORT_TILE;
+    const int lane = threadIdx.x & 31;
+    for (int s = 0; s < SORT_ITEMS; s++) {
+        uint32_t j = base + s * SORT_THREADS + threadIdx.x;
+        bool valid = j < n;
+        uint32_t d = valid ? digit_of(load_key(kin, key, n, j, first), shift) : 0xffffffffu;
+        unsigned int peers = __match_any_sync(0xffffffffu, d);
+        if (valid && lane == __ffs(peers) - 1) atomicAdd(&hist[d], (uint32_t)__popc(peers));
+    }
+    __syncthreads();
+    for (int d = threadIdx.x; d < RADIX; d += SORT_THREADS) counts[(size_t)d * ntiles + tile] = hist[d];
+}
+
+// Exclusive scan of `total` counters in place by one CTA of 1024 threads.
+__global__ void __launch_bounds__(1024) k_sort_scan(uint32_t *__restrict__ counts, uint32_t total) {
+    __shared__ uint32_t part[1024];
+    const uint32_t per = (total + 1023) / 1024;
+    const uint32_t b = threadIdx.x * per, e = min(total, b + per);
+    uint32_t sum = 0;
+    for (uint32_t i = b; i < e; i++) sum += counts[i];
+    part[threadIdx.x] = sum;
+    __syncthreads();
+    // Hillis-Steele inclusive scan over the 1024 partial sums
+    for (int off = 1; off < 1024; off <<= 1) {
+        uint32_t v = threadIdx.x >= (unsigned)off ? part[threadIdx.x - off] : 0;
+        __syncthreads();
+        part[threadIdx.x] += v;
+        __syncthreads();
+    }
+    uint32_t run = threadIdx.x ? part[threadIdx.x - 1] : 0;
+    for (uint32_t i = b; i < e; i++) {
+        uint32_t c = counts[i];
+        counts[i] = run;
+        run += c;
+    }
+}
+
+__global__ void __launch_bounds__(SORT_THREADS) k_sort_scatter(const uint32_t *__restrict__ kin, const uint32_t *__restrict__ vin,
+                                                               const uint32_t *__restrict__ key, uint32_t n, int shift,
+                                                               int first, const uint32_t *__restrict__ offsets,
+                                                               uint32_t ntiles, uint32_t *__restrict__ kout,
+                                                               uint32_t *__restrict__ vout) {
+    __shared__ uint32_t wcnt[SORT_WARPS][RADIX];
+    __shared__ uint32_t gbase[RADIX];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int d = lane; d < RADIX; d += 32) wcnt[warp][d] = 0;
+    for (int d = threadIdx.x; d < RADIX; d += SORT_THREADS) gbase[d] = offsets[(size_t)d * ntiles + blockIdx.x];
+    __syncwarp();
+    const uint32_t wbase = blockIdx.x * SORT_TILE + warp * (32 * SORT_ITEMS);
+    uint32_t k[SORT_ITEMS], v[SORT_ITEMS], pos[SORT_ITEMS];
+    const unsigned int lt = (1u << lane) - 1u;
+#pragma unroll
+    for (int s = 0; s < SORT_ITEMS; s++) {
+        uint32_t j = wbase + s * 32 + lane;
+        bool valid = j < n;
+        k[s] = valid ? load_key(kin, key, n, j, first) : 0u;
+        v[s] = valid ? (first ? j : vin[j]) : 0u;
+        uint32_t d = valid ? digit_of(k[s], shift) : 0xffffffffu;
+        unsigned int peers = __match_any_sync(0xffffffffu, d);
+        uint32_t before = valid ? wcnt[warp][d] : 0;
+        pos[s] = before + __popc(peers & lt);
+        __syncwarp();
+        if (valid && lane == __ffs(peers) - 1) wcnt[warp][d] = before + __popc(peers);
+        __syncwarp();
+    }
+    __syncthreads();
+    // per digit: exclusive prefix across warps, then add the tile's global offset
+    for (int d = threadIdx.x; d < RADIX; d += SORT_THREADS) {
+        uint32_t run = gbase[d];
+        for (int w = 0; w < SORT_WARPS; w++) {
+            uint32_t c = wcnt[w][d];
+            wcnt[w][d] = run;
+            run += c;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int s = 0; s < SORT_ITEMS; s++) {
+        uint32_t j = wbase + s * 32 + lane;
+        if (j < n) {
+            uint32_t dst = wcnt[warp][digit_of(k[s], shift)] + pos[s];
+            kout[dst] = k[s];
+            vout[dst] = v[s];
+        }
+    }
+}
+
+__global__ void k_iota(uint32_t *__restrict__ out, uint32_t n) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = i;
+}
+
+}  // namespace
+
+// Sorts into g->order.  key_bits: number of low key bits that may be non-zero.
+gc_status gc_sort_order_bits(gc_graph *g, int key_bits) {
+    gc_ctx *ctx = g->ctx;
+    gc_status s;
+    const uint32_t n = g->N;
+    if (n == 0) return GC_OK;
+    if ((s = gc_alloc(ctx, &g->sort_buf, 4 * (size_t)g->cap_N, "sort buffers")) != GC_OK) return s;
+    const uint32_t ntiles = (n + SORT_TILE - 1) / SORT_TILE;
+    if (g->sort_hist_cap < (size_t)RADIX * ntiles) {
+        if (g->sort_hist) cudaFree(g->sort_hist);
+        g->sort_hist = nullptr;
+        if ((s = gc_alloc(ctx, &g->sort_hist, (size_t)RADIX * ntiles, "sort histogram")) != GC_OK) return s;
+        g->sort_hist_cap = RADIX * ntiles;
+    }
+    if (key_bits <= 0) {
+        // every key is 0: ascending id order
+        // (a single stable pass over a constant digit produces exactly that)
+        key_bits = 1;
+    }
+    const int passes = (key_bits + 7) / 8;
+    uint32_t *k0 = g->sort_buf, *v0 = g->sort_buf + g->cap_N;
+    uint32_t *k1 = g->sort_buf + 2 * (size_t)g->cap_N, *v1 = g->sort_buf + 3 * (size_t)g->cap_N;
+    const uint32_t *kin = nullptr, *vin = nullptr;
+    for (int p = 0; p < passes; p++) {
+        const int shift = 8 * p;
+        const int first = (p == 0);
+        uint32_t *kout = (p & 1) ? k1 : k0, *vout = (p & 1) ? v1 : v0;
+        if (p == passes - 1) vout = g->order;  // last pass writes the ticket order directly
+        k_sort_hist<<<ntiles, SORT_THREADS, 0, ctx->stream>>>(kin, g->key, n, shift, first, g->sort_hist, ntiles);
+        k_sort_scan<<<1, 1024, 0, ctx->stream>>>(g->sort_hist, RADIX * ntiles);
+        k_sort_scatter<<<ntiles, SORT_THREADS, 0, ctx->stream>>>(kin, vin, g->key, n, shift, first, g->sort_hist, ntiles,
+                                                                 kout, vout);
+        ctx->launches += 3;
+        if ((s = gc_check_launch(ctx, "radix sort")) != GC_OK) return s;
+        kin = kout;
+        vin = vout;
+    }
+    return GC_OK;
+}
+
+gc_status gc_order_identity(gc_graph *g) {
+    gc_ctx *ctx = g->ctx;
+    if (g->N == 0) return GC_OK;
+    k_iota<<<ctx->num_sms * 4, 256, 0, ctx->stream>>>(g->order, g->N);
+    ctx->launches++;
+    return gc_check_launch(ctx, "identity order");
+}

@@ -1,0 +1,416 @@
+"""ctypes binding of libgnncolor.so (the B200 greedy-coloring library).
+
+Two layers, mirroring include/:
+  * the native device API (include/gnn_coloring.h): Context, Graph, Model, priority(), color();
+  * the reference-named drop-in functions (include/coloring.h, first_fit.h, ... of
+    KennethLangedal/GNN-COLORING), exposed as ``legacy.<name>`` with numpy arrays.
+
+Plus seeded graph generators and .gnn model helpers (host side).
+
+The library is the product; it runs only on the GPU.  Importing this module fails loudly if the
+in-tree shared library is missing; creating a Context fails with GCError(GC_ERR_NODEV) when no
+CUDA device is visible.  Nothing here falls back to the CPU.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional, Tuple
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libgnncolor.so")
+
+if not os.path.exists(LIB_PATH):
+    raise ImportError(f"{LIB_PATH} is missing: build it with `make -C {HERE}` (or __graft_entry__.build())")
+lib = C.CDLL(LIB_PATH)
+
+u32p = C.POINTER(C.c_uint32)
+i32p = C.POINTER(C.c_int32)
+f32p = C.POINTER(C.c_float)
+f64p = C.POINTER(C.c_double)
+vp = C.c_void_p
+
+STATUS = {
+    0: "GC_OK", 1: "GC_ERR_INVALID", 2: "GC_ERR_NOMEM", 3: "GC_ERR_CUDA", 4: "GC_ERR_DEVICE",
+    5: "GC_ERR_IO", 6: "GC_ERR_FORMAT", 7: "GC_ERR_BUDGET", 8: "GC_ERR_NODEV", 9: "GC_ERR_STATE",
+}
+GC_FF, GC_LF, GC_LLF, GC_SL, GC_SLL, GC_GNN = range(6)
+HEURISTICS = {"FF": GC_FF, "LF": GC_LF, "LLF": GC_LLF, "SL": GC_SL, "SLL": GC_SLL, "GNN": GC_GNN}
+
+
+class GCError(RuntimeError):
+    def __init__(self, status: int, msg: str = ""):
+        self.status = status
+        self.name = STATUS.get(status, str(status))
+        super().__init__(f"{self.name}: {msg}" if msg else self.name)
+
+
+def _sig(name, res, *args):
+    f = getattr(lib, name)
+    f.restype = res
+    f.argtypes = list(args)
+    return f
+
+
+# native API
+_sig("gc_status_string", C.c_char_p, C.c_int)
+_sig("gc_ctx_create", C.c_int, C.c_int, C.POINTER(vp))
+_sig("gc_ctx_destroy", None, vp)
+_sig("gc_last_error", C.c_char_p, vp)
+_sig("gc_ctx_stream", vp, vp)
+_sig("gc_sync", C.c_int, vp)
+_sig("gc_ctx_launches", C.c_uint64, vp)
+_sig("gc_graph_upload", C.c_int, vp, C.c_uint32, u32p, u32p, C.POINTER(vp))
+_sig("gc_graph_create", C.c_int, vp, C.c_uint32, C.c_uint32, C.POINTER(vp))
+_sig("gc_graph_reupload", C.c_int, vp, vp, C.c_uint32, u32p, u32p)
+_sig("gc_graph_wrap_device", C.c_int, vp, C.c_uint32, C.c_uint32, vp, vp, C.POINTER(vp))
+_sig("gc_graph_free", None, vp)
+_sig("gc_graph_num_vertices", C.c_uint32, vp)
+_sig("gc_graph_num_edges", C.c_uint32, vp)
+_sig("gc_graph_max_degree", C.c_uint32, vp)
+_sig("gc_graph_device_keys", vp, vp)
+_sig("gc_graph_device_colors", vp, vp)
+_sig("gc_model_load", C.c_int, vp, C.c_char_p, C.POINTER(vp))
+_sig("gc_model_create", C.c_int, vp, C.c_int, C.c_int, f32p, C.POINTER(vp))
+_sig("gc_model_free", None, vp)
+_sig("gc_model_layers", C.c_int, vp)
+_sig("gc_priority", C.c_int, vp, vp, C.c_int, vp)
+_sig("gc_priority_set", C.c_int, vp, vp, f64p)
+_sig("gc_color", C.c_int, vp, vp, C.c_int, C.POINTER(C.c_int))
+_sig("gc_recolor", C.c_int, vp, vp, C.c_int, C.POINTER(C.c_int))
+_sig("gc_validate", C.c_int, vp, vp, C.POINTER(C.c_int))
+_sig("gc_upload_colors", C.c_int, vp, vp, i32p)
+_sig("gc_download_colors", C.c_int, vp, vp, i32p)
+_sig("gc_download_priority", C.c_int, vp, vp, f64p)
+# host helpers
+_sig("gc_mtx_read", C.c_int, C.c_char_p, u32p, C.POINTER(u32p), C.POINTER(u32p))
+_sig("gc_mtx_write", C.c_int, C.c_char_p, C.c_uint32, u32p, u32p)
+_sig("gc_csr_from_pairs", C.c_int, C.c_uint32, C.c_uint64, u32p, u32p, C.POINTER(u32p), C.POINTER(u32p))
+_sig("gc_model_read", C.c_int, C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(f32p))
+_sig("gc_host_free", None, vp)
+_sig("gc_gen_er", C.c_int, C.c_uint32, C.c_uint64, C.c_uint64, C.POINTER(u32p), C.POINTER(u32p))
+_sig("gc_gen_rmat", C.c_int, C.c_uint32, C.c_double, C.c_double, C.c_double, C.c_double, C.c_uint64,
+     C.POINTER(u32p), C.POINTER(u32p))
+_sig("gc_gen_rgg2d", C.c_int, C.c_uint32, C.c_double, C.c_uint64, C.POINTER(u32p), C.POINTER(u32p))
+_sig("gc_gen_stencil27", C.c_int, C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(u32p), C.POINTER(u32p))
+
+
+def _ptr(a: np.ndarray, t):
+    return a.ctypes.data_as(t)
+
+
+def _check(status: int, ctx_handle=None, what: str = ""):
+    if status != 0:
+        msg = what
+        if ctx_handle:
+            detail = lib.gc_last_error(ctx_handle)
+            if detail:
+                msg = f"{what}: {detail.decode()}" if what else detail.decode()
+        raise GCError(status, msg)
+
+
+# ---- host-side graphs ------------------------------------------------------------------------
+
+def _take_csr(N: int, Vp, Ep) -> Tuple[int, np.ndarray, np.ndarray]:
+    V = np.ctypeslib.as_array(Vp, shape=(N + 1,)).copy()
+    M = int(V[N])
+    E = np.ctypeslib.as_array(Ep, shape=(max(M, 1),))[:M].copy() if M else np.zeros(0, np.uint32)
+    lib.gc_host_free(C.cast(Vp, vp))
+    lib.gc_host_free(C.cast(Ep, vp))
+    return N, V, E
+
+
+def gen_er(n: int, m: int, seed: int):
+    Vp, Ep = u32p(), u32p()
+    _check(lib.gc_gen_er(n, m, seed, C.byref(Vp), C.byref(Ep)), what="gen_er")
+    return _take_csr(n, Vp, Ep)
+
+
+def gen_rmat(n: int, ef: float, seed: int, a: float = 0.57, b: float = 0.19, c: float = 0.19):
+    Vp, Ep = u32p(), u32p()
+    _check(lib.gc_gen_rmat(n, ef, a, b, c, seed, C.byref(Vp), C.byref(Ep)), what="gen_rmat")
+    return _take_csr(n, Vp, Ep)
+
+
+def gen_rgg2d(n: int, radius: float, seed: int):
+    Vp, Ep = u32p(), u32p()
+    _check(lib.gc_gen_rgg2d(n, radius, seed, C.byref(Vp), C.byref(Ep)), what="gen_rgg2d")
+    return _take_csr(n, Vp, Ep)
+
+
+def gen_stencil27(nx: int, ny: int, nz: int):
+    Vp, Ep = u32p(), u32p()
+    _check(lib.gc_gen_stencil27(nx, ny, nz, C.byref(Vp), C.byref(Ep)), what="gen_stencil27")
+    return _take_csr(nx * ny * nz, Vp, Ep)
+
+
+def csr_from_pairs(n: int, I: np.ndarray, J: np.ndarray):
+    I = np.ascontiguousarray(I, dtype=np.uint32)
+    J = np.ascontiguousarray(J, dtype=np.uint32)
+    Vp, Ep = u32p(), u32p()
+    _check(lib.gc_csr_from_pairs(n, len(I), _ptr(I, u32p), _ptr(J, u32p), C.byref(Vp), C.byref(Ep)),
+           what="csr_from_pairs")
+    return _take_csr(n, Vp, Ep)
+
+
+def mtx_read(path: str):
+    N = C.c_uint32()
+    Vp, Ep = u32p(), u32p()
+    _check(lib.gc_mtx_read(path.encode(), C.byref(N), C.byref(Vp), C.byref(Ep)), what=f"mtx_read {path}")
+    return _take_csr(N.value, Vp, Ep)
+
+
+def mtx_write(path: str, N: int, V: np.ndarray, E: np.ndarray):
+    V = np.ascontiguousarray(V, np.uint32)
+    E = np.ascontiguousarray(E, np.uint32)
+    _check(lib.gc_mtx_write(path.encode(), N, _ptr(V, u32p), _ptr(E, u32p)), what="mtx_write")
+
+
+# ---- .gnn models -------------------------------------------------------------------------------
+
+def model_read(path: str) -> Tuple[np.ndarray, int]:
+    params, md, P = C.c_int(), C.c_int(), f32p()
+    _check(lib.gc_model_read(path.encode(), C.byref(params), C.byref(md), C.byref(P)), what=f"model_read {path}")
+    arr = np.ctypeslib.as_array(P, shape=(params.value,)).copy()
+    lib.gc_host_free(C.cast(P, vp))
+    return arr, md.value
+
+
+def synthetic_model(layers: int, seed: int, md: int = 100) -> Tuple[np.ndarray, int]:
+    """Seeded GraphSAGE-16 weights in the .gnn layout: per layer W[32x16] row-major, then b[16].
+
+    Weights ~ N(0, 0.5), biases ~ N(0.1, 0.5), rounded to 10 decimals as .gnn files store them,
+    so that writing and re-reading the file gives the same floats."""
+    rng = np.random.default_rng(seed)
+    P = []
+    for _ in range(layers):
+        P.append(rng.normal(0.0, 0.5, 512))
+        P.append(rng.normal(0.1, 0.5, 16))
+    P = np.round(np.concatenate(P), 10)
+    return P.astype(np.float32), md
+
+
+def model_write(path: str, params: np.ndarray, md: int):
+    """Writes a .gnn file ("params md" then the floats); the float32 values round-trip exactly."""
+    with open(path, "w") as f:
+        f.write(f"{len(params)} {md}\n")
+        f.write(" ".join(f"{float(x):.9g}" for x in params))
+        f.write("\n")
+
+
+# ---- native device API ---------------------------------------------------------------------------
+
+class Context:
+    def __init__(self, device: int = 0):
+        h = vp()
+        st = lib.gc_ctx_create(device, C.byref(h))
+        if st != 0:
+            raise GCError(st, "gc_ctx_create")
+        self.h = h
+
+    def close(self):
+        if self.h:
+            lib.gc_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def check(self, st, what=""):
+        _check(st, self.h, what)
+
+    @property
+    def stream(self) -> int:
+        return lib.gc_ctx_stream(self.h) or 0
+
+    @property
+    def launches(self) -> int:
+        return int(lib.gc_ctx_launches(self.h))
+
+    def sync(self):
+        self.check(lib.gc_sync(self.h), "sync")
+
+
+class Model:
+    def __init__(self, ctx: Context, params: np.ndarray, md: int):
+        self.ctx = ctx
+        params = np.ascontiguousarray(params, np.float32)
+        h = vp()
+        ctx.check(lib.gc_model_create(ctx.h, len(params), md, _ptr(params, f32p), C.byref(h)), "model")
+        self.h = h
+
+    @classmethod
+    def load(cls, ctx: Context, path: str) -> "Model":
+        params, md = model_read(path)
+        return cls(ctx, params, md)
+
+    @property
+    def layers(self) -> int:
+        return lib.gc_model_layers(self.h)
+
+    def close(self):
+        if self.h:
+            lib.gc_model_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Graph:
+    def __init__(self, ctx: Context, N: int, V: np.ndarray, E: np.ndarray):
+        self.ctx = ctx
+        self.V = np.ascontiguousarray(V, np.uint32)
+        self.E = np.ascontiguousarray(E, np.uint32) if len(E) else np.zeros(1, np.uint32)
+        self.N = int(N)
+        h = vp()
+        ctx.check(lib.gc_graph_upload(ctx.h, self.N, _ptr(self.V, u32p), _ptr(self.E, u32p), C.byref(h)), "upload")
+        self.h = h
+
+    @property
+    def M(self) -> int:
+        return int(lib.gc_graph_num_edges(self.h))
+
+    @property
+    def max_degree(self) -> int:
+        return int(lib.gc_graph_max_degree(self.h))
+
+    def priority(self, heuristic, model: Optional[Model] = None):
+        h = HEURISTICS[heuristic] if isinstance(heuristic, str) else int(heuristic)
+        self.ctx.check(lib.gc_priority(self.ctx.h, self.h, h, model.h if model else None), "priority")
+
+    def set_priority(self, p: np.ndarray):
+        p = np.ascontiguousarray(p, np.float64)
+        self.ctx.check(lib.gc_priority_set(self.ctx.h, self.h, _ptr(p, f64p)), "priority_set")
+
+    def color(self, recolor: int = 0, count: bool = True) -> int:
+        c = C.c_int(0)
+        self.ctx.check(lib.gc_color(self.ctx.h, self.h, recolor, C.byref(c) if count else None), "color")
+        return c.value
+
+    def recolor(self, iters: int = 1) -> int:
+        c = C.c_int(0)
+        self.ctx.check(lib.gc_recolor(self.ctx.h, self.h, iters, C.byref(c)), "recolor")
+        return c.value
+
+    def validate(self) -> int:
+        c = C.c_int(0)
+        self.ctx.check(lib.gc_validate(self.ctx.h, self.h, C.byref(c)), "validate")
+        return c.value
+
+    def colors(self) -> np.ndarray:
+        out = np.empty(max(self.N, 1), np.int32)
+        self.ctx.check(lib.gc_download_colors(self.ctx.h, self.h, _ptr(out, i32p)), "download colors")
+        return out[: self.N]
+
+    def set_colors(self, color: np.ndarray):
+        color = np.ascontiguousarray(color, np.int32)
+        self.ctx.check(lib.gc_upload_colors(self.ctx.h, self.h, _ptr(color, i32p)), "upload colors")
+
+    def priorities(self) -> np.ndarray:
+        out = np.empty(max(self.N, 1), np.float64)
+        self.ctx.check(lib.gc_download_priority(self.ctx.h, self.h, _ptr(out, f64p)), "download priority")
+        return out[: self.N]
+
+    @property
+    def device_keys(self) -> int:
+        return lib.gc_graph_device_keys(self.h) or 0
+
+    def close(self):
+        if self.h:
+            lib.gc_graph_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ---- the reference-named drop-in functions ------------------------------------------------------
+
+class _Legacy:
+    """numpy front-end of the reference's own entry points, as exported by libgnncolor.so."""
+
+    def __init__(self):
+        for name in ("first_fit_ordering", "first_fit_ordering_par", "largest_degree_first_ordering",
+                     "largest_log_degree_first_ordering", "smallest_degree_last_ordering",
+                     "smallest_log_degree_last_ordering"):
+            _sig(name, None, C.c_uint32, u32p, u32p, f64p)
+        _sig("gnn_ordering", None, C.c_uint32, u32p, u32p, f64p, C.c_int)
+        for name in ("jones_plassmann_coloring", "greedy_coloring"):
+            _sig(name, i32p, C.c_uint32, u32p, u32p, f64p)
+        for name in ("first_fit_coloring", "first_fit_coloring_par", "largest_degree_first_coloring",
+                     "largest_degree_first_coloring_par", "largest_log_degree_first_coloring",
+                     "largest_log_degree_first_coloring_par", "smallest_degree_last_coloring",
+                     "smallest_degree_last_coloring_par", "smallest_log_degree_last_coloring",
+                     "smallest_log_degree_last_coloring_par"):
+            _sig(name, i32p, C.c_uint32, u32p, u32p)
+        for name in ("validate_coloring", "validate_coloring_par"):
+            _sig(name, C.c_int, C.c_uint32, u32p, u32p, i32p)
+        for name in ("jones_plassmann_setup", "greedy_setup", "gnn_setup", "first_fit_setup"):
+            _sig(name, vp, C.c_uint32, C.c_uint32)
+        for name in ("jones_plassmann_cleanup", "greedy_cleanup", "gnn_cleanup", "first_fit_cleanup"):
+            _sig(name, None, vp)
+        for name in ("jones_plassmann_internal", "greedy_internal"):
+            _sig(name, None, C.c_uint32, u32p, u32p, vp, f64p, i32p)
+        for name in ("gnn_internal_par", "gnn_internal", "first_fit_internal_par"):
+            _sig(name, None, C.c_uint32, u32p, u32p, vp, vp, f64p, i32p)
+        for name in ("cgnn_graph_sage_16", "cgnn_graph_sage_16_par"):
+            _sig(name, None, C.c_int, f32p, C.c_uint32, u32p, u32p, C.c_int, f32p, f32p, f64p)
+        self.libc = C.CDLL(None)
+        self.libc.free.argtypes = [vp]
+
+    @staticmethod
+    def _csr(V, E):
+        V = np.ascontiguousarray(V, np.uint32)
+        E = np.ascontiguousarray(E, np.uint32) if len(E) else np.zeros(1, np.uint32)
+        return V, E
+
+    def ordering(self, name: str, N, V, E, layers: int = 0) -> np.ndarray:
+        V, E = self._csr(V, E)
+        p = np.zeros(N + 8, np.float64)
+        if name == "gnn_ordering":
+            lib.gnn_ordering(N, _ptr(V, u32p), _ptr(E, u32p), _ptr(p, f64p), layers)
+        else:
+            getattr(lib, name)(N, _ptr(V, u32p), _ptr(E, u32p), _ptr(p, f64p))
+        return p[:N]
+
+    def _take(self, ptr, N) -> np.ndarray:
+        out = np.ctypeslib.as_array(ptr, shape=(max(N, 1),))[:N].copy()
+        self.libc.free(C.cast(ptr, vp))
+        return out
+
+    def coloring(self, name: str, N, V, E, p: Optional[np.ndarray] = None) -> np.ndarray:
+        V, E = self._csr(V, E)
+        if p is None:
+            ptr = getattr(lib, name)(N, _ptr(V, u32p), _ptr(E, u32p))
+        else:
+            p = np.ascontiguousarray(p, np.float64)
+            ptr = getattr(lib, name)(N, _ptr(V, u32p), _ptr(E, u32p), _ptr(p, f64p))
+        return self._take(ptr, N)
+
+    def validate(self, N, V, E, color) -> int:
+        V, E = self._csr(V, E)
+        color = np.ascontiguousarray(color, np.int32)
+        return lib.validate_coloring_par(N, _ptr(V, u32p), _ptr(E, u32p), _ptr(color, i32p))
+
+    def graph_sage(self, params: np.ndarray, md: int, N, V, E) -> np.ndarray:
+        V, E = self._csr(V, E)
+        params = np.ascontiguousarray(params, np.float32)
+        p = np.zeros(N + 8, np.float64)
+        lib.cgnn_graph_sage_16_par(len(params), _ptr(params, f32p), N, _ptr(V, u32p), _ptr(E, u32p), md, None,
+                                   None, _ptr(p, f64p))
+        return p[:N]
+
+
+legacy = _Legacy()

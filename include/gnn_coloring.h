@@ -1,0 +1,163 @@
+/*
+ * gnn_coloring.h -- status-returning C ABI of the B200 greedy-coloring library.
+ *
+ * The reference program (KennethLangedal/GNN-COLORING) has no device API; its
+ * operator boundary is a set of host functions (coloring.h, first_fit.h,
+ * largest_degree_first.h, smallest_degree_last.h, gnn.h, fast_gnn.h) that this
+ * library also exports under the reference's own names (see the other headers
+ * in this directory).  Those entry points take host buffers and return void.
+ * This header is the native interface underneath them: a context owns one CUDA
+ * stream on one device, graphs and models live in device memory, every call
+ * returns a gc_status, and nothing ever falls back to the CPU.
+ *
+ * Plain C types only: pointers, sizes and opaque handles.
+ *
+ * Arithmetic contract (what "identical to the reference" means here):
+ *   - priorities are per-vertex keys; vertex v precedes u when
+ *     key[v] > key[u], or key[v] == key[u] and v < u
+ *     (src/coloring.c:249 of the reference);
+ *   - color[u] = smallest c >= 1 not used by any predecessor of u, i.e. the
+ *     Jones-Plassmann / priority-order greedy coloring of src/coloring.c:223-330;
+ *   - the GraphSAGE-16 priorities reproduce src/fast_gnn.c:13-243 bit for bit
+ *     (sequential FP32 neighbour sums in CSR order, IEEE division, FMA chain
+ *     in input order, fixed-tree output sum).
+ */
+#pragma once
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum gc_status {
+    GC_OK = 0,
+    GC_ERR_INVALID = 1,   /* bad argument: null pointer, size out of range, malformed CSR, NaN priority */
+    GC_ERR_NOMEM = 2,     /* host or device allocation failed */
+    GC_ERR_CUDA = 3,      /* a CUDA runtime call failed (message in gc_last_error) */
+    GC_ERR_DEVICE = 4,    /* a kernel raised its error flag (bounded wait expired, internal bound exceeded) */
+    GC_ERR_IO = 5,        /* file missing or unreadable */
+    GC_ERR_FORMAT = 6,    /* malformed Matrix Market or .gnn content */
+    GC_ERR_BUDGET = 7,    /* admission refused: the request does not fit the HBM budget */
+    GC_ERR_NODEV = 8,     /* no usable CUDA device */
+    GC_ERR_STATE = 9      /* call out of order (e.g. coloring before a priority was computed) */
+} gc_status;
+
+/* Priority heuristics, named as in the reference's output lines (src/main.c:199-208). */
+typedef enum gc_heuristic {
+    GC_FF = 0,   /* first fit: p[i] = N - i                       (src/first_fit.c:8-12)              */
+    GC_LF = 1,   /* largest degree first: p = deg                 (src/largest_degree_first.c:12-16)  */
+    GC_LLF = 2,  /* largest log degree first: p = 32 - clz(deg)   (src/largest_degree_first.c:87-97)  */
+    GC_SL = 3,   /* smallest degree last (bucket peeling)          (src/smallest_degree_last.c:62-124) */
+    GC_SLL = 4,  /* smallest log degree last                       (src/smallest_degree_last.c:274-328)*/
+    GC_GNN = 5   /* GraphSAGE-16 inference; needs a model          (src/fast_gnn.c:297-347)            */
+} gc_heuristic;
+
+typedef struct gc_ctx gc_ctx;       /* device + stream + scratch; not shared between host threads */
+typedef struct gc_graph gc_graph;   /* device-resident CSR with its key / color / work buffers    */
+typedef struct gc_model gc_model;   /* device-resident GraphSAGE-16 weights (L * 528 floats)      */
+
+const char *gc_status_string(gc_status s);
+
+/* ---- context ------------------------------------------------------------------------------ */
+
+/* Creates a context on `device` with its own non-blocking stream. */
+gc_status gc_ctx_create(int device, gc_ctx **ctx);
+void gc_ctx_destroy(gc_ctx *ctx);
+/* Last error message of this context ("" when none). */
+const char *gc_last_error(const gc_ctx *ctx);
+/* The cudaStream_t the context launches on (returned as void* to keep CUDA types out of the ABI). */
+void *gc_ctx_stream(gc_ctx *ctx);
+/* Blocks until the context's stream is idle; reports deferred device errors. */
+gc_status gc_sync(gc_ctx *ctx);
+/* Number of kernels this context has launched so far (instrumentation for benchmarks). */
+uint64_t gc_ctx_launches(const gc_ctx *ctx);
+
+/* ---- graphs ------------------------------------------------------------------------------- */
+
+/* Copies a host CSR (V[N+1], E[V[N]]) to the device.  The CSR must be simple and symmetric with
+ * ascending adjacency lists, as produced by the reference's graph_sort_edges + graph_make_simple
+ * (src/fast_io.c:450-477); only V's monotonicity and E's range are checked here. */
+gc_status gc_graph_upload(gc_ctx *ctx, uint32_t N, const uint32_t *V, const uint32_t *E, gc_graph **g);
+/* Allocates an empty graph able to hold up to cap_N vertices and cap_M directed edges; fill it
+ * with gc_graph_reupload.  Lets callers reserve device memory once and reuse it per job. */
+gc_status gc_graph_create(gc_ctx *ctx, uint32_t cap_N, uint32_t cap_M, gc_graph **g);
+/* Same as gc_graph_upload, from pinned or pageable host memory, reusing an existing graph object whose capacity
+ * (N, M) is at least the new graph's: no device allocation happens. */
+gc_status gc_graph_reupload(gc_ctx *ctx, gc_graph *g, uint32_t N, const uint32_t *V, const uint32_t *E);
+/* Wraps a CSR that already lives in device memory (no copy; the caller keeps ownership). */
+gc_status gc_graph_wrap_device(gc_ctx *ctx, uint32_t N, uint32_t M, const uint32_t *dV,
+                               const uint32_t *dE, gc_graph **g);
+void gc_graph_free(gc_graph *g);
+uint32_t gc_graph_num_vertices(const gc_graph *g);
+uint32_t gc_graph_num_edges(const gc_graph *g);
+uint32_t gc_graph_max_degree(const gc_graph *g);
+/* Device pointers of the graph's buffers (for zero-copy readers such as benchmarks). */
+const uint32_t *gc_graph_device_keys(const gc_graph *g);
+const int32_t *gc_graph_device_colors(const gc_graph *g);
+
+/* ---- models ------------------------------------------------------------------------------- */
+
+/* Reads a .gnn model file: "params md" followed by `params` floats (src/gnn.c:33-40). */
+gc_status gc_model_load(gc_ctx *ctx, const char *path, gc_model **m);
+/* Builds a model from host parameters: params = L * 528, L >= 2 (W[32x16] row-major then b[16]
+ * per layer, src/fast_gnn.c:256-258); md is the degree normaliser of the input layer. */
+gc_status gc_model_create(gc_ctx *ctx, int params, int md, const float *param, gc_model **m);
+void gc_model_free(gc_model *m);
+int gc_model_layers(const gc_model *m);
+
+/* ---- the hot path --------------------------------------------------------------------------- */
+
+/* Computes the heuristic's priority keys on the device into the graph's key buffer.
+ * `model` is required for GC_GNN and ignored otherwise. */
+gc_status gc_priority(gc_ctx *ctx, gc_graph *g, gc_heuristic h, const gc_model *model);
+/* Sets arbitrary host priorities (the reference's `double *p`); -0.0 equals +0.0, NaN is rejected. */
+gc_status gc_priority_set(gc_ctx *ctx, gc_graph *g, const double *p);
+/* Jones-Plassmann coloring by the current keys, then `recolor` Culberson iterations
+ * (key := color, recolor), as in src/runner.c:139-152.  `colors_used` (optional) receives the
+ * number of colors of the final coloring.  Colors stay on the device. */
+gc_status gc_color(gc_ctx *ctx, gc_graph *g, int recolor, int *colors_used);
+/* `iters` Culberson iterations on the current coloring: key := color, recolor (the loop body of
+ * src/runner.c:139-152).  The color count never increases. */
+gc_status gc_recolor(gc_ctx *ctx, gc_graph *g, int iters, int *colors_used);
+/* Checks the current coloring on the device: *max_color = number of colors if proper and all
+ * colors positive, 0 otherwise (src/coloring.c:332-352). */
+gc_status gc_validate(gc_ctx *ctx, gc_graph *g, int *max_color);
+/* Sets the graph's coloring from host memory (e.g. to validate an external coloring). */
+gc_status gc_upload_colors(gc_ctx *ctx, gc_graph *g, const int32_t *color);
+/* Copies results to host memory. */
+gc_status gc_download_colors(gc_ctx *ctx, gc_graph *g, int32_t *color);
+/* Priorities as the reference's doubles: FF N-i, LF deg, LLF/SL/SLL delta, GNN the FP32 sum, and
+ * after Culberson the colors. */
+gc_status gc_download_priority(gc_ctx *ctx, gc_graph *g, double *p);
+
+/* ---- host-side graph preparation (no device involved) --------------------------------------- */
+
+/* Reads a Matrix Market file into a simple, symmetric, sorted CSR with the reference's rules:
+ * N = max(rows, cols), every entry added in both directions, adjacency sorted ascending,
+ * self-loops and duplicates dropped (src/fast_io.c:68-222, 450-477).  Arrays are malloc'd. */
+gc_status gc_mtx_read(const char *path, uint32_t *N, uint32_t **V, uint32_t **E);
+/* Builds the same CSR from L 0-based vertex pairs. */
+gc_status gc_csr_from_pairs(uint32_t N, uint64_t L, const uint32_t *I, const uint32_t *J,
+                            uint32_t **V, uint32_t **E);
+/* Writes a CSR as a symmetric pattern Matrix Market file (each undirected edge once, 1-based). */
+gc_status gc_mtx_write(const char *path, uint32_t N, const uint32_t *V, const uint32_t *E);
+/* Reads a .gnn file on the host (malloc'd params). */
+gc_status gc_model_read(const char *path, int *params, int *md, float **param);
+void gc_host_free(void *p);
+
+/* Seeded synthetic graphs (same seed => same graph on every host and thread count). */
+/* Erdos-Renyi G(n, m): the first m distinct non-loop pairs of a splitmix64 stream. */
+gc_status gc_gen_er(uint32_t n, uint64_t m, uint64_t seed, uint32_t **V, uint32_t **E);
+/* R-MAT: ef * n samples over 2^ceil(log2 n) ids with quadrant probabilities a, b, c (d = 1-a-b-c);
+ * samples with an endpoint >= n are dropped; symmetrised, deduplicated, loops removed. */
+gc_status gc_gen_rmat(uint32_t n, double ef, double a, double b, double c, uint64_t seed,
+                      uint32_t **V, uint32_t **E);
+/* 2D random geometric graph: n uniform points in [0,1]^2, edge when distance < radius. */
+gc_status gc_gen_rgg2d(uint32_t n, double radius, uint64_t seed, uint32_t **V, uint32_t **E);
+/* 3D 27-point stencil on an nx * ny * nz grid (all 26 neighbours at Chebyshev distance 1). */
+gc_status gc_gen_stencil27(uint32_t nx, uint32_t ny, uint32_t nz, uint32_t **V, uint32_t **E);
+
+#ifdef __cplusplus
+}
+#endif

@@ -1,0 +1,150 @@
+"""ctypes loader of the reference's own C code (oracle/_ref/libref.so, built by oracle/Makefile
+from the reference's unchanged sources).  Used to pin the oracle, to generate golden vectors and
+as the timed CPU baseline.  Test/bench infrastructure only.
+
+The reference's fast_gnn.c uses aligned AVX loads and streaming stores on x, y and p, so every
+buffer handed to it here is 64-byte aligned and padded by 8 rows, as fast_gnn.h:4-11 asks."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PATH = os.path.join(HERE, "_ref", "libref.so")
+MODELS = os.path.join(HERE, "_ref", "models")
+
+
+def available() -> bool:
+    return os.path.exists(PATH)
+
+
+u32p, i32p, f32p, f64p = (C.POINTER(C.c_uint32), C.POINTER(C.c_int32), C.POINTER(C.c_float),
+                          C.POINTER(C.c_double))
+vp = C.c_void_p
+_lib = None
+_gomp = None
+
+
+def lib():
+    global _lib, _gomp
+    if _lib is None:
+        if not available():
+            raise ImportError(f"{PATH} missing: run `make -C {HERE}` where the reference sources exist")
+        _lib = C.CDLL(PATH)
+        _gomp = C.CDLL("libgomp.so.1")
+        for name in ("first_fit_ordering", "first_fit_ordering_par", "largest_degree_first_ordering",
+                     "largest_log_degree_first_ordering", "largest_log_degree_first_ordering_par",
+                     "smallest_degree_last_ordering", "smallest_log_degree_last_ordering"):
+            getattr(_lib, name).argtypes = [C.c_uint32, u32p, u32p, vp]
+        for name in ("cgnn_graph_sage_16", "cgnn_graph_sage_16_par"):
+            getattr(_lib, name).argtypes = [C.c_int, vp, C.c_uint32, u32p, u32p, C.c_int, vp, vp, vp]
+        for name in ("jones_plassmann_coloring", "greedy_coloring"):
+            getattr(_lib, name).argtypes = [C.c_uint32, u32p, u32p, vp]
+            getattr(_lib, name).restype = i32p
+        for name in ("jones_plassmann_setup", "greedy_setup", "smallest_degree_last_setup"):
+            getattr(_lib, name).argtypes = [C.c_uint32, C.c_uint32]
+            getattr(_lib, name).restype = vp
+        for name in ("jones_plassmann_cleanup", "greedy_cleanup", "smallest_degree_last_cleanup"):
+            getattr(_lib, name).argtypes = [vp]
+        for name in ("jones_plassmann_internal", "greedy_internal"):
+            getattr(_lib, name).argtypes = [C.c_uint32, u32p, u32p, vp, vp, i32p]
+        for name in ("smallest_degree_last_internal_par", "smallest_log_degree_last_internal_par"):
+            getattr(_lib, name).argtypes = [C.c_uint32, u32p, u32p, vp, vp, vp, i32p]
+        _lib.validate_coloring_par.argtypes = [C.c_uint32, u32p, u32p, i32p]
+        _lib.validate_coloring_par.restype = C.c_int
+        _gomp.omp_set_num_threads.argtypes = [C.c_int]
+        _gomp.omp_get_max_threads.restype = C.c_int
+    return _lib
+
+
+def set_threads(n: int):
+    lib()
+    _gomp.omp_set_num_threads(int(n))
+
+
+def max_threads() -> int:
+    lib()
+    return int(_gomp.omp_get_max_threads())
+
+
+def aligned(n: int, dtype) -> np.ndarray:
+    """Zeroed array of n elements whose data starts on a 64-byte boundary."""
+    itemsize = np.dtype(dtype).itemsize
+    raw = np.zeros(n * itemsize + 64, np.uint8)
+    off = (-raw.ctypes.data) % 64
+    return raw[off:off + n * itemsize].view(dtype)
+
+
+def _csr(V, E):
+    V = np.ascontiguousarray(V, np.uint32)
+    E = np.ascontiguousarray(E, np.uint32) if len(E) else np.zeros(1, np.uint32)
+    return V, E, V.ctypes.data_as(u32p), E.ctypes.data_as(u32p)
+
+
+def ordering(name: str, N: int, V, E) -> np.ndarray:
+    L = lib()
+    V, E, Vp, Ep = _csr(V, E)
+    p = aligned(N + 8, np.float64)
+    fn = {"FF": "first_fit_ordering_par", "LF": "largest_degree_first_ordering",
+          "LLF": "largest_log_degree_first_ordering", "SL": "smallest_degree_last_ordering",
+          "SLL": "smallest_log_degree_last_ordering"}[name]
+    getattr(L, fn)(N, Vp, Ep, p.ctypes.data)
+    return p[:N].copy()
+
+
+def peel_par(name: str, N: int, V, E) -> tuple[np.ndarray, np.ndarray]:
+    """The parallel SL/SLL variants (smallest_degree_last.c:155-246, :359-443): p and colors."""
+    L = lib()
+    V, E, Vp, Ep = _csr(V, E)
+    p = aligned(N + 8, np.float64)
+    color = np.zeros(max(N, 1), np.int32)
+    sl = L.smallest_degree_last_setup(N, int(V[N]))
+    jp = L.jones_plassmann_setup(N, int(V[N]))
+    fn = L.smallest_degree_last_internal_par if name == "SL" else L.smallest_log_degree_last_internal_par
+    fn(N, Vp, Ep, sl, jp, p.ctypes.data, color.ctypes.data_as(i32p))
+    L.smallest_degree_last_cleanup(sl)
+    L.jones_plassmann_cleanup(jp)
+    return p[:N].copy(), color[:N].copy()
+
+
+def graph_sage(params: np.ndarray, md: int, N: int, V, E) -> np.ndarray:
+    L = lib()
+    V, E, Vp, Ep = _csr(V, E)
+    P = aligned(len(params), np.float32)
+    P[:] = params
+    x = aligned((N + 8) * 16, np.float32)
+    y = aligned((N + 8) * 16, np.float32)
+    p = aligned(N + 8, np.float64)
+    L.cgnn_graph_sage_16_par(len(params), P.ctypes.data, N, Vp, Ep, md, x.ctypes.data, y.ctypes.data, p.ctypes.data)
+    return p[:N].copy()
+
+
+def jp_color(N: int, V, E, p) -> np.ndarray:
+    L = lib()
+    V, E, Vp, Ep = _csr(V, E)
+    pp = aligned(N + 8, np.float64)
+    pp[:N] = p
+    c = L.jones_plassmann_coloring(N, Vp, Ep, pp.ctypes.data)
+    out = np.ctypeslib.as_array(c, shape=(max(N, 1),))[:N].copy()
+    C.CDLL(None).free(C.cast(c, vp))
+    return out
+
+
+def greedy_color(N: int, V, E, p) -> np.ndarray:
+    L = lib()
+    V, E, Vp, Ep = _csr(V, E)
+    pp = aligned(N + 8, np.float64)
+    pp[:N] = p
+    c = L.greedy_coloring(N, Vp, Ep, pp.ctypes.data)
+    out = np.ctypeslib.as_array(c, shape=(max(N, 1),))[:N].copy()
+    C.CDLL(None).free(C.cast(c, vp))
+    return out
+
+
+def validate(N: int, V, E, color) -> int:
+    L = lib()
+    V, E, Vp, Ep = _csr(V, E)
+    color = np.ascontiguousarray(color, np.int32)
+    return int(L.validate_coloring_par(N, Vp, Ep, color.ctypes.data_as(i32p)))
