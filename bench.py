@@ -1,0 +1,442 @@
+#!/usr/bin/env python
+"""Benchmark: GraphSAGE GNN3 priorities + Jones-Plassmann coloring on one B200 (plain path).
+
+Workload (one "step" = one coloring job): R-MAT scale 22 (4,194,304 vertices), edge factor 16,
+a/b/c/d = 0.57/0.19/0.19/0.05, seed 2, symmetrised, deduplicated, loops removed; GNN3 priorities
+with seeded synthetic GraphSAGE-16 weights (the reference's layout and value range), then JP.
+Metric: colored edges/s = |E| (directed CSR length, the reference's |E|) / job time.
+
+  value   device-resident: CSR on the GPU, CUDA events on the library's stream around K steps
+          of gc_priority(GNN3) + gc_color; E (513 MB) is larger than L2, so no flush is needed.
+  e2e     the reference-facing call with host buffers: gnn_internal_par(N, V, E, ad, jp, p, color)
+          from pinned memory, H2D of V/E and D2H of p/colors inside every timed step.
+  roofline  the dominant kernel's algorithmic bytes per launch / its average event-timed
+          duration, against MEASURED_PEAKS.json's HBM copy bandwidth.
+  cpu_baseline  the reference's own OpenMP code (oracle/_ref) on the host cores, same job.
+
+--impl reference runs the reference's own CPU implementation of the same job (rank 0 only).
+--gpus N > 1 runs N independent replicas, one per GPU (the path does not shard): weak scaling.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "gnn-coloring_b200")
+for p in (ROOT, PKG):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+METRIC = "GNN3+JP colored edges/s"
+UNIT = "edges/s"
+MODEL_SEED = 1003  # synthetic GNN3 weights (same seed as the golden vectors)
+
+
+def workload(name: str):
+    import gnn_coloring as gcn
+    if name == "rmat22":
+        N, V, E = gcn.gen_rmat(1 << 22, 16, 2)
+        desc = "R-MAT scale 22, ef 16, a/b/c=0.57/0.19/0.19, seed 2"
+    elif name == "rmat18":
+        N, V, E = gcn.gen_rmat(1 << 18, 16, 2)
+        desc = "R-MAT scale 18, ef 16, a/b/c=0.57/0.19/0.19, seed 2"
+    elif name == "er65k":
+        N, V, E = gcn.gen_er(65536, 524288, 1)
+        desc = "Erdos-Renyi n=65536, m=524288, seed 1"
+    else:
+        raise SystemExit(f"unknown workload {name}")
+    return desc, N, V, E
+
+
+# Algorithmic (compulsory) HBM bytes per launch of each kernel group, M = directed edges,
+# N = vertices, P = predecessor entries (sum of predecessor counts).
+def algorithmic_bytes(kernel: str, N: int, M: int, P: int) -> float:
+    table = {
+        "gnn_input": 4 * M + 4 * N + 8 * N + 64 * N,     # E, V, own layer-0 inputs, y rows
+        "gnn_hidden": 4 * M + 4 * N + 64 * N + 64 * N,   # E, V, own x row, y row
+        "gnn_output": 4 * M + 4 * N + 64 * N + 4 * N,    # E, V, own x row, key
+        "gnn_table0": 4 * N + 8 * N,
+        "jp_split": 4 * M + 4 * N + 4 * N + 4 * P + 4 * N + 4 * N,  # E, V, key, P written, pc, color reset
+        "jp_color": 4 * N + 4 * N + 4 * N + 4 * P + 4 * N,          # order, V, pc, P read, color written
+        "sort_pass": 4 * N * 4,                                      # keys+ids read and written
+    }
+    return float(table.get(kernel, 0))
+
+
+def step_bytes(N: int, M: int, layers: int = 3) -> float:
+    """Whole-job algorithmic bytes: GNN with L layers 4LM + (132L-124)N, JP 8M + 32N."""
+    return 4 * layers * M + (132 * layers - 124) * N + 8 * M + 32 * N
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons, sampled every 100 ms while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.out = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=self.out, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        self.out.flush()
+        self.out.seek(0)
+        rows = [ln.strip().split(", ") for ln in self.out.read().splitlines() if ln.strip()]
+        self.out.close()
+        os.unlink(self.out.name)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx.append(float(r[2]))
+                for n, v in zip(names, r[5:9]):
+                    if v.strip().lower() == "active":
+                        reasons.add(n)
+            except (ValueError, IndexError):
+                continue
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup(n_gpus: int):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def max_over_ranks(x: float, world: int, device=None) -> float:
+    """The slowest rank's value (timing is reported as the max over ranks)."""
+    if world <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device if device is not None else "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+# ---- the reference's CPU implementation -------------------------------------------------------
+
+def reference_job_runner(N, V, E, params, md):
+    """Sets up the reference's own gnn_setup / jones_plassmann_setup (models/m3.gnn written to a
+    scratch directory, as src/gnn.c:24-25 reads it from the working directory) and returns a
+    callable running its f_par, gnn_internal_par (src/gnn.c:78-83), once."""
+    import gnn_coloring as gcn
+    from oracle import reference as R
+    L = R.lib()
+    L.gnn_setup.argtypes = [C.c_uint32, C.c_uint32]
+    L.gnn_setup.restype = C.c_void_p
+    L.gnn_internal_par.argtypes = [C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    L.gnn_cleanup.argtypes = [C.c_void_p]
+    work = tempfile.mkdtemp(prefix="gnnref_")
+    os.makedirs(os.path.join(work, "models"), exist_ok=True)
+    gcn.model_write(os.path.join(work, "models", "m3.gnn"), params, md)
+    C.c_int.in_dll(L, "layers").value = 3
+    cwd = os.getcwd()
+    os.chdir(work)
+    try:
+        ad = L.gnn_setup(N, int(V[N]))
+    finally:
+        os.chdir(cwd)
+    jp = L.jones_plassmann_setup(N, int(V[N]))
+    Vc = np.ascontiguousarray(V, np.uint32)
+    Ec = np.ascontiguousarray(E, np.uint32)
+    p = R.aligned(N + 8, np.float64)
+    color = np.zeros(N, np.int32)
+
+    def run():
+        L.gnn_internal_par(N, Vc.ctypes.data, Ec.ctypes.data, ad, jp, p.ctypes.data, color.ctypes.data)
+        return color
+
+    return run
+
+
+def run_reference(args):
+    world, rank, local = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
+    if rank != 0:
+        return
+    import gnn_coloring as gcn
+    from oracle import reference as R
+    desc, N, V, E = workload(args.workload)
+    M = int(V[N])
+    params, md = gcn.synthetic_model(3, MODEL_SEED)
+    if not R.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libref.so was not built (reference "
+                                                                "sources absent where build() ran)"}))
+        return
+    cores = os.cpu_count() or 1
+    R.set_threads(cores)
+    run = reference_job_runner(N, V, E, params, md)
+    for _ in range(args.warmup):
+        run()
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        run()
+        times.append(time.perf_counter() - t0)
+    total = sum(times)
+    value = M * len(times) / total
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * total / len(times), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
+        "config": {"workload": f"{args.workload}_gnn3_jp", "graph": desc, "N": N, "M": M,
+                   "heuristic": "GNN3", "threads": cores},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
+                         "sample": f"{args.steps} full GNN3+JP jobs through the reference's gnn_internal_par "
+                                   f"(src/gnn.c:78-83), OpenMP over {cores} threads"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+def cpu_baseline(N, V, E, params, md, budget_s: float = 20.0):
+    from oracle import reference as R
+    cores = os.cpu_count() or 1
+    if R.available():
+        R.set_threads(cores)
+        run = reference_job_runner(N, V, E, params, md)
+        run()  # warm-up
+        times = []
+        t_start = time.perf_counter()
+        while len(times) < 3 and time.perf_counter() - t_start < budget_s:
+            t0 = time.perf_counter()
+            run()
+            times.append(time.perf_counter() - t0)
+        return {"value": int(V[N]) * len(times) / sum(times), "unit": UNIT, "cores": cores, "kind": "reference",
+                "sample": f"{len(times)} full GNN3+JP jobs on the same graph (reference gnn_internal_par, "
+                          f"{cores} OpenMP threads), best-effort within {budget_s:.0f} s"}
+    # port: the scalar restatement on one core, on a smaller graph of the same family
+    import gnn_coloring as gcn
+    from oracle import restatement as O
+    n2, V2, E2 = gcn.gen_rmat(1 << 18, 16, 2)
+    t0 = time.perf_counter()
+    p = O.ordering("GNN", n2, V2, E2, params, md)
+    O.greedy_color(n2, V2, E2, p)
+    dt = time.perf_counter() - t0
+    return {"value": int(V2[n2]) / dt, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": "1 GNN3+JP job on R-MAT scale 18 (same generator) with the scalar oracle"}
+
+
+# ---- our arm -------------------------------------------------------------------------------------
+
+def run_ours(args):
+    import torch
+    import gnn_coloring as gcn
+    world, rank, local = dist_setup(args.gpus)
+    device = local
+    torch.cuda.set_device(device)
+    desc, N, V, E = workload(args.workload)
+    M = int(V[N])
+    params, md = gcn.synthetic_model(3, MODEL_SEED)
+
+    ctx = gcn.Context(device)
+    model = gcn.Model(ctx, params, md)
+    g = gcn.Graph(ctx, N, V, E)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", device))
+
+    def step():
+        g.priority("GNN", model)
+        g.color(count=False)
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    colors_used = g.validate()
+    assert colors_used > 0, "invalid coloring"
+
+    sampler = ClockSampler(device)
+    sampler.start()
+    time.sleep(0.25)
+    barrier(world)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    launches0 = ctx.launches
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    launches = ctx.launches - launches0
+    elapsed_ms = e0.elapsed_time(e1)
+    time.sleep(0.15)
+    clocks = sampler.stop()
+    elapsed_ms = max_over_ranks(elapsed_ms, world, torch.device("cuda", device))
+    ms_per_step = elapsed_ms / args.steps
+    value = world * M * args.steps / (elapsed_ms / 1e3)
+
+    # per-kernel durations: event pairs on each kernel's own stream over a few more steps
+    gcn.lib.gc_prof_enable(ctx.h, 1)
+    prof_steps = max(1, min(args.steps, 5))
+    for _ in range(prof_steps):
+        step()
+    names = (C.c_char_p * 64)()
+    tot = (C.c_double * 64)()
+    cnt = (C.c_uint64 * 64)()
+    gcn.lib.gc_prof_read.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
+    nk = gcn.lib.gc_prof_read(ctx.h, names, tot, cnt, 64)
+    gcn.lib.gc_prof_enable(ctx.h, 0)
+    kernels = {names[i].decode(): {"ms_per_step": tot[i] / prof_steps, "launches_per_step": cnt[i] / prof_steps}
+               for i in range(min(nk, 64))}
+    P = M // 2  # each undirected edge has exactly one predecessor end
+    hbm_peak, peak_kind = peaks()
+    dominant = max(kernels, key=lambda k: kernels[k]["ms_per_step"]) if kernels else None
+    roofline = None
+    if dominant:
+        per_launch_ms = kernels[dominant]["ms_per_step"] / max(kernels[dominant]["launches_per_step"], 1)
+        alg = algorithmic_bytes(dominant, N, M, P)
+        achieved = alg / (per_launch_ms / 1e3) / 1e9
+        traffic = None
+        tpath = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+        if os.path.exists(tpath):
+            try:
+                with open(tpath) as f:
+                    traffic = json.load(f).get(args.workload, {}).get(dominant)
+            except Exception:
+                traffic = None
+        roofline = {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                    "frac": achieved / hbm_peak, "peak_kind": f"{peak_kind} (copy bandwidth)",
+                    "algorithmic_bytes_per_launch": alg, "ms_per_launch": per_launch_ms, "traffic": traffic}
+    job_bytes = step_bytes(N, M)
+    step_roof = {"algorithmic_bytes": job_bytes, "achieved_gbs": job_bytes / (ms_per_step / 1e3) / 1e9,
+                 "frac": job_bytes / (ms_per_step / 1e3) / 1e9 / hbm_peak}
+
+    # e2e through the reference-facing entry point with host buffers
+    e2e = None
+    if not args.no_e2e:
+        e2e = run_e2e(args, N, V, E, params, md, torch)
+
+    result = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": max(3, args.warmup), "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
+        "config": {"workload": f"{args.workload}_gnn3_jp", "graph": desc, "N": N, "M": M, "heuristic": "GNN3",
+                   "model": f"synthetic GraphSAGE-16 weights (3 layers, seed {MODEL_SEED}, md 100)",
+                   "l2": "inputs larger than L2 (E is %.0f MB); no flush" % (4 * M / 1e6),
+                   "parallelism": "replicas" if world > 1 else "single GPU", "colors": colors_used},
+        "gpu_launches": launches, "clocks": clocks, "roofline": roofline, "step_roofline": step_roof,
+        "kernels": kernels, "e2e": e2e,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        result["cpu_baseline"] = cpu_baseline(N, V, E, params, md)
+    if rank == 0:
+        print(json.dumps(result))
+    g.close()
+    model.close()
+    ctx.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def run_e2e(args, N, V, E, params, md, torch):
+    import gnn_coloring as gcn
+    M = int(V[N])
+    work = tempfile.mkdtemp(prefix="gnne2e_")
+    gcn.model_write(os.path.join(work, "m3.gnn"), params, md)
+    os.environ["GC_MODEL_DIR"] = work
+    os.environ["GC_DEVICE"] = str(torch.cuda.current_device())
+    lib = gcn.lib
+    C.c_int.in_dll(lib, "layers").value = 3
+    lib.gnn_setup.argtypes = [C.c_uint32, C.c_uint32]
+    lib.gnn_setup.restype = C.c_void_p
+    lib.jones_plassmann_setup.argtypes = [C.c_uint32, C.c_uint32]
+    lib.jones_plassmann_setup.restype = C.c_void_p
+    lib.gnn_internal_par.argtypes = [C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                     C.c_void_p]
+    lib.gnn_cleanup.argtypes = [C.c_void_p]
+    lib.jones_plassmann_cleanup.argtypes = [C.c_void_p]
+    ad = lib.gnn_setup(N, M)
+    jp = lib.jones_plassmann_setup(N, M)
+    hV = torch.from_numpy(np.ascontiguousarray(V).view(np.int32)).pin_memory()
+    hE = torch.from_numpy(np.ascontiguousarray(E).view(np.int32)).pin_memory()
+    hp = torch.empty(N + 8, dtype=torch.float64).pin_memory()
+    hc = torch.empty(N, dtype=torch.int32).pin_memory()
+
+    def call():
+        lib.gnn_internal_par(N, hV.data_ptr(), hE.data_ptr(), ad, jp, hp.data_ptr(), hc.data_ptr())
+
+    for _ in range(max(3, args.warmup)):
+        call()
+    steps = max(1, args.steps)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        call()
+    dt = time.perf_counter() - t0
+    lib.gnn_cleanup(ad)
+    lib.jones_plassmann_cleanup(jp)
+    return {"value": M * steps / dt, "unit": UNIT, "h2d_bytes_per_step": 4 * (N + 1) + 4 * M,
+            "d2h_bytes_per_step": 8 * N + 4 * N, "ms_per_step": 1e3 * dt / steps,
+            "entry_point": "gnn_internal_par (include/gnn.h) from pinned host memory"}
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", default="rmat22", choices=["rmat22", "rmat18", "er65k"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

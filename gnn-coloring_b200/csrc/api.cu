@@ -10,7 +10,6 @@
 #include "gc_internal.h"
 #include "host_graph.h"
 
-gc_status gc_sort_order_bits(gc_graph *g, int key_bits);
 
 // ---- errors ------------------------------------------------------------------------------------
 
@@ -50,6 +49,31 @@ gc_status gc_read_state(gc_ctx *ctx) {
     return GC_OK;
 }
 
+ProfScope::ProfScope(gc_ctx *c, const char *n, cudaStream_t s) : ctx(c), stream(s), name(n) {
+    if (!ctx->prof) return;
+    if (ctx->prof_pool.empty()) {
+        cudaEvent_t e;
+        if (cudaEventCreate(&e) != cudaSuccess) return;
+        ctx->prof_pool.push_back(e);
+    }
+    a = ctx->prof_pool.back();
+    ctx->prof_pool.pop_back();
+    cudaEventRecord(a, stream);
+}
+
+ProfScope::~ProfScope() {
+    if (!a) return;
+    cudaEvent_t b;
+    if (ctx->prof_pool.empty()) {
+        if (cudaEventCreate(&b) != cudaSuccess) return;
+    } else {
+        b = ctx->prof_pool.back();
+        ctx->prof_pool.pop_back();
+    }
+    cudaEventRecord(b, stream);
+    ctx->prof_recs.push_back({name, a, b});
+}
+
 namespace {
 
 struct DeviceGuard {
@@ -76,7 +100,7 @@ void free_graph_buffers(gc_graph *g) {
     }
     void *bufs[] = {g->key,     g->color,    g->P,       g->pc,      g->order,    g->sort_buf, g->sort_hist,
                     g->big,     g->hubs,     g->x,       g->y,       g->t01,      g->deg_rem,  g->frontier,
-                    g->frontier2, g->removed};
+                    g->frontier2, g->removed, g->leaf_list};
     for (void *p : bufs)
         if (p) cudaFree(p);
 }
@@ -162,20 +186,81 @@ gc_status gc_ctx_create(int device, gc_ctx **out) {
     return GC_OK;
 }
 
+// Graphs and models keep their context alive: destruction order is free.
+static void ctx_release(gc_ctx *ctx);
+
 void gc_ctx_destroy(gc_ctx *ctx) {
-    if (!ctx) return;
+    if (!ctx || ctx->destroy_requested) return;
+    ctx->destroy_requested = true;
+    ctx_release(ctx);
+}
+
+static void ctx_retain(gc_ctx *ctx) { ctx->refs++; }
+
+static void ctx_release(gc_ctx *ctx) {
+    if (--ctx->refs > 0) return;
     DeviceGuard dg(ctx);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     if (ctx->side_stream) {
         cudaStreamSynchronize(ctx->side_stream);
         cudaStreamDestroy(ctx->side_stream);
     }
+    for (auto &r : ctx->prof_recs) {
+        cudaEventDestroy(r.a);
+        cudaEventDestroy(r.b);
+    }
+    for (auto e : ctx->prof_pool) cudaEventDestroy(e);
     if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
     if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
     if (ctx->dstate) cudaFree(ctx->dstate);
     if (ctx->hstate) cudaFreeHost(ctx->hstate);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
+}
+
+gc_status gc_prof_enable(gc_ctx *ctx, int on) {
+    if (!ctx) return GC_ERR_INVALID;
+    DeviceGuard dg(ctx);
+    cudaStreamSynchronize(ctx->stream);
+    for (auto &r : ctx->prof_recs) {
+        ctx->prof_pool.push_back(r.a);
+        ctx->prof_pool.push_back(r.b);
+    }
+    ctx->prof_recs.clear();
+    ctx->prof = on != 0;
+    return GC_OK;
+}
+
+int gc_prof_read(gc_ctx *ctx, const char **names, double *total_ms, uint64_t *launches, int max) {
+    if (!ctx) return 0;
+    DeviceGuard dg(ctx);
+    cudaStreamSynchronize(ctx->stream);
+    if (ctx->side_stream) cudaStreamSynchronize(ctx->side_stream);
+    std::vector<const char *> nm;
+    std::vector<double> ms;
+    std::vector<uint64_t> cnt;
+    for (auto &r : ctx->prof_recs) {
+        float t = 0.0f;
+        if (cudaEventElapsedTime(&t, r.a, r.b) != cudaSuccess) {
+            cudaGetLastError();
+            continue;
+        }
+        size_t i = 0;
+        while (i < nm.size() && strcmp(nm[i], r.name) != 0) i++;
+        if (i == nm.size()) {
+            nm.push_back(r.name);
+            ms.push_back(0.0);
+            cnt.push_back(0);
+        }
+        ms[i] += t;
+        cnt[i]++;
+    }
+    for (size_t i = 0; i < nm.size() && (int)i < max; i++) {
+        if (names) names[i] = nm[i];
+        if (total_ms) total_ms[i] = ms[i];
+        if (launches) launches[i] = cnt[i];
+    }
+    return (int)nm.size();
 }
 
 const char *gc_last_error(const gc_ctx *ctx) { return ctx ? ctx->last_error.c_str() : "no context"; }
@@ -198,6 +283,7 @@ gc_status gc_graph_upload(gc_ctx *ctx, uint32_t N, const uint32_t *V, const uint
     if (s != GC_OK) return s;
     gc_graph *g = new gc_graph();
     g->ctx = ctx;
+    ctx_retain(ctx);
     if ((s = alloc_graph(ctx, g, N, V[N], true)) != GC_OK) {
         gc_graph_free(g);
         return s;
@@ -216,6 +302,7 @@ gc_status gc_graph_create(gc_ctx *ctx, uint32_t cap_N, uint32_t cap_M, gc_graph 
     *out = nullptr;
     gc_graph *g = new gc_graph();
     g->ctx = ctx;
+    ctx_retain(ctx);
     gc_status s = alloc_graph(ctx, g, cap_N, cap_M, true);
     if (s != GC_OK) {
         gc_graph_free(g);
@@ -250,6 +337,7 @@ gc_status gc_graph_wrap_device(gc_ctx *ctx, uint32_t N, uint32_t M, const uint32
     *out = nullptr;
     gc_graph *g = new gc_graph();
     g->ctx = ctx;
+    ctx_retain(ctx);
     g->owns_csr = false;
     g->V = const_cast<uint32_t *>(dV);
     g->E = const_cast<uint32_t *>(dE);
@@ -269,10 +357,14 @@ gc_status gc_graph_wrap_device(gc_ctx *ctx, uint32_t N, uint32_t M, const uint32
 
 void gc_graph_free(gc_graph *g) {
     if (!g) return;
-    DeviceGuard dg(g->ctx);
-    if (g->ctx) cudaStreamSynchronize(g->ctx->stream);
-    free_graph_buffers(g);
+    gc_ctx *ctx = g->ctx;
+    {
+        DeviceGuard dg(ctx);
+        if (ctx) cudaStreamSynchronize(ctx->stream);
+        free_graph_buffers(g);
+    }
     delete g;
+    if (ctx) ctx_release(ctx);
 }
 
 uint32_t gc_graph_num_vertices(const gc_graph *g) { return g ? g->N : 0; }
@@ -291,6 +383,7 @@ gc_status gc_model_create(gc_ctx *ctx, int params, int md, const float *param, g
         return gc_fail(ctx, GC_ERR_INVALID, "a GraphSAGE-16 model needs at least 2 layers (1056 parameters)");
     gc_model *m = new gc_model();
     m->ctx = ctx;
+    ctx_retain(ctx);
     m->params = params;
     m->md = md;
     m->layers = params / gc::LAYER_PARAMS;
@@ -326,10 +419,14 @@ gc_status gc_model_load(gc_ctx *ctx, const char *path, gc_model **out) {
 
 void gc_model_free(gc_model *m) {
     if (!m) return;
-    DeviceGuard dg(m->ctx);
-    if (m->d_param) cudaFree(m->d_param);
+    gc_ctx *ctx = m->ctx;
+    {
+        DeviceGuard dg(ctx);
+        if (m->d_param) cudaFree(m->d_param);
+    }
     free(m->h_param);
     delete m;
+    if (ctx) ctx_release(ctx);
 }
 
 int gc_model_layers(const gc_model *m) { return m ? m->layers : 0; }

@@ -20,7 +20,9 @@ struct DevState {
     unsigned int count;       // generic counter (frontier sizes, compaction)
     unsigned int count2;      // generic counter
     unsigned int min_deg;     // SL peeling: smallest remaining degree
-    unsigned int pad[8];
+    unsigned int ordered;     // coloring: vertices that go through the ordered kernel
+    unsigned int big_leaves;  // coloring: leaves with too many neighbours for one thread
+    unsigned int pad[6];
 };
 
 enum DevErr : unsigned int {

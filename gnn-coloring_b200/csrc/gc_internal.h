@@ -10,6 +10,13 @@
 #include "gc_device.cuh"
 #include "gnn_coloring.h"
 
+// Optional per-kernel timing: when enabled, each kernel launch group records an event pair on
+// the stream it runs on; gc_prof_read aggregates the durations by name.
+struct gc_prof_rec {
+    const char *name;
+    cudaEvent_t a, b;
+};
+
 struct gc_ctx {
     int device = 0;
     int num_sms = 0;
@@ -22,6 +29,21 @@ struct gc_ctx {
     uint64_t launches = 0;
     std::string last_error;
     unsigned int spin_limit = 1u << 22;  // iterations a kernel waits on a predecessor before giving up
+    bool prof = false;
+    int refs = 1;                   // the owner's reference plus one per live graph and model
+    bool destroy_requested = false; // gc_ctx_destroy was called; freed when refs reaches 0
+    std::vector<gc_prof_rec> prof_recs;
+    std::vector<cudaEvent_t> prof_pool;
+};
+
+// Records an event pair around the launches in its scope when profiling is on.
+struct ProfScope {
+    gc_ctx *ctx;
+    cudaStream_t stream;
+    const char *name;
+    cudaEvent_t a = nullptr;
+    ProfScope(gc_ctx *c, const char *n, cudaStream_t s);
+    ~ProfScope();
 };
 
 // Vertices with more neighbours than this are handled by a whole CTA in the GNN layers.
@@ -46,6 +68,7 @@ struct gc_graph {
     uint32_t *P = nullptr;      // predecessor lists, packed at the front of each CSR segment
     uint32_t *pc = nullptr;     // predecessor counts
     uint32_t *order = nullptr;  // vertices by descending key, ascending id on ties: the ticket order
+    uint32_t *leaf_list = nullptr;  // leaves too large for one thread
     uint32_t *sort_buf = nullptr;  // radix sort ping-pong (keys and values), 4 * cap_N words
     uint32_t *sort_hist = nullptr;
     uint32_t sort_hist_cap = 0;
@@ -96,4 +119,4 @@ gc_status gc_priority_gnn(gc_graph *g, const gc_model *m);         // GraphSAGE 
 gc_status gc_jp_color(gc_graph *g);                                // JP by current keys (k_jp.cu)
 gc_status gc_keys_from_colors(gc_graph *g);                        // Culberson step (k_jp.cu)
 gc_status gc_validate_device(gc_graph *g, int *max_color);         // (k_jp.cu)
-gc_status gc_sort_order(gc_graph *g);                              // ticket order (k_sort.cu)
+gc_status gc_sort_order_bits(gc_graph *g, int key_bits, bool filter, uint32_t *d_count);  // (k_sort.cu)

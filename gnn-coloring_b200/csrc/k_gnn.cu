@@ -256,12 +256,18 @@ gc_status launch_layer(gc_graph *g, const float *Wb, const float *x, float *y, c
             return s;
         if ((s = gc_check_cuda(ctx, cudaEventRecord(fork, ctx->stream), "fork")) != GC_OK) return s;
         if ((s = gc_check_cuda(ctx, cudaStreamWaitEvent(side, fork, 0), "fork")) != GC_OK) return s;
+        ProfScope ps(ctx, MODE == MODE_INPUT ? "gnn_hub_input" : (MODE == MODE_HIDDEN ? "gnn_hub_hidden" : "gnn_hub_output"),
+                     side);
         k_gnn_hub<MODE><<<g->n_hubs, HUB_THREADS, smem, side>>>(g->V, g->E, g->N, g->hubs, g->t01, x, y, g->key, Wb);
         ctx->launches++;
         if ((s = gc_check_launch(ctx, "gnn hub layer")) != GC_OK) return s;
     }
     int grid = ctx->num_sms * 8;
-    k_gnn_layer<MODE><<<grid, 256, 0, ctx->stream>>>(g->V, g->E, g->N, g->t01, x, y, g->key, Wb, GC_GNN_HUB_DEGREE);
+    {
+        ProfScope ps(ctx, MODE == MODE_INPUT ? "gnn_input" : (MODE == MODE_HIDDEN ? "gnn_hidden" : "gnn_output"),
+                     ctx->stream);
+        k_gnn_layer<MODE><<<grid, 256, 0, ctx->stream>>>(g->V, g->E, g->N, g->t01, x, y, g->key, Wb, GC_GNN_HUB_DEGREE);
+    }
     ctx->launches++;
     if ((s = gc_check_launch(ctx, "gnn layer")) != GC_OK) return s;
     if (g->n_hubs) {
@@ -290,7 +296,10 @@ gc_status gc_priority_gnn(gc_graph *g, const gc_model *m) {
         if ((s = gc_check_cuda(ctx, cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming), "event")) != GC_OK)
             return s;
     }
-    k_gnn_table0<<<ctx->num_sms * 4, 256, 0, ctx->stream>>>(g->V, g->N, (float)m->md, g->t01);
+    {
+        ProfScope ps(ctx, "gnn_table0", ctx->stream);
+        k_gnn_table0<<<ctx->num_sms * 4, 256, 0, ctx->stream>>>(g->V, g->N, (float)m->md, g->t01);
+    }
     ctx->launches++;
     if ((s = gc_check_launch(ctx, "gnn input table")) != GC_OK) return s;
     const int L = m->layers;

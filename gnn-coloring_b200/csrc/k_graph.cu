@@ -40,6 +40,15 @@ __global__ void k_degree_classes(const uint32_t *__restrict__ V, uint32_t N, uin
     }
 }
 
+__global__ void k_hub_degrees(const uint32_t *__restrict__ V, const uint32_t *__restrict__ hubs, uint32_t n,
+                              uint32_t *__restrict__ out) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        uint32_t u = hubs[i];
+        out[2 * i] = u;
+        out[2 * i + 1] = V[u + 1] - V[u];
+    }
+}
+
 }  // namespace
 
 gc_status gc_graph_prepare(gc_graph *g) {
@@ -80,18 +89,24 @@ gc_status gc_graph_prepare(gc_graph *g) {
     g->n_hubs = n_hubs;
     // hubs by descending degree, so the longest FP32 add chains start first
     if (n_hubs > 1) {
-        std::vector<uint32_t> h(n_hubs), Vh((size_t)g->N + 1);
-        if ((s = gc_check_cuda(ctx, cudaMemcpyAsync(h.data(), g->hubs, 4 * (size_t)n_hubs,
-                                                    cudaMemcpyDeviceToHost, ctx->stream), "hub list")) != GC_OK)
-            return s;
-        if ((s = gc_check_cuda(ctx, cudaMemcpyAsync(Vh.data(), g->V, 4 * ((size_t)g->N + 1),
-                                                    cudaMemcpyDeviceToHost, ctx->stream), "V")) != GC_OK)
-            return s;
-        if ((s = gc_check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "hub list")) != GC_OK) return s;
-        std::sort(h.begin(), h.end(), [&](uint32_t a, uint32_t b) {
-            uint32_t da = Vh[a + 1] - Vh[a], db = Vh[b + 1] - Vh[b];
-            return da != db ? da > db : a < b;
+        // (vertex, degree) pairs of the hubs, sorted on the host by descending degree
+        uint32_t *pairs = nullptr;
+        if ((s = gc_alloc(ctx, &pairs, 2 * (size_t)n_hubs, "hub degrees")) != GC_OK) return s;
+        k_hub_degrees<<<ctx->num_sms, 256, 0, ctx->stream>>>(g->V, g->hubs, n_hubs, pairs);
+        ctx->launches++;
+        std::vector<uint32_t> hp(2 * (size_t)n_hubs), h(n_hubs);
+        s = gc_check_cuda(ctx, cudaMemcpyAsync(hp.data(), pairs, 8 * (size_t)n_hubs, cudaMemcpyDeviceToHost,
+                                               ctx->stream), "hub degrees");
+        if (s == GC_OK) s = gc_check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "hub degrees");
+        cudaFree(pairs);
+        if (s != GC_OK) return s;
+        std::vector<uint32_t> idx(n_hubs);
+        for (uint32_t i = 0; i < n_hubs; i++) idx[i] = i;
+        std::sort(idx.begin(), idx.end(), [&](uint32_t a, uint32_t b) {
+            uint32_t da = hp[2 * a + 1], db = hp[2 * b + 1];
+            return da != db ? da > db : hp[2 * a] < hp[2 * b];
         });
+        for (uint32_t i = 0; i < n_hubs; i++) h[i] = hp[2 * idx[i]];
         if ((s = gc_check_cuda(ctx, cudaMemcpyAsync(g->hubs, h.data(), 4 * (size_t)n_hubs,
                                                     cudaMemcpyHostToDevice, ctx->stream), "hub list")) != GC_OK)
             return s;

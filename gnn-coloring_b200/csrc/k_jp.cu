@@ -18,21 +18,21 @@
 //
 // Colors are published with relaxed GPU-scope stores and read with relaxed GPU-scope loads: the
 // color value is itself the whole message, so no fences are needed.
+#include <cstdlib>
+
 #include "gc_internal.h"
 
-gc_status gc_sort_order_bits(gc_graph *g, int key_bits);
-gc_status gc_order_identity(gc_graph *g);
+gc_status gc_sort_order_bits(gc_graph *g, int key_bits, bool filter, uint32_t *d_count);
 
 namespace {
 using namespace gc;
 
-// Vertices with at most GC_SPLIT_BIG_DEGREE neighbours: one thread each.  Also resets colors.
+// Vertices with at most GC_SPLIT_BIG_DEGREE neighbours: one thread each.
 __global__ void k_jp_split_small(const uint32_t *__restrict__ V, const uint32_t *__restrict__ E,
                                  const uint32_t *__restrict__ key, uint32_t N, uint32_t *__restrict__ P,
-                                 uint32_t *__restrict__ pc, int *__restrict__ color) {
+                                 uint32_t *__restrict__ pc) {
     for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < N; u += gridDim.x * blockDim.x) {
         const uint32_t beg = V[u], end = V[u + 1];
-        color[u] = 0;
         if (end - beg > GC_SPLIT_BIG_DEGREE) {
             pc[u] = 0;  // filled by k_jp_split_big
             continue;
@@ -77,65 +77,173 @@ __global__ void k_jp_split_big(const uint32_t *__restrict__ V, const uint32_t *_
     }
 }
 
+// Sources (no predecessor) take color 1 now; everything else starts uncolored.
+__global__ void k_jp_init_colors(const uint32_t *__restrict__ pc, uint32_t N, int *__restrict__ color) {
+    for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < N; u += gridDim.x * blockDim.x)
+        color[u] = pc[u] == 0 ? 1 : 0;
+}
+
 constexpr int COLOR_THREADS = 256;
 constexpr int COLOR_WARPS = COLOR_THREADS / 32;
-constexpr uint32_t WINDOW = 1024;  // colors covered by one pass over the predecessors
+constexpr uint32_t WINDOW = 1024;   // colors covered by one pass over the predecessors
+constexpr int TRACK = 64;           // per lane: predecessors whose wait is tracked in a bitmask
+constexpr int LOADS = 4;            // predecessor colors in flight per lane
+constexpr uint32_t CORE_TICKETS = 1u << 16;  // first tickets handed out one at a time
 
-__global__ void __launch_bounds__(COLOR_THREADS) k_jp_color(const uint32_t *__restrict__ V, const uint32_t *__restrict__ P,
+__device__ __forceinline__ void mark(uint32_t *fb, int c, uint32_t window) {
+    const uint32_t idx = (uint32_t)(c - 1) - window * WINDOW;
+    if (idx < WINDOW) atomicOr(&fb[idx >> 5], 1u << (idx & 31));
+}
+
+// Smallest free color of the window from the warp's shared bitmap; 0 if the window is full.
+__device__ __forceinline__ int window_mex(const uint32_t *fb, int lane, uint32_t window) {
+    const uint32_t free_bits = ~fb[lane];
+    const unsigned int has = __ballot_sync(0xffffffffu, free_bits != 0);
+    if (!has) return 0;
+    const int l = __ffs(has) - 1;
+    const uint32_t fw = __shfl_sync(0xffffffffu, free_bits, l);
+    return (int)(window * WINDOW + (uint32_t)l * 32 + (uint32_t)(__ffs(fw) - 1) + 1);
+}
+
+// Colors one vertex whose predecessors are list[0..cnt): the smallest color >= 1 none of them
+// has.  Predecessor colors are loaded without waiting first (LOADS per lane in flight); lane
+// entries found uncolored are remembered in a bitmask (the first TRACK entries of each lane) and
+// polled until they are colored, so a warp waiting on its last predecessor re-reads one word, not
+// the whole list.  Entries beyond TRACK per lane (lists longer than 32 * TRACK) are waited on in
+// place.  Returns -1 when a wait exceeded spin_limit polls or another warp raised the error flag.
+__device__ int color_one(const uint32_t *__restrict__ list, uint32_t cnt, const int *color, uint32_t *fb, int lane,
+                         DevState *st, unsigned int spin_limit) {
+    for (uint32_t window = 0;; window++) {
+        fb[lane] = 0;
+        __syncwarp();
+        unsigned long long waiting = 0;  // bit k: entry lane + 32k still uncolored
+        bool gave_up = false;
+        for (uint32_t j0 = 0; j0 < cnt && !gave_up; j0 += 32 * LOADS) {
+            uint32_t v[LOADS];
+            int c[LOADS];
+#pragma unroll
+            for (int q = 0; q < LOADS; q++) {
+                const uint32_t j = j0 + q * 32 + lane;
+                v[q] = j < cnt ? list[j] : 0xffffffffu;
+            }
+#pragma unroll
+            for (int q = 0; q < LOADS; q++) c[q] = v[q] != 0xffffffffu ? ld_relaxed(color + v[q]) : -1;
+#pragma unroll
+            for (int q = 0; q < LOADS; q++) {
+                if (c[q] > 0) {
+                    mark(fb, c[q], window);
+                } else if (c[q] == 0) {
+                    const uint32_t k = (j0 >> 5) + q;  // entry index within the lane
+                    if (k < TRACK) {
+                        waiting |= 1ull << k;
+                    } else {  // untracked: wait in place
+                        unsigned int spins = 0;
+                        int cc;
+                        while ((cc = ld_relaxed(color + v[q])) == 0) {
+                            if (++spins > spin_limit || ((spins & 255u) == 0 && ld_relaxed_u32(&st->err))) {
+                                gave_up = true;
+                                break;
+                            }
+                            __nanosleep(64);
+                        }
+                        if (!gave_up) mark(fb, cc, window);
+                    }
+                }
+            }
+        }
+        // poll the tracked entries until every one is colored
+        unsigned int spins = 0;
+        while (__any_sync(0xffffffffu, waiting != 0 && !gave_up)) {
+            bool progress = false;
+            unsigned long long w = waiting;
+            while (w && !gave_up) {
+                const int k = __ffsll((long long)w) - 1;
+                w &= w - 1;
+                const int cc = ld_relaxed(color + list[(uint32_t)k * 32 + lane]);
+                if (cc) {
+                    mark(fb, cc, window);
+                    waiting &= ~(1ull << k);
+                    progress = true;
+                }
+            }
+            if (waiting && !progress) {
+                if (++spins > spin_limit || ((spins & 255u) == 0 && ld_relaxed_u32(&st->err))) gave_up = true;
+                else if (spins > 32) __nanosleep(spins > 512 ? 256 : 32);
+            }
+        }
+        if (__any_sync(0xffffffffu, gave_up)) return -1;
+        __syncwarp();
+        const int m = window_mex(fb, lane, window);
+        __syncwarp();
+        if (m) return m;
+    }
+}
+
+// The ordered vertices (neither sources nor leaves), one warp each, in ticket order.  Tickets are
+// taken one at a time for the first CORE_TICKETS (the deep, narrow part of the DAG), then in
+// batches of 8 that the warp colors in order.
+__global__ void __launch_bounds__(COLOR_THREADS, 6) k_jp_color(const uint32_t *__restrict__ V, const uint32_t *__restrict__ P,
                                                             const uint32_t *__restrict__ pc,
-                                                            const uint32_t *__restrict__ order, uint32_t n,
-                                                            int *color, DevState *st, unsigned int spin_limit) {
+                                                            const uint32_t *__restrict__ order, int *color,
+                                                            DevState *st, unsigned int spin_limit) {
     __shared__ uint32_t forbid[COLOR_WARPS][32];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     uint32_t *fb = forbid[warp];
+    const uint32_t n = ld_relaxed_u32(&st->ordered);
     for (;;) {
-        uint32_t t = 0;
-        if (lane == 0) t = atomicAdd(&st->ticket, 1u);
-        t = __shfl_sync(0xffffffffu, t, 0);
-        if (t >= n) break;
-        const uint32_t u = order[t];
-        const uint32_t base = V[u], cnt = pc[u];
-        int result = 1;
-        if (cnt) {
-            for (uint32_t window = 0;; window++) {
-                fb[lane] = 0;
-                __syncwarp();
-                bool gave_up = false;
-                for (uint32_t j = lane; j < cnt; j += 32) {
-                    const uint32_t v = P[base + j];
-                    int c = ld_relaxed(color + v);
-                    uint32_t spins = 0;
-                    while (c == 0) {
-                        ++spins;
-                        if (spins > spin_limit || ((spins & 1023u) == 0 && ld_relaxed_u32(&st->err))) {
-                            gave_up = true;
-                            break;
-                        }
-                        if (spins > 256) __nanosleep(128);
-                        c = ld_relaxed(color + v);
-                    }
-                    if (gave_up) break;
-                    const uint32_t idx = (uint32_t)(c - 1) - window * WINDOW;
-                    if (idx < WINDOW) atomicOr(&fb[idx >> 5], 1u << (idx & 31));
-                }
-                if (__any_sync(0xffffffffu, gave_up)) {
-                    if (lane == 0) raise_error(st, ERR_WAIT_EXPIRED, u);
-                    result = -1;  // non-zero, so successors stop waiting; the host reports the error
-                    break;
-                }
-                __syncwarp();
-                const uint32_t free_bits = ~fb[lane];
-                const unsigned int has = __ballot_sync(0xffffffffu, free_bits != 0);
-                if (has) {
-                    const int l = __ffs(has) - 1;
-                    const uint32_t fw = __shfl_sync(0xffffffffu, free_bits, l);
-                    result = (int)(window * WINDOW + (uint32_t)l * 32 + (uint32_t)(__ffs(fw) - 1) + 1);
-                    break;
-                }
-                __syncwarp();
-            }
+        uint32_t t = 0, b = 1;
+        if (lane == 0) {
+            b = ld_relaxed_u32(&st->ticket) < CORE_TICKETS ? 1u : 8u;
+            t = atomicAdd(&st->ticket, b);
         }
-        if (lane == 0) st_relaxed(color + u, result);
+        t = __shfl_sync(0xffffffffu, t, 0);
+        b = __shfl_sync(0xffffffffu, b, 0);
+        if (t >= n) break;
+        const uint32_t t_end = min(n, t + b);
+        for (; t < t_end; t++) {
+            const uint32_t u = order[t];
+            const int c = color_one(P + V[u], pc[u], color, fb, lane, st, spin_limit);
+            if (c < 0 && lane == 0) raise_error(st, ERR_WAIT_EXPIRED, u);
+            // -1 on error is non-zero, so successors stop waiting; the host reports the error
+            if (lane == 0) st_relaxed(color + u, c);
+            __syncwarp();
+        }
+    }
+}
+
+// Leaves (every neighbour is a predecessor) are colored after all other vertices, in parallel:
+// nothing waits on them.  One thread per leaf with a 64-bit mask for degrees up to 62 (so the mex,
+// at most degree + 1, is a bit of the mask); larger leaves are listed for the warp kernel.
+__global__ void k_jp_leaves(const uint32_t *__restrict__ V, const uint32_t *__restrict__ E, const uint32_t *__restrict__ pc,
+                            uint32_t N, int *__restrict__ color, uint32_t *__restrict__ big, DevState *st) {
+    for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < N; u += gridDim.x * blockDim.x) {
+        const uint32_t beg = V[u], d = V[u + 1] - beg;
+        if (d == 0 || pc[u] != d) continue;
+        if (d > 62) {
+            big[atomicAdd(&st->big_leaves, 1u)] = u;
+            continue;
+        }
+        unsigned long long used = 1;  // bit 0 stands for "color 0", never free
+        for (uint32_t i = beg; i < beg + d; i++) {
+            const int c = color[ld_stream(E + i)];
+            if (c > 0 && c < 64) used |= 1ull << c;
+        }
+        color[u] = __ffsll((long long)~used) - 1;
+    }
+}
+
+__global__ void __launch_bounds__(COLOR_THREADS, 6) k_jp_big_leaves(const uint32_t *__restrict__ V, const uint32_t *__restrict__ E,
+                                                                 const uint32_t *__restrict__ big, int *color,
+                                                                 DevState *st) {
+    __shared__ uint32_t forbid[COLOR_WARPS][32];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t n = st->big_leaves;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += nwarps) {
+        const uint32_t u = big[i];
+        // every neighbour is colored already: color_one never waits here
+        const int c = color_one(E + V[u], V[u + 1] - V[u], color, forbid[warp], lane, st, 0xffffffffu);
+        if (lane == 0) color[u] = c;
         __syncwarp();
     }
 }
@@ -168,7 +276,10 @@ __global__ void k_keys_from_colors(const int *__restrict__ color, uint32_t N, ui
         key[u] = (uint32_t)color[u];
 }
 
-__global__ void k_reset_ticket(DevState *st) { st->ticket = 0; }
+__global__ void k_reset_ticket(DevState *st) {
+    st->ticket = 0;
+    st->big_leaves = 0;
+}
 
 int bit_length(uint64_t x) {
     int b = 0;
@@ -189,27 +300,30 @@ gc_status gc_jp_color(gc_graph *g) {
     if ((s = gc_alloc(ctx, &g->P, g->cap_M, "predecessor lists")) != GC_OK) return s;
     if ((s = gc_alloc(ctx, &g->pc, g->cap_N, "predecessor counts")) != GC_OK) return s;
     if ((s = gc_alloc(ctx, &g->order, g->cap_N, "ticket order")) != GC_OK) return s;
+    if ((s = gc_alloc(ctx, &g->leaf_list, g->cap_N, "leaf list")) != GC_OK) return s;
+    const int grid = ctx->num_sms * 8;
 
-    // 1. split
-    k_jp_split_small<<<ctx->num_sms * 8, 256, 0, ctx->stream>>>(g->V, g->E, g->key, N, g->P, g->pc, g->color);
-    ctx->launches++;
-    if (g->n_big_tasks) {
-        k_jp_split_big<<<ctx->num_sms * 8, 256, 0, ctx->stream>>>(g->V, g->E, g->key, g->big, g->n_big_tasks, g->P, g->pc);
+    // 1. split, and color the sources
+    {
+        ProfScope ps(ctx, "jp_split", ctx->stream);
+        k_jp_split_small<<<grid, 256, 0, ctx->stream>>>(g->V, g->E, g->key, N, g->P, g->pc);
+        ctx->launches++;
+        if (g->n_big_tasks) {
+            k_jp_split_big<<<grid, 256, 0, ctx->stream>>>(g->V, g->E, g->key, g->big, g->n_big_tasks, g->P, g->pc);
+            ctx->launches++;
+        }
+        k_jp_init_colors<<<ctx->num_sms * 4, 256, 0, ctx->stream>>>(g->pc, N, g->color);
         ctx->launches++;
     }
     if ((s = gc_check_launch(ctx, "jp split")) != GC_OK) return s;
 
-    // 2. ticket order
-    if (g->key_kind == GC_FF) {
-        s = gc_order_identity(g);  // key = N - u: descending key is ascending id
-    } else {
-        int bits = 32;
-        if (g->key_kind == GC_LF || g->key_kind == GC_SL) bits = bit_length(g->max_deg);
-        else if (g->key_kind == GC_LLF || g->key_kind == GC_SLL) bits = 6;
-        else if (g->key_kind == 100) bits = bit_length((uint64_t)g->max_deg + 1);
-        s = gc_sort_order_bits(g, bits);
-    }
-    if (s != GC_OK) return s;
+    // 2. ticket order of the inner vertices (0 < predecessors < degree)
+    int bits = 32;
+    if (g->key_kind == GC_FF) bits = 0;  // key = N - u: descending key is ascending id
+    else if (g->key_kind == GC_LF || g->key_kind == GC_SL) bits = bit_length(g->max_deg);
+    else if (g->key_kind == GC_LLF || g->key_kind == GC_SLL) bits = 6;
+    else if (g->key_kind == 100) bits = bit_length((uint64_t)g->max_deg + 1);
+    if ((s = gc_sort_order_bits(g, bits, true, &ctx->dstate->ordered)) != GC_OK) return s;
 
     // 3. ordered coloring
     int &blocks_per_sm = ctx->color_blocks_per_sm;
@@ -219,11 +333,28 @@ gc_status gc_jp_color(gc_graph *g) {
                                "occupancy")) != GC_OK)
             return s;
         if (blocks_per_sm < 1) blocks_per_sm = 1;
+        if (const char *e = getenv("GC_JP_BLOCKS_PER_SM")) {
+            int b = atoi(e);
+            if (b >= 1 && b < blocks_per_sm) blocks_per_sm = b;
+        }
     }
     k_reset_ticket<<<1, 1, 0, ctx->stream>>>(ctx->dstate);
-    k_jp_color<<<ctx->num_sms * blocks_per_sm, COLOR_THREADS, 0, ctx->stream>>>(g->V, g->P, g->pc, g->order, N, g->color,
-                                                                                ctx->dstate, ctx->spin_limit);
-    ctx->launches += 2;
+    ctx->launches++;
+    {
+        ProfScope ps(ctx, "jp_color", ctx->stream);
+        k_jp_color<<<ctx->num_sms * blocks_per_sm, COLOR_THREADS, 0, ctx->stream>>>(g->V, g->P, g->pc, g->order,
+                                                                                    g->color, ctx->dstate,
+                                                                                    ctx->spin_limit);
+        ctx->launches++;
+    }
+    // 4. leaves
+    {
+        ProfScope ps(ctx, "jp_leaves", ctx->stream);
+        k_jp_leaves<<<grid, 256, 0, ctx->stream>>>(g->V, g->E, g->pc, N, g->color, g->leaf_list, ctx->dstate);
+        k_jp_big_leaves<<<ctx->num_sms * 2, COLOR_THREADS, 0, ctx->stream>>>(g->V, g->E, g->leaf_list, g->color,
+                                                                              ctx->dstate);
+        ctx->launches += 2;
+    }
     if ((s = gc_check_launch(ctx, "jp color")) != GC_OK) return s;
     g->has_colors = true;
     return GC_OK;
@@ -232,6 +363,7 @@ gc_status gc_jp_color(gc_graph *g) {
 gc_status gc_keys_from_colors(gc_graph *g) {
     gc_ctx *ctx = g->ctx;
     if (g->N == 0) return GC_OK;
+    ProfScope ps(ctx, "culberson_keys", ctx->stream);
     k_keys_from_colors<<<ctx->num_sms * 4, 256, 0, ctx->stream>>>(g->color, g->N, g->key);
     ctx->launches++;
     g->key_kind = 100;
@@ -246,7 +378,10 @@ gc_status gc_validate_device(gc_graph *g, int *max_color) {
         return GC_OK;
     }
     if ((s = gc_reset_state(ctx)) != GC_OK) return s;
-    k_validate<<<ctx->num_sms * 8, 256, 0, ctx->stream>>>(g->V, g->E, g->N, g->color, ctx->dstate);
+    {
+        ProfScope ps(ctx, "validate", ctx->stream);
+        k_validate<<<ctx->num_sms * 8, 256, 0, ctx->stream>>>(g->V, g->E, g->N, g->color, ctx->dstate);
+    }
     ctx->launches++;
     if ((s = gc_check_launch(ctx, "validate")) != GC_OK) return s;
     if ((s = gc_read_state(ctx)) != GC_OK) return s;

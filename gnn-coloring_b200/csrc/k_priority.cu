@@ -162,6 +162,7 @@ gc_status gc_priority_simple(gc_graph *g, gc_heuristic h) {
     gc_ctx *ctx = g->ctx;
     if (g->N == 0) return GC_OK;
     int grid = ctx->num_sms * 4;
+    ProfScope ps(ctx, "priority_keys", ctx->stream);
     k_simple_keys<<<grid, 256, 0, ctx->stream>>>(g->V, g->N, (int)h, g->key);
     ctx->launches++;
     return gc_check_launch(ctx, "priority keys");
@@ -194,6 +195,7 @@ gc_status gc_priority_peel(gc_graph *g, bool log_thresholds) {
     uint32_t queued = 0;
     uint32_t batch = log_thresholds ? 16 : 32;
     for (;;) {
+        ProfScope prof(ctx, "peel_rounds", ctx->stream);
         for (uint32_t r = 0; r < batch; r++) {
             k_peel_filter<<<grid, 256, 0, ctx->stream>>>(g->frontier, g->frontier2, g->removed, g->deg_rem,
                                                         g->key, ps);

@@ -22,33 +22,64 @@ constexpr int SORT_ITEMS = 32;                               // per lane
 constexpr int SORT_TILE = SORT_THREADS * SORT_ITEMS;          // 8192 elements per CTA
 constexpr int RADIX = 256;
 
-__device__ __forceinline__ uint32_t load_key(const uint32_t *kin, const uint32_t *key, uint32_t n, uint32_t j, bool first) {
-    return first ? key[j] : kin[j];
-}
-__device__ __forceinline__ uint32_t digit_of(uint32_t k, int shift) { return ((~k) >> shift) & (RADIX - 1); }
+// Element j of a pass: the first pass reads the heuristic's keys directly (optionally keeping
+// only vertices the filter selects); later passes read the previous pass's output, whose length
+// the first pass's scan left in device memory.
+struct SortIn {
+    const uint32_t *kin, *vin;  // previous pass (later passes)
+    const uint32_t *key;        // keys by vertex (first pass)
+    const uint32_t *V, *pc;     // filter: keep u when 0 < pc[u] < deg(u)
+    const uint32_t *d_n;        // element count of later passes
+    uint32_t N;
+    int first, filter;
+};
 
-__global__ void __launch_bounds__(SORT_THREADS) k_sort_hist(const uint32_t *__restrict__ kin, const uint32_t *__restrict__ key,
-                                                            uint32_t n, int shift, int first,
+__device__ __forceinline__ bool sort_elem(const SortIn &in, uint32_t j, uint32_t n, uint32_t &k, uint32_t &v) {
+    if (in.first) {
+        if (j >= in.N) return false;
+        if (in.filter) {
+            const uint32_t p = in.pc[j], d = in.V[j + 1] - in.V[j];
+            if (p == 0 || p >= d) return false;
+        }
+        k = in.key[j];
+        v = j;
+        return true;
+    }
+    if (j >= n) return false;
+    k = in.kin[j];
+    v = in.vin[j];
+    return true;
+}
+
+__device__ __forceinline__ uint32_t digit_of(uint32_t k, int shift, uint32_t mask) { return ((~k) >> shift) & mask; }
+
+__device__ __forceinline__ uint32_t pass_len(const SortIn &in) { return in.first ? in.N : min(in.N, *in.d_n); }
+
+__global__ void __launch_bounds__(SORT_THREADS) k_sort_hist(SortIn in, int shift, uint32_t mask,
                                                             uint32_t *__restrict__ counts, uint32_t ntiles) {
     __shared__ uint32_t hist[RADIX];
     for (int i = threadIdx.x; i < RADIX; i += SORT_THREADS) hist[i] = 0;
     __syncthreads();
     const uint32_t tile = blockIdx.x;
     const uint32_t base = tile * SORT_TILE;
+    const uint32_t n = pass_len(in);
     const int lane = threadIdx.x & 31;
-    for (int s = 0; s < SORT_ITEMS; s++) {
-        uint32_t j = base + s * SORT_THREADS + threadIdx.x;
-        bool valid = j < n;
-        uint32_t d = valid ? digit_of(load_key(kin, key, n, j, first), shift) : 0xffffffffu;
-        unsigned int peers = __match_any_sync(0xffffffffu, d);
-        if (valid && lane == __ffs(peers) - 1) atomicAdd(&hist[d], (uint32_t)__popc(peers));
+    if (base < n) {
+        for (int s = 0; s < SORT_ITEMS; s++) {
+            uint32_t j = base + s * SORT_THREADS + threadIdx.x, k, v;
+            bool valid = sort_elem(in, j, n, k, v);
+            uint32_t d = valid ? digit_of(k, shift, mask) : 0xffffffffu;
+            unsigned int peers = __match_any_sync(0xffffffffu, d);
+            if (valid && lane == __ffs(peers) - 1) atomicAdd(&hist[d], (uint32_t)__popc(peers));
+        }
     }
     __syncthreads();
     for (int d = threadIdx.x; d < RADIX; d += SORT_THREADS) counts[(size_t)d * ntiles + tile] = hist[d];
 }
 
-// Exclusive scan of `total` counters in place by one CTA of 1024 threads.
-__global__ void __launch_bounds__(1024) k_sort_scan(uint32_t *__restrict__ counts, uint32_t total) {
+// Exclusive scan of `total` counters in place by one CTA of 1024 threads; the grand total (the
+// number of sorted elements) goes to *d_total when given.
+__global__ void __launch_bounds__(1024) k_sort_scan(uint32_t *__restrict__ counts, uint32_t total, uint32_t *d_total) {
     __shared__ uint32_t part[1024];
     const uint32_t per = (total + 1023) / 1024;
     const uint32_t b = threadIdx.x * per, e = min(total, b + per);
@@ -69,29 +100,30 @@ __global__ void __launch_bounds__(1024) k_sort_scan(uint32_t *__restrict__ count
         counts[i] = run;
         run += c;
     }
+    if (d_total && threadIdx.x == 1023) *d_total = part[1023];
 }
 
-__global__ void __launch_bounds__(SORT_THREADS) k_sort_scatter(const uint32_t *__restrict__ kin, const uint32_t *__restrict__ vin,
-                                                               const uint32_t *__restrict__ key, uint32_t n, int shift,
-                                                               int first, const uint32_t *__restrict__ offsets,
-                                                               uint32_t ntiles, uint32_t *__restrict__ kout,
-                                                               uint32_t *__restrict__ vout) {
+__global__ void __launch_bounds__(SORT_THREADS) k_sort_scatter(SortIn in, int shift, uint32_t mask,
+                                                               const uint32_t *__restrict__ offsets, uint32_t ntiles,
+                                                               uint32_t *__restrict__ kout, uint32_t *__restrict__ vout) {
     __shared__ uint32_t wcnt[SORT_WARPS][RADIX];
     __shared__ uint32_t gbase[RADIX];
+    const uint32_t n = pass_len(in);
+    if (blockIdx.x * SORT_TILE >= n) return;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (int d = lane; d < RADIX; d += 32) wcnt[warp][d] = 0;
     for (int d = threadIdx.x; d < RADIX; d += SORT_THREADS) gbase[d] = offsets[(size_t)d * ntiles + blockIdx.x];
     __syncwarp();
     const uint32_t wbase = blockIdx.x * SORT_TILE + warp * (32 * SORT_ITEMS);
     uint32_t k[SORT_ITEMS], v[SORT_ITEMS], pos[SORT_ITEMS];
+    uint32_t valid_mask = 0;
     const unsigned int lt = (1u << lane) - 1u;
 #pragma unroll
     for (int s = 0; s < SORT_ITEMS; s++) {
         uint32_t j = wbase + s * 32 + lane;
-        bool valid = j < n;
-        k[s] = valid ? load_key(kin, key, n, j, first) : 0u;
-        v[s] = valid ? (first ? j : vin[j]) : 0u;
-        uint32_t d = valid ? digit_of(k[s], shift) : 0xffffffffu;
+        bool valid = sort_elem(in, j, n, k[s], v[s]);
+        if (valid) valid_mask |= 1u << s;
+        uint32_t d = valid ? digit_of(k[s], shift, mask) : 0xffffffffu;
         unsigned int peers = __match_any_sync(0xffffffffu, d);
         uint32_t before = valid ? wcnt[warp][d] : 0;
         pos[s] = before + __popc(peers & lt);
@@ -112,65 +144,57 @@ __global__ void __launch_bounds__(SORT_THREADS) k_sort_scatter(const uint32_t *_
     __syncthreads();
 #pragma unroll
     for (int s = 0; s < SORT_ITEMS; s++) {
-        uint32_t j = wbase + s * 32 + lane;
-        if (j < n) {
-            uint32_t dst = wcnt[warp][digit_of(k[s], shift)] + pos[s];
+        if (valid_mask & (1u << s)) {
+            uint32_t dst = wcnt[warp][digit_of(k[s], shift, mask)] + pos[s];
             kout[dst] = k[s];
             vout[dst] = v[s];
         }
     }
 }
 
-__global__ void k_iota(uint32_t *__restrict__ out, uint32_t n) {
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = i;
-}
-
 }  // namespace
 
-// Sorts into g->order.  key_bits: number of low key bits that may be non-zero.
-gc_status gc_sort_order_bits(gc_graph *g, int key_bits) {
+// Sorts into g->order.  key_bits: number of low key bits that may be non-zero; 0 means "all keys
+// equal" (a stable compaction by id).  With `filter`, only vertices with 0 < pc < deg take part
+// (the inner vertices of the coloring DAG) and their number is left in *d_count; otherwise
+// *d_count = N.
+gc_status gc_sort_order_bits(gc_graph *g, int key_bits, bool filter, uint32_t *d_count) {
     gc_ctx *ctx = g->ctx;
     gc_status s;
-    const uint32_t n = g->N;
-    if (n == 0) return GC_OK;
+    const uint32_t N = g->N;
+    if (N == 0) return GC_OK;
     if ((s = gc_alloc(ctx, &g->sort_buf, 4 * (size_t)g->cap_N, "sort buffers")) != GC_OK) return s;
-    const uint32_t ntiles = (n + SORT_TILE - 1) / SORT_TILE;
+    const uint32_t ntiles = (N + SORT_TILE - 1) / SORT_TILE;
     if (g->sort_hist_cap < (size_t)RADIX * ntiles) {
         if (g->sort_hist) cudaFree(g->sort_hist);
         g->sort_hist = nullptr;
         if ((s = gc_alloc(ctx, &g->sort_hist, (size_t)RADIX * ntiles, "sort histogram")) != GC_OK) return s;
         g->sort_hist_cap = RADIX * ntiles;
     }
-    if (key_bits <= 0) {
-        // every key is 0: ascending id order
-        // (a single stable pass over a constant digit produces exactly that)
-        key_bits = 1;
-    }
-    const int passes = (key_bits + 7) / 8;
+    const int passes = key_bits <= 0 ? 1 : (key_bits + 7) / 8;
     uint32_t *k0 = g->sort_buf, *v0 = g->sort_buf + g->cap_N;
     uint32_t *k1 = g->sort_buf + 2 * (size_t)g->cap_N, *v1 = g->sort_buf + 3 * (size_t)g->cap_N;
-    const uint32_t *kin = nullptr, *vin = nullptr;
+    SortIn in{};
+    in.key = g->key;
+    in.V = g->V;
+    in.pc = g->pc;
+    in.d_n = d_count;
+    in.N = N;
+    in.filter = filter ? 1 : 0;
+    ProfScope ps(ctx, "sort", ctx->stream);
     for (int p = 0; p < passes; p++) {
         const int shift = 8 * p;
-        const int first = (p == 0);
+        const uint32_t mask = key_bits <= 0 ? 0u : (uint32_t)(RADIX - 1);
+        in.first = (p == 0);
         uint32_t *kout = (p & 1) ? k1 : k0, *vout = (p & 1) ? v1 : v0;
         if (p == passes - 1) vout = g->order;  // last pass writes the ticket order directly
-        k_sort_hist<<<ntiles, SORT_THREADS, 0, ctx->stream>>>(kin, g->key, n, shift, first, g->sort_hist, ntiles);
-        k_sort_scan<<<1, 1024, 0, ctx->stream>>>(g->sort_hist, RADIX * ntiles);
-        k_sort_scatter<<<ntiles, SORT_THREADS, 0, ctx->stream>>>(kin, vin, g->key, n, shift, first, g->sort_hist, ntiles,
-                                                                 kout, vout);
+        k_sort_hist<<<ntiles, SORT_THREADS, 0, ctx->stream>>>(in, shift, mask, g->sort_hist, ntiles);
+        k_sort_scan<<<1, 1024, 0, ctx->stream>>>(g->sort_hist, RADIX * ntiles, p == 0 ? d_count : nullptr);
+        k_sort_scatter<<<ntiles, SORT_THREADS, 0, ctx->stream>>>(in, shift, mask, g->sort_hist, ntiles, kout, vout);
         ctx->launches += 3;
         if ((s = gc_check_launch(ctx, "radix sort")) != GC_OK) return s;
-        kin = kout;
-        vin = vout;
+        in.kin = kout;
+        in.vin = vout;
     }
     return GC_OK;
-}
-
-gc_status gc_order_identity(gc_graph *g) {
-    gc_ctx *ctx = g->ctx;
-    if (g->N == 0) return GC_OK;
-    k_iota<<<ctx->num_sms * 4, 256, 0, ctx->stream>>>(g->order, g->N);
-    ctx->launches++;
-    return gc_check_launch(ctx, "identity order");
 }

@@ -13,8 +13,10 @@ CUDA device is visible.  Nothing here falls back to the CPU.
 """
 from __future__ import annotations
 
+import atexit
 import ctypes as C
 import os
+import weakref
 from typing import Optional, Tuple
 
 import numpy as np
@@ -202,6 +204,26 @@ def model_write(path: str, params: np.ndarray, md: int):
 
 # ---- native device API ---------------------------------------------------------------------------
 
+# Live handles, closed at interpreter exit before module teardown (graphs and models first), so no
+# CUDA call runs after the CUDA runtime has shut down.
+_live_objects: "weakref.WeakSet" = weakref.WeakSet()
+_live_contexts: "weakref.WeakSet" = weakref.WeakSet()
+
+
+@atexit.register
+def _close_all():
+    for obj in list(_live_objects):
+        try:
+            obj.close()
+        except Exception:
+            pass
+    for ctx in list(_live_contexts):
+        try:
+            ctx.close()
+        except Exception:
+            pass
+
+
 class Context:
     def __init__(self, device: int = 0):
         h = vp()
@@ -209,6 +231,7 @@ class Context:
         if st != 0:
             raise GCError(st, "gc_ctx_create")
         self.h = h
+        _live_contexts.add(self)
 
     def close(self):
         if self.h:
@@ -243,6 +266,7 @@ class Model:
         h = vp()
         ctx.check(lib.gc_model_create(ctx.h, len(params), md, _ptr(params, f32p), C.byref(h)), "model")
         self.h = h
+        _live_objects.add(self)
 
     @classmethod
     def load(cls, ctx: Context, path: str) -> "Model":
@@ -274,6 +298,7 @@ class Graph:
         h = vp()
         ctx.check(lib.gc_graph_upload(ctx.h, self.N, _ptr(self.V, u32p), _ptr(self.E, u32p), C.byref(h)), "upload")
         self.h = h
+        _live_objects.add(self)
 
     @property
     def M(self) -> int:

@@ -63,6 +63,8 @@ const char *gc_status_string(gc_status s);
 
 /* Creates a context on `device` with its own non-blocking stream. */
 gc_status gc_ctx_create(int device, gc_ctx **ctx);
+/* Releases the caller's handle.  Graphs and models hold their context: its memory and stream go
+ * when the last of them is freed, so handles may be released in any order. */
 void gc_ctx_destroy(gc_ctx *ctx);
 /* Last error message of this context ("" when none). */
 const char *gc_last_error(const gc_ctx *ctx);
@@ -72,6 +74,12 @@ void *gc_ctx_stream(gc_ctx *ctx);
 gc_status gc_sync(gc_ctx *ctx);
 /* Number of kernels this context has launched so far (instrumentation for benchmarks). */
 uint64_t gc_ctx_launches(const gc_ctx *ctx);
+/* Per-kernel timing: when on, every kernel launch group is bracketed by CUDA events on the stream
+ * it runs on.  Turning it on clears earlier records. */
+gc_status gc_prof_enable(gc_ctx *ctx, int on);
+/* Waits for the stream, then aggregates the records by kernel name: up to `max` entries of
+ * (name, total milliseconds, launches).  Returns the number of distinct names (may exceed max). */
+int gc_prof_read(gc_ctx *ctx, const char **names, double *total_ms, uint64_t *launches, int max);
 
 /* ---- graphs ------------------------------------------------------------------------------- */
 

@@ -132,6 +132,28 @@ def jp_color(N: int, V, E, p) -> np.ndarray:
     return out
 
 
+def greedy_color_defined(N: int, V, E, p) -> np.ndarray:
+    """The reference's greedy_internal (coloring.c:60-125) with its uninitialized reads made
+    deterministic.  Its mex loop reads marks[c] for c up to max_degree + 1, but only entries
+    0..max_degree are initialized (coloring.c:89-90), and marks holds only N entries.  Here the
+    state is set up for N + 2 vertices and marks is filled with 0xFFFFFFFF (never a vertex id)
+    before the call, so those reads see "not marked", which is what the algorithm means."""
+    L = lib()
+    V, E, Vp, Ep = _csr(V, E)
+    if N == 0:
+        return np.zeros(0, np.int32)
+    pp = aligned(N + 8, np.float64)
+    pp[:N] = p
+    color = np.zeros(N, np.int32)
+    gd = L.greedy_setup(N + 2, max(int(V[N]), 1))
+    # struct gd_data { uint32_t *next, *prev, *count, *pred, *E_split, *marks; } (coloring.c:18-24)
+    marks = C.cast(gd, C.POINTER(C.c_void_p))[5]
+    C.memset(marks, 0xFF, 4 * (N + 2))
+    L.greedy_internal(N, Vp, Ep, gd, pp.ctypes.data, color.ctypes.data_as(i32p))
+    L.greedy_cleanup(gd)
+    return color
+
+
 def greedy_color(N: int, V, E, p) -> np.ndarray:
     L = lib()
     V, E, Vp, Ep = _csr(V, E)

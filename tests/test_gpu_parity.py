@@ -1,0 +1,261 @@
+"""GPU parity: the CUDA path (through the C ABI) against the reference's golden vectors and the
+oracle.  Integer heuristics and colors must be identical; GraphSAGE priorities must be identical
+bit for bit (tolerance 0: the kernels reproduce the reference's FP32 operation order)."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import gnn_coloring as gcn
+from conftest import HEURISTICS, PKG
+from oracle import reference as R
+from oracle import restatement as O
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def models(gpu_ctx, golden):
+    return {L: gcn.Model(gpu_ctx, *golden.model(L)) for L in (2, 3, 4)}
+
+
+def gpu_run(ctx, N, V, E, heur, models):
+    g = gcn.Graph(ctx, N, V, E)
+    if heur.startswith("GNN"):
+        g.priority("GNN", models[int(heur[3:])])
+    else:
+        g.priority(heur)
+    count = g.color()
+    return g, g.priorities(), g.colors(), count
+
+
+@pytest.mark.parametrize("heur", HEURISTICS)
+def test_golden_parity(gpu_ctx, golden, models, heur):
+    for name in golden.graphs:
+        N, V, E = golden.graph(name)
+        g, p, c, count = gpu_run(gpu_ctx, N, V, E, heur, models)
+        assert np.array_equal(p, golden.get(name, heur, "p")), (name, heur, "priorities")
+        assert np.array_equal(c, golden.get(name, heur, "color")), (name, heur, "colors")
+        assert count == (int(c.max()) if N else 1)
+        assert count == O.validate(N, V, E, c)
+        g.recolor(3)
+        assert np.array_equal(g.colors(), golden.get(name, heur, "culb3")), (name, heur, "culberson")
+        g.close()
+
+
+def test_reference_models(gpu_ctx, golden, golden_ref):
+    if not os.path.exists(os.path.join(R.MODELS, "m3.gnn")):
+        pytest.skip("reference model files not present (oracle/_ref/models)")
+    for L in (2, 3, 4):
+        m = gcn.Model.load(gpu_ctx, os.path.join(R.MODELS, f"m{L}.gnn"))
+        for name in ("er1500", "rmat11", "bridged"):
+            N, V, E = golden.graph(name)
+            g = gcn.Graph(gpu_ctx, N, V, E)
+            g.priority("GNN", m)
+            g.color()
+            assert np.array_equal(g.priorities(), golden_ref[f"{name}/GNN{L}/p"]), (name, L)
+            assert np.array_equal(g.colors(), golden_ref[f"{name}/GNN{L}/color"]), (name, L)
+
+
+def er65k():
+    # the plain CPU-runnable configuration: ER n=65,536, 524,288 undirected edges, seed 1
+    return gcn.gen_er(65536, 524288, 1)
+
+
+@pytest.mark.parametrize("heur", HEURISTICS)
+def test_er65k_all_heuristics(gpu_ctx, golden, models, heur):
+    N, V, E = er65k()
+    g, p, c, count = gpu_run(gpu_ctx, N, V, E, heur, models)
+    if heur.startswith("GNN"):
+        params, md = golden.model(int(heur[3:]))
+        po = O.ordering("GNN", N, V, E, params, md)
+    else:
+        po = O.ordering(heur, N, V, E)
+    assert np.array_equal(p, po), heur
+    co, _ = O.greedy_color(N, V, E, po)
+    assert np.array_equal(c, co), heur
+    assert count == int(co.max())
+
+
+@pytest.mark.parametrize("scale,heur", [(16, "GNN3"), (16, "SL"), (18, "GNN3"), (18, "LF"), (18, "SLL"),
+                                        (18, "LLF"), (18, "FF")])
+def test_rmat_vs_oracle(gpu_ctx, golden, models, scale, heur):
+    N, V, E = gcn.gen_rmat(1 << scale, 16, 2)
+    g, p, c, count = gpu_run(gpu_ctx, N, V, E, heur, models)
+    if heur.startswith("GNN"):
+        params, md = golden.model(int(heur[3:]))
+        po = O.ordering("GNN", N, V, E, params, md)
+    else:
+        po = O.ordering(heur, N, V, E)
+    assert np.array_equal(p, po)
+    co, _ = O.greedy_color(N, V, E, po)
+    assert np.array_equal(c, co)
+    g.recolor(2)
+    assert np.array_equal(g.colors(), O.culberson(N, V, E, co, 2))
+
+
+def test_mesh_graphs_culberson(gpu_ctx, golden, models):
+    """Mesh-like inputs with GNN4 + JP + 9 Culberson recolorings (the -c 10 protocol)."""
+    for N, V, E in (gcn.gen_rgg2d(1 << 16, float(np.sqrt(12 / (np.pi * (1 << 16)))), 3),
+                    gcn.gen_stencil27(24, 24, 24)):
+        g, p, c, count = gpu_run(gpu_ctx, N, V, E, "GNN4", models)
+        params, md = golden.model(4)
+        po = O.ordering("GNN", N, V, E, params, md)
+        assert np.array_equal(p, po)
+        co, _ = O.greedy_color(N, V, E, po)
+        assert np.array_equal(c, co)
+        counts = [count]
+        for _ in range(9):
+            counts.append(g.recolor(1))
+        assert all(b <= a for a, b in zip(counts, counts[1:]))
+        assert np.array_equal(g.colors(), O.culberson(N, V, E, co, 9))
+
+
+def test_user_priorities(gpu_ctx):
+    N, V, E = gcn.gen_rmat(1 << 12, 8, 21)
+    rng = np.random.default_rng(0)
+    for p in (rng.integers(0, 5, N).astype(np.float64),                 # many ties
+              rng.normal(size=N),                                      # negatives, non-integers
+              np.where(rng.random(N) < 0.5, -0.0, 0.0),                # -0.0 equals +0.0
+              rng.integers(0, 2**32 - 1, N).astype(np.float64)):       # full uint32 range
+        g = gcn.Graph(gpu_ctx, N, V, E)
+        g.set_priority(p)
+        g.color()
+        co, _ = O.greedy_color(N, V, E, p)
+        assert np.array_equal(g.colors(), co)
+        assert np.array_equal(g.priorities(), p)
+    g = gcn.Graph(gpu_ctx, N, V, E)
+    bad = np.zeros(N)
+    bad[5] = np.nan
+    with pytest.raises(gcn.GCError) as e:
+        g.set_priority(bad)
+    assert e.value.name == "GC_ERR_INVALID"
+
+
+def test_deterministic_repeats(gpu_ctx, models):
+    N, V, E = gcn.gen_rmat(1 << 15, 16, 5)
+    g = gcn.Graph(gpu_ctx, N, V, E)
+    ref = None
+    for _ in range(3):
+        g.priority("GNN", models[3])
+        g.color()
+        c = g.colors()
+        if ref is None:
+            ref = c
+        assert np.array_equal(c, ref)
+
+
+def test_call_order_and_bad_input(gpu_ctx):
+    N, V, E = gcn.gen_er(100, 300, 1)
+    g = gcn.Graph(gpu_ctx, N, V, E)
+    with pytest.raises(gcn.GCError) as e:
+        g.color()
+    assert e.value.name == "GC_ERR_STATE"
+    with pytest.raises(gcn.GCError) as e:
+        g.priority("GNN")  # no model
+    assert e.value.name == "GC_ERR_INVALID"
+    bad = E.copy()
+    bad[3] = 1000  # out of range
+    with pytest.raises(gcn.GCError) as e:
+        gcn.Graph(gpu_ctx, N, V, bad)
+    assert e.value.name == "GC_ERR_INVALID"
+    # the context is still usable
+    g.priority("LF")
+    assert g.color() > 0
+
+
+def test_bounded_wait_expires_cleanly(monkeypatch):
+    """A context whose wait limit is 0 gives up on the first uncolored predecessor: the kernel
+    raises its error flag and returns, the host reports GC_ERR_DEVICE, and the context stays usable."""
+    monkeypatch.setenv("GC_SPIN_LIMIT", "0")
+    ctx = gcn.Context(int(os.environ.get("GC_DEVICE", "0")))
+    n = 200000
+    I = np.arange(n - 1, dtype=np.uint32)
+    N, V, E = gcn.csr_from_pairs(n, I, I + 1)  # a path: FF makes one chain of n waits
+    g = gcn.Graph(ctx, N, V, E)
+    g.priority("FF")
+    with pytest.raises(gcn.GCError) as e:
+        g.color()
+    assert e.value.name == "GC_ERR_DEVICE"
+    # no waits at all: succeeds on the same context
+    N2, V2, E2 = gcn.csr_from_pairs(1000, np.zeros(0, np.uint32), np.zeros(0, np.uint32))
+    g2 = gcn.Graph(ctx, N2, V2, E2)
+    g2.priority("LF")
+    assert g2.color() == 1
+    g.close()
+    g2.close()
+    ctx.close()
+
+
+def test_legacy_abi(golden):
+    """The reference-named entry points (include/coloring.h etc.) with host buffers."""
+    L = gcn.legacy
+    for name in ("er1500", "rmat11", "bridged", "path7"):
+        N, V, E = golden.graph(name)
+        for fn, h in (("first_fit_ordering", "FF"), ("largest_degree_first_ordering", "LF"),
+                      ("largest_log_degree_first_ordering", "LLF"), ("smallest_degree_last_ordering", "SL"),
+                      ("smallest_log_degree_last_ordering", "SLL")):
+            p = L.ordering(fn, N, V, E)
+            assert np.array_equal(p, golden.get(name, h, "p")), (name, fn)
+            c = L.coloring("jones_plassmann_coloring", N, V, E, p)
+            assert np.array_equal(c, golden.get(name, h, "color")), (name, fn)
+            assert np.array_equal(L.coloring("greedy_coloring", N, V, E, p), c)
+            assert L.validate(N, V, E, c) == int(c.max())
+        for fn, h in (("first_fit_coloring", "FF"), ("largest_degree_first_coloring_par", "LF"),
+                      ("largest_log_degree_first_coloring", "LLF"), ("smallest_degree_last_coloring_par", "SL"),
+                      ("smallest_log_degree_last_coloring", "SLL")):
+            assert np.array_equal(L.coloring(fn, N, V, E), golden.get(name, h, "color")), (name, fn)
+        params, md = golden.model(3)
+        p = L.graph_sage(params, md, N, V, E)
+        assert np.array_equal(p, golden.get(name, "GNN3", "p"))
+        bad = golden.get(name, "FF", "color").copy()
+        if len(E):
+            u = int(np.argmax(np.diff(V) > 0))
+            bad[u] = bad[E[V[u]]]
+            assert L.validate(N, V, E, bad) == 0
+
+
+def test_legacy_gnn_ordering_reads_model_dir(golden, tmp_path, monkeypatch):
+    for L in (2, 3, 4):
+        params, md = golden.model(L)
+        gcn.model_write(str(tmp_path / f"m{L}.gnn"), params, md)
+    monkeypatch.setenv("GC_MODEL_DIR", str(tmp_path))
+    N, V, E = golden.graph("rmat11")
+    for L in (2, 3, 4):
+        p = gcn.legacy.ordering("gnn_ordering", N, V, E, layers=L)
+        assert np.array_equal(p, golden.get("rmat11", f"GNN{L}", "p"))
+
+
+def test_cli_output_lines(golden, tmp_path):
+    """./coloring prints the reference's line format with the oracle's color counts."""
+    for L in (2, 3, 4):
+        params, md = golden.model(L)
+        gcn.model_write(str(tmp_path / f"m{L}.gnn"), params, md)
+    N, V, E = golden.graph("er1500")
+    path = str(tmp_path / "g.mtx")
+    gcn.mtx_write(path, N, V, E)
+    env = dict(os.environ, GC_MODEL_DIR=str(tmp_path))
+    r = subprocess.run([os.path.join(PKG, "cli", "coloring"), "-g", path, "-c", "2", "1", "8"],
+                       capture_output=True, text=True, timeout=600, env=env)
+    assert r.returncode == 0, r.stderr
+    lines = r.stdout.rstrip("\n").split("\n")
+    names = [ln.split()[0] for ln in lines]
+    assert names == [f"{h}_{i}" for h in ("FF", "LF", "LLF", "SL", "SLL", "GNN2", "GNN3", "GNN4") for i in (0, 1)]
+    for ln in lines:
+        parts = ln.split(" ")
+        assert parts[-1] == ""  # trailing space as in src/runner.c:166-168
+        name, colors, times = parts[0], int(parts[1]), parts[2:-1]
+        assert len(times) == 3 and all(len(t.split(".")[1]) == 6 for t in times)
+        h, i = name.split("_")
+        want = golden.get("er1500", h, "color")
+        if i == "1":
+            want = O.culberson(N, V, E, want, 1)
+        assert colors == int(want.max()), name
+    q = subprocess.run([os.path.join(PKG, "cli", "coloring"), "-g", path, "-q"], capture_output=True, text=True,
+                       timeout=600, env=env)
+    assert q.returncode == 0, q.stderr
+    vals = [int(x) for x in q.stdout.split()]
+    expect = [int(golden.get("er1500", h, "color").max()) for h in ("FF", "LF", "LLF", "SL", "SLL")]
+    expect += [0, 0, 0] + [int(golden.get("er1500", f"GNN{L}", "color").max()) for L in (2, 3, 4)]
+    assert vals == expect

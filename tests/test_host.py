@@ -1,0 +1,111 @@
+"""Host-side graph preparation: Matrix Market rules, generators, .gnn models (no GPU)."""
+import os
+
+import numpy as np
+import pytest
+
+import gnn_coloring as gcn
+
+
+def is_simple_sorted_symmetric(N, V, E):
+    if V[0] != 0 or np.any(np.diff(V.astype(np.int64)) < 0) or V[N] != len(E):
+        return False
+    edges = set()
+    for u in range(N):
+        row = E[V[u]:V[u + 1]]
+        if np.any(np.diff(row.astype(np.int64)) <= 0) or np.any(row == u) or np.any(row >= N):
+            return False
+        edges.update((u, int(v)) for v in row)
+    return all((v, u) in edges for (u, v) in edges)
+
+
+def test_mtx_matches_reference_csr(golden_mtx, tmp_path):
+    names = sorted({k.split("/")[0] for k in golden_mtx.files})
+    for name in names:
+        path = tmp_path / f"{name}.mtx"
+        path.write_bytes(golden_mtx[f"{name}/text"].tobytes())
+        N, V, E = gcn.mtx_read(str(path))
+        assert N == int(golden_mtx[f"{name}/N"]), name
+        assert np.array_equal(V, golden_mtx[f"{name}/V"]), name
+        assert np.array_equal(E, golden_mtx[f"{name}/E"]), name
+
+
+def test_mtx_rejects_bad_indices(tmp_path):
+    bad = tmp_path / "bad.mtx"
+    bad.write_text("%%MatrixMarket matrix coordinate pattern symmetric\n3 3 2\n1 2\n0 3\n")
+    with pytest.raises(gcn.GCError) as e:
+        gcn.mtx_read(str(bad))
+    assert e.value.name == "GC_ERR_FORMAT"
+    trunc = tmp_path / "trunc.mtx"
+    trunc.write_text("%%MatrixMarket matrix coordinate pattern symmetric\n3 3 5\n1 2\n")
+    with pytest.raises(gcn.GCError):
+        gcn.mtx_read(str(trunc))
+    with pytest.raises(gcn.GCError) as e:
+        gcn.mtx_read(str(tmp_path / "missing.mtx"))
+    assert e.value.name == "GC_ERR_IO"
+
+
+def test_mtx_roundtrip(tmp_path):
+    N, V, E = gcn.gen_rmat(1 << 10, 8, 5)
+    path = str(tmp_path / "g.mtx")
+    gcn.mtx_write(path, N, V, E)
+    N2, V2, E2 = gcn.mtx_read(path)
+    assert N2 == N and np.array_equal(V, V2) and np.array_equal(E, E2)
+
+
+def test_generators_deterministic_and_simple():
+    a = gcn.gen_er(3000, 20000, 5)
+    b = gcn.gen_er(3000, 20000, 5)
+    assert np.array_equal(a[1], b[1]) and np.array_equal(a[2], b[2])
+    assert a[1][-1] == 40000  # exactly m undirected edges
+    assert is_simple_sorted_symmetric(*a)
+    r = gcn.gen_rmat(1 << 12, 8, 9)
+    assert is_simple_sorted_symmetric(*r)
+    g = gcn.gen_rgg2d(4000, 0.03, 1)
+    assert is_simple_sorted_symmetric(*g)
+    s = gcn.gen_stencil27(5, 4, 3)
+    assert is_simple_sorted_symmetric(*s)
+    # interior vertices of a 27-point stencil have 26 neighbours; M = prod(3n-2) - prod(n)
+    assert s[1][-1] == (13 * 10 * 7) - (5 * 4 * 3)
+
+
+def test_generators_match_golden_graphs(golden):
+    """The committed fixtures were made on these generators: they must not drift."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("mk", os.path.join(os.path.dirname(__file__), "golden",
+                                                                     "make_golden.py"))
+    mk = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mk)
+    for name, (N, V, E) in {**mk.synth_graphs(), **mk.edge_case_graphs()}.items():
+        n2, V2, E2 = golden.graph(name)
+        assert N == n2 and np.array_equal(V, V2) and np.array_equal(E, E2), name
+    for L, seed in mk.SYNTH_MODEL_SEEDS.items():
+        params, md = gcn.synthetic_model(L, seed)
+        gp, gmd = golden.model(L)
+        assert np.array_equal(params, gp) and md == gmd
+
+
+def test_rmat_non_power_of_two_rejects_out_of_range():
+    N, V, E = gcn.gen_rmat(1000, 8, 4)
+    assert N == 1000 and (len(E) == 0 or E.max() < 1000)
+    assert is_simple_sorted_symmetric(N, V, E)
+
+
+def test_model_roundtrip(tmp_path):
+    for L in (2, 3, 4):
+        params, md = gcn.synthetic_model(L, 40 + L)
+        path = str(tmp_path / f"m{L}.gnn")
+        gcn.model_write(path, params, md)
+        p2, md2 = gcn.model_read(path)
+        assert md2 == md and np.array_equal(p2, params)
+
+
+def test_model_format_errors(tmp_path):
+    bad = tmp_path / "bad.gnn"
+    bad.write_text("100 5\n1 2 3\n")  # fewer than 2 layers
+    with pytest.raises(gcn.GCError):
+        gcn.model_read(str(bad))
+    short = tmp_path / "short.gnn"
+    short.write_text("1056 100\n" + " ".join(["0.5"] * 100))
+    with pytest.raises(gcn.GCError):
+        gcn.model_read(str(short))
