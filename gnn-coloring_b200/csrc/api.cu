@@ -100,7 +100,7 @@ void free_graph_buffers(gc_graph *g) {
     }
     void *bufs[] = {g->key,     g->color,    g->P,       g->pc,      g->order,    g->sort_buf, g->sort_hist,
                     g->big,     g->hubs,     g->x,       g->y,       g->t01,      g->deg_rem,  g->frontier,
-                    g->frontier2, g->removed, g->leaf_list};
+                    g->frontier2, g->removed, g->leaf_list, g->vorder, g->rank};
     for (void *p : bufs)
         if (p) cudaFree(p);
 }
@@ -178,6 +178,11 @@ gc_status gc_ctx_create(int device, gc_ctx **out) {
     if (s == GC_OK) s = gc_check_cuda(ctx, cudaMallocHost((void **)&ctx->hstate, sizeof(gc::DevState)), "host state");
     if (s == GC_OK) s = gc_reset_state(ctx);
     if (const char *lim = getenv("GC_SPIN_LIMIT")) ctx->spin_limit = (unsigned int)strtoul(lim, nullptr, 10);
+    // tuning of the coloring kernel's polling (defaults measured on B200)
+    if (const char *e = getenv("GC_JP_CTAS_PER_SM")) ctx->jp_ctas_per_sm = atoi(e);
+    if (const char *e = getenv("GC_JP_TIGHT")) ctx->jp_tight = (unsigned int)strtoul(e, nullptr, 10);
+    if (const char *e = getenv("GC_JP_NAP")) ctx->jp_nap = (unsigned int)strtoul(e, nullptr, 10);
+    if (const char *e = getenv("GC_GNN_SERIAL")) ctx->gnn_serial = atoi(e) != 0;
     if (s != GC_OK) {
         gc_ctx_destroy(ctx);
         return s;

@@ -24,6 +24,11 @@ struct gc_ctx {
     cudaStream_t side_stream = nullptr;  // GNN hub CTAs run here, overlapping the bulk of a layer
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     int color_blocks_per_sm = 0;         // resident CTAs of the coloring kernel (occupancy query)
+    int jp_ctas_per_sm = 2;              // cap on the above: fewer pollers beat more lookahead (measured)
+    unsigned int jp_tight = 32;          // coloring: unproductive polling rounds before sleeping
+    unsigned int jp_nap = 32;            // coloring: first sleep between polling rounds (ns)
+    int gnn_blocks_per_sm[3] = {0, 0, 0};  // resident CTAs of each GNN layer kernel
+    bool gnn_serial = false;             // run hub CTAs before the bulk instead of beside it
     gc::DevState *dstate = nullptr;      // device status block
     gc::DevState *hstate = nullptr;      // pinned host mirror for read-back
     uint64_t launches = 0;
@@ -46,8 +51,10 @@ struct ProfScope {
     ~ProfScope();
 };
 
-// Vertices with more neighbours than this are handled by a whole CTA in the GNN layers.
-constexpr uint32_t GC_GNN_HUB_DEGREE = 1024;
+// GNN layer tiers by neighbour count: a whole CTA above GC_GNN_HUB_DEGREE, one warp above
+// GC_GNN_WARP_DEGREE, four lanes otherwise.
+constexpr uint32_t GC_GNN_HUB_DEGREE = 16384;
+constexpr uint32_t GC_GNN_WARP_DEGREE = 256;
 // Vertices with more neighbours than this are split across several warps in the JP split pass.
 constexpr uint32_t GC_SPLIT_BIG_DEGREE = 32;
 constexpr uint32_t GC_SPLIT_CHUNK = 2048;
@@ -69,6 +76,7 @@ struct gc_graph {
     uint32_t *pc = nullptr;     // predecessor counts
     uint32_t *order = nullptr;  // vertices by descending key, ascending id on ties: the ticket order
     uint32_t *leaf_list = nullptr;  // leaves too large for one thread
+    uint32_t *rank = nullptr;       // ticket of each ordered vertex (all ones elsewhere)
     uint32_t *sort_buf = nullptr;  // radix sort ping-pong (keys and values), 4 * cap_N words
     uint32_t *sort_hist = nullptr;
     uint32_t sort_hist_cap = 0;
@@ -77,6 +85,9 @@ struct gc_graph {
     uint32_t n_big_tasks = 0;
     uint32_t *hubs = nullptr;        // vertices with deg > GC_GNN_HUB_DEGREE
     uint32_t n_hubs = 0;
+    uint32_t *vorder = nullptr;      // the other vertices by descending degree (GNN schedule)
+    uint32_t n_vorder = 0;
+    uint32_t n_wide = 0;             // leading vorder entries with more than GC_GNN_WARP_DEGREE neighbours
     // GNN scratch (allocated on first use)
     float *x = nullptr, *y = nullptr;
     float2 *t01 = nullptr;
@@ -119,4 +130,8 @@ gc_status gc_priority_gnn(gc_graph *g, const gc_model *m);         // GraphSAGE 
 gc_status gc_jp_color(gc_graph *g);                                // JP by current keys (k_jp.cu)
 gc_status gc_keys_from_colors(gc_graph *g);                        // Culberson step (k_jp.cu)
 gc_status gc_validate_device(gc_graph *g, int *max_color);         // (k_jp.cu)
-gc_status gc_sort_order_bits(gc_graph *g, int key_bits, bool filter, uint32_t *d_count);  // (k_sort.cu)
+// Vertex sorts (k_sort.cu): descending key, ascending id on ties, over the vertices a filter keeps.
+enum { SORT_KEEP_ALL = 0, SORT_KEEP_INNER = 1, SORT_KEEP_DEG_AT_MOST = 2 };
+gc_status gc_sort_vertices(gc_graph *g, const uint32_t *keys, int key_bits, int filter, uint32_t max_deg,
+                           uint32_t *out, uint32_t *d_count);
+gc_status gc_sort_order_bits(gc_graph *g, int key_bits, bool filter, uint32_t *d_count);

@@ -37,66 +37,189 @@ __global__ void k_gnn_table0(const uint32_t *__restrict__ V, uint32_t N, float f
     }
 }
 
-// Dense 32x16 + ReLU for the half-warp's vertex; lane j returns output j.
-// nb / self are this lane's feature values (hidden layers) or the four layer-0 scalars.
+// ---- shared pieces: four lanes per vertex, lane q owns features 4q..4q+3 ---------------------
+
+constexpr unsigned int FULL = 0xffffffffu;
+
+__device__ __forceinline__ float4 add4(float4 s, float4 r) {
+    return make_float4(__fadd_rn(s.x, r.x), __fadd_rn(s.y, r.y), __fadd_rn(s.z, r.z), __fadd_rn(s.w, r.w));
+}
+__device__ __forceinline__ float comp(const float4 &v, int c) { return c == 0 ? v.x : (c == 1 ? v.y : (c == 2 ? v.z : v.w)); }
+__device__ __forceinline__ float relu(float c) { return c > 0.0f ? c : 0.0f; }
+
+// Dense 32x16 + ReLU for the quad's vertex.  Input feature i is a_i; lane q returns outputs
+// 4q..4q+3.  For hidden/output layers a_i (i < 16: neighbour mean, else own row) is held by quad
+// lane (i & 15) >> 2 as component i & 3, and is broadcast with a shuffle; for the input layer the
+// four scalars are already in every lane.  Each output accumulates i = 0..31 in order with FMA.
 template <int MODE>
-__device__ __forceinline__ float dense_relu(const float (&w)[32], float bias, float nb, float self, float s0,
-                                            float s1, float self0, float self1, unsigned int hmask) {
-    float c = bias;
+__device__ __forceinline__ float4 dense_quad(const float4 *__restrict__ W4, float4 b4, int q, int qbase,
+                                             unsigned int mask, float4 nb, float4 self, float s0, float s1,
+                                             float self0, float self1) {
+    float c0 = b4.x, c1 = b4.y, c2 = b4.z, c3 = b4.w;
 #pragma unroll
     for (int i = 0; i < 32; i++) {
         float a;
         if (MODE == MODE_INPUT) {
             a = i < 8 ? s0 : (i < 16 ? s1 : (i < 24 ? self0 : self1));
         } else {
-            a = __shfl_sync(hmask, i < 16 ? nb : self, i & 15, 16);
+            const float mine = comp(i < 16 ? nb : self, i & 3);
+            a = __shfl_sync(mask, mine, qbase + ((i & 15) >> 2));
         }
-        c = __fmaf_rn(w[i], a, c);
+        const float4 w = W4[i * 4 + q];
+        c0 = __fmaf_rn(w.x, a, c0);
+        c1 = __fmaf_rn(w.y, a, c1);
+        c2 = __fmaf_rn(w.z, a, c2);
+        c3 = __fmaf_rn(w.w, a, c3);
     }
-    return c > 0.0f ? c : 0.0f;
+    return make_float4(relu(c0), relu(c1), relu(c2), relu(c3));
 }
 
-// Fixed-tree sum of the 16 outputs held by lanes 0..15 of a half-warp; valid in lane 0.
-__device__ __forceinline__ float output_tree(float o, unsigned int hmask) {
-    float t = __fadd_rn(o, __shfl_down_sync(hmask, o, 8, 16));   // t_k = o_k + o_{k+8}, lanes 0..7
-    float q = __fadd_rn(t, __shfl_down_sync(hmask, t, 1, 16));   // t0+t1, t2+t3, t4+t5, t6+t7
-    float r = __fadd_rn(q, __shfl_down_sync(hmask, q, 2, 16));   // (t0+t1)+(t2+t3), (t4+t5)+(t6+t7)
-    return __fadd_rn(r, __shfl_down_sync(hmask, r, 4, 16));      // lane 0: the whole sum
+// The reference's output sum (dense_kernel_output :223-242) over the quad's 16 outputs:
+// t_k = o_k + o_{k+8}, then ((t0+t1)+(t2+t3)) + ((t4+t5)+(t6+t7)).  Valid in quad lane 0.
+__device__ __forceinline__ float output_sum(float4 o, unsigned int mask) {
+    const float p0 = __shfl_down_sync(mask, o.x, 2, 4), p1 = __shfl_down_sync(mask, o.y, 2, 4);
+    const float p2 = __shfl_down_sync(mask, o.z, 2, 4), p3 = __shfl_down_sync(mask, o.w, 2, 4);
+    // lanes 0 and 1 of the quad now hold t_{4q..4q+3}
+    const float t0 = __fadd_rn(o.x, p0), t1 = __fadd_rn(o.y, p1), t2 = __fadd_rn(o.z, p2), t3 = __fadd_rn(o.w, p3);
+    const float h = __fadd_rn(__fadd_rn(t0, t1), __fadd_rn(t2, t3));
+    return __fadd_rn(h, __shfl_down_sync(mask, h, 1, 4));
 }
 
+// ---- regular vertices: 8 per warp, taken from the degree order --------------------------------
+
+constexpr int GNN_THREADS = 256;
+
+// Warp tier: one vertex of up to GC_GNN_HUB_DEGREE neighbours per warp.  All 32 lanes fetch 32
+// neighbour rows per step (one id each, then one float4 per lane for 8 rows at a time), stage
+// them in the warp's shared-memory slab, and lanes 0..15 add them in CSR order, one feature each.
 template <int MODE>
-__global__ void __launch_bounds__(256) k_gnn_layer(const uint32_t *__restrict__ V, const uint32_t *__restrict__ E,
-                                                   uint32_t N, const float2 *__restrict__ t01,
-                                                   const float *__restrict__ x, float *__restrict__ y,
-                                                   uint32_t *__restrict__ key, const float *__restrict__ Wb,
-                                                   uint32_t hub_deg) {
-    __shared__ float sW[LAYER_PARAMS];
+__device__ __forceinline__ void warp_vertex(uint32_t u, const uint32_t *__restrict__ V, const uint32_t *__restrict__ E,
+                                            const float2 *__restrict__ t01, const float *__restrict__ x, float *__restrict__ y,
+                                            uint32_t *__restrict__ key, const float4 *W4, const float *sW, float *slab,
+                                            int lane) {
+    const uint32_t beg = V[u], d = V[u + 1] - beg;
+    const float fd = __uint2float_rn(d);
+    const int q = lane & 3;
+    const float4 zero4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    float s = 0.0f, s1 = 0.0f;  // lane l < 16: feature l (input layer: lane 0 sums deg/md, lane 1 id/N)
+    for (uint32_t c = 0; c < d; c += 32) {
+        const uint32_t e = c + lane < d ? ld_stream(E + beg + c + lane) : 0u;
+        if (MODE == MODE_INPUT) {
+            const float2 t = c + lane < d ? t01[e] : make_float2(0.0f, 0.0f);
+            reinterpret_cast<float2 *>(slab)[lane] = t;
+            __syncwarp();
+            const uint32_t cnt = min(32u, d - c);
+            if (lane < 2)
+                for (uint32_t m = 0; m < cnt; m++) s = __fadd_rn(s, slab[2 * m + lane]);
+        } else {
+            const float4 *X4 = reinterpret_cast<const float4 *>(x);
+            float4 r[4];
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const int m = j * 8 + (lane >> 2);  // this lane fetches features 4q..4q+3 of row m
+                const uint32_t v = __shfl_sync(FULL, e, m);
+                r[j] = c + m < d ? X4[(size_t)v * 4 + q] : zero4;
+            }
+#pragma unroll
+            for (int j = 0; j < 4; j++) reinterpret_cast<float4 *>(slab)[(j * 8 + (lane >> 2)) * 4 + q] = r[j];
+            __syncwarp();
+            const uint32_t cnt = min(32u, d - c);
+            if (lane < FEAT) {
+                float t[8];
+                uint32_t m = 0;
+                for (; m + 8 <= cnt; m += 8) {
+#pragma unroll
+                    for (int k = 0; k < 8; k++) t[k] = slab[(m + k) * FEAT + lane];
+#pragma unroll
+                    for (int k = 0; k < 8; k++) s = __fadd_rn(s, t[k]);
+                }
+                for (; m < cnt; m++) s = __fadd_rn(s, slab[m * FEAT + lane]);
+            }
+        }
+        __syncwarp();
+    }
+    (void)s1;
+    // gather the 16 feature sums into float4s for the quad that runs the dense part (lanes 0..3)
+    float4 nb;
+    nb.x = __shfl_sync(FULL, s, 4 * q + 0);
+    nb.y = __shfl_sync(FULL, s, 4 * q + 1);
+    nb.z = __shfl_sync(FULL, s, 4 * q + 2);
+    nb.w = __shfl_sync(FULL, s, 4 * q + 3);
+    const float in0 = __shfl_sync(FULL, s, 0), in1 = __shfl_sync(FULL, s, 1);
+    if (lane >= 4) return;
+    const unsigned int mask = 0xfu;
+    const float4 b4 = reinterpret_cast<const float4 *>(sW + 2 * FEAT * FEAT)[q];
+    float4 out;
+    if (MODE == MODE_INPUT) {
+        float s0 = in0, sid = in1;
+        if (fd > 0.0f) {
+            s0 = __fdiv_rn(s0, fd);
+            sid = __fdiv_rn(sid, fd);
+        }
+        const float2 self = t01[u];
+        out = dense_quad<MODE_INPUT>(W4, b4, q, 0, mask, zero4, zero4, s0, sid, self.x, self.y);
+    } else {
+        if (fd > 0.0f) nb = make_float4(__fdiv_rn(nb.x, fd), __fdiv_rn(nb.y, fd), __fdiv_rn(nb.z, fd), __fdiv_rn(nb.w, fd));
+        const float4 self = reinterpret_cast<const float4 *>(x)[(size_t)u * 4 + q];
+        out = dense_quad<MODE>(W4, b4, q, 0, mask, nb, self, 0.0f, 0.0f, 0.0f, 0.0f);
+    }
+    if (MODE == MODE_OUTPUT) {
+        const float sum = output_sum(out, mask);
+        if (q == 0) key[u] = __float_as_uint(sum);
+    } else {
+        reinterpret_cast<float4 *>(y)[(size_t)u * 4 + q] = out;
+    }
+}
+
+// Degree order split in two tiers: the first n_wide vertices (more than GC_GNN_WARP_DEGREE
+// neighbours) one per warp, the rest eight per warp (four lanes each).  Work items are handed out
+// by warp index, heaviest first.
+template <int MODE>
+__global__ void __launch_bounds__(GNN_THREADS, 4) k_gnn_layer(const uint32_t *__restrict__ V, const uint32_t *__restrict__ E,
+                                                              const uint32_t *__restrict__ vorder, uint32_t n_wide,
+                                                              uint32_t n_vorder, const float2 *__restrict__ t01,
+                                                              const float *__restrict__ x, float *__restrict__ y,
+                                                              uint32_t *__restrict__ key, const float *__restrict__ Wb) {
+    __shared__ __align__(16) float sW[LAYER_PARAMS];
+    __shared__ __align__(16) float slabs[GNN_THREADS / 32][32 * FEAT];
     for (int i = threadIdx.x; i < LAYER_PARAMS; i += blockDim.x) sW[i] = Wb[i];
     __syncthreads();
-    const int lane = threadIdx.x & 15;
-    const unsigned int hmask = 0xffffu << (threadIdx.x & 16);
-    float w[32];
-#pragma unroll
-    for (int i = 0; i < 32; i++) w[i] = sW[i * FEAT + lane];
-    const float bias = sW[2 * FEAT * FEAT + lane];
+    const int lane = threadIdx.x & 31, q = lane & 3, qbase = lane & ~3;
+    const float4 *W4 = reinterpret_cast<const float4 *>(sW);
+    const float4 b4 = reinterpret_cast<const float4 *>(sW + 2 * FEAT * FEAT)[q];
+    const float4 *X4 = reinterpret_cast<const float4 *>(x);
+    float4 *Y4 = reinterpret_cast<float4 *>(y);
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    const float4 zero4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    float *slab = slabs[threadIdx.x >> 5];
+    const uint32_t n_items = n_wide + (n_vorder - n_wide + 7) / 8;
 
-    const uint32_t groups = (gridDim.x * blockDim.x) >> 4;
-    for (uint32_t u = (blockIdx.x * blockDim.x + threadIdx.x) >> 4; u < N; u += groups) {
-        const uint32_t beg = V[u], end = V[u + 1], d = end - beg;
-        if (d > hub_deg) continue;  // hub CTAs own this vertex
+    for (uint32_t it = warp; it < n_items; it += nwarps) {
+        if (it < n_wide) {
+            warp_vertex<MODE>(vorder[it], V, E, t01, x, y, key, W4, sW, slab, lane);
+            __syncwarp();
+            continue;
+        }
+        const uint32_t g0 = n_wide + (it - n_wide) * 8;
+        const uint32_t slot = g0 + (lane >> 2);
+        const bool valid = slot < n_vorder;
+        const uint32_t u = valid ? vorder[slot] : 0u;
+        const uint32_t beg = valid ? V[u] : 0u;
+        const uint32_t d = valid ? V[u + 1] - beg : 0u;
+        const uint32_t dmax = __reduce_max_sync(FULL, d);  // loop bounds stay warp-uniform
         const float fd = __uint2float_rn(d);
-        float out;
+        float4 out;
         if (MODE == MODE_INPUT) {
             float s0 = 0.0f, s1 = 0.0f;
-            for (uint32_t b = beg; b < end; b += 16) {
-                const uint32_t cnt = min(16u, end - b);
+            for (uint32_t c = 0; c < dmax; c += 4) {
                 float2 t = make_float2(0.0f, 0.0f);
-                if ((uint32_t)lane < cnt) t = t01[ld_stream(E + b + lane)];
+                if (c + q < d) t = t01[ld_stream(E + beg + c + q)];
 #pragma unroll
-                for (uint32_t k = 0; k < 16; k++) {
-                    float a0 = __shfl_sync(hmask, t.x, k, 16);
-                    float a1 = __shfl_sync(hmask, t.y, k, 16);
-                    if (k < cnt) {
+                for (int k = 0; k < 4; k++) {
+                    const float a0 = __shfl_sync(FULL, t.x, qbase + k);
+                    const float a1 = __shfl_sync(FULL, t.y, qbase + k);
+                    if (c + k < d) {
                         s0 = __fadd_rn(s0, a0);
                         s1 = __fadd_rn(s1, a1);
                     }
@@ -106,49 +229,51 @@ __global__ void __launch_bounds__(256) k_gnn_layer(const uint32_t *__restrict__ 
                 s0 = __fdiv_rn(s0, fd);
                 s1 = __fdiv_rn(s1, fd);
             }
-            const float2 self = t01[u];
-            out = dense_relu<MODE_INPUT>(w, bias, 0.0f, 0.0f, s0, s1, self.x, self.y, hmask);
+            const float2 self = valid ? t01[u] : make_float2(0.0f, 0.0f);
+            out = dense_quad<MODE_INPUT>(W4, b4, q, qbase, FULL, zero4, zero4, s0, s1, self.x, self.y);
         } else {
-            float s = 0.0f;
-            for (uint32_t b = beg; b < end; b += 16) {
-                const uint32_t cnt = min(16u, end - b);
-                uint32_t e = (uint32_t)lane < cnt ? ld_stream(E + b + lane) : 0u;
-                float vals[16];
+            float4 s = zero4;
+            for (uint32_t c = 0; c < dmax; c += 8) {
+                // two groups of four neighbours in flight per quad
+                const uint32_t e0 = c + q < d ? ld_stream(E + beg + c + q) : 0u;
+                const uint32_t e1 = c + 4 + q < d ? ld_stream(E + beg + c + 4 + q) : 0u;
+                float4 r[8];
 #pragma unroll
-                for (uint32_t k = 0; k < 16; k++) {
-                    uint32_t v = __shfl_sync(hmask, e, k, 16);
-                    vals[k] = k < cnt ? x[(size_t)v * FEAT + lane] : 0.0f;
+                for (int k = 0; k < 8; k++) {
+                    const uint32_t v = __shfl_sync(FULL, k < 4 ? e0 : e1, qbase + (k & 3));
+                    r[k] = c + k < d ? X4[(size_t)v * 4 + q] : zero4;
                 }
 #pragma unroll
-                for (uint32_t k = 0; k < 16; k++)
-                    if (k < cnt) s = __fadd_rn(s, vals[k]);
+                for (int k = 0; k < 8; k++)
+                    if (c + k < d) s = add4(s, r[k]);
             }
-            if (fd > 0.0f) s = __fdiv_rn(s, fd);
-            const float self = x[(size_t)u * FEAT + lane];
-            out = dense_relu<MODE>(w, bias, s, self, 0.0f, 0.0f, 0.0f, 0.0f, hmask);
+            if (fd > 0.0f) s = make_float4(__fdiv_rn(s.x, fd), __fdiv_rn(s.y, fd), __fdiv_rn(s.z, fd), __fdiv_rn(s.w, fd));
+            const float4 self = valid ? X4[(size_t)u * 4 + q] : zero4;
+            out = dense_quad<MODE>(W4, b4, q, qbase, FULL, s, self, 0.0f, 0.0f, 0.0f, 0.0f);
         }
         if (MODE == MODE_OUTPUT) {
-            float sum = output_tree(out, hmask);
-            if (lane == 0) key[u] = __float_as_uint(sum);
-        } else {
-            y[(size_t)u * FEAT + lane] = out;
+            const float sum = output_sum(out, FULL);
+            if (valid && q == 0) key[u] = __float_as_uint(sum);
+        } else if (valid) {
+            Y4[(size_t)u * 4 + q] = out;
         }
     }
 }
 
 // ---- hub vertices: one CTA each --------------------------------------------------------------
 
-constexpr int HUB_THREADS = 256;
-constexpr int HUB_ROWS = 256;  // neighbour rows per pipeline stage
-constexpr int HUB_STAGES = 4;
+constexpr int HUB_THREADS = 128;  // one neighbour row per thread per stage
+constexpr int HUB_ROWS = HUB_THREADS;
+constexpr int HUB_STAGES = 8;      // rows in flight: 7 stages ahead of the adder
+constexpr int HUB_ID_AHEAD = 4;    // neighbour ids are loaded this many stages before their rows
 
 __device__ __forceinline__ void cp_async_16(void *smem, const void *gmem) {
-    unsigned int s = (unsigned int)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
+    unsigned int sa = (unsigned int)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(gmem) : "memory");
 }
 __device__ __forceinline__ void cp_async_8(void *smem, const void *gmem) {
-    unsigned int s = (unsigned int)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(s), "l"(gmem) : "memory");
+    unsigned int sa = (unsigned int)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(sa), "l"(gmem) : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int N>
@@ -156,90 +281,133 @@ __device__ __forceinline__ void cp_async_wait() {
     asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
+// All threads stream the hub's neighbour rows into a shared-memory ring (cp.async, HUB_STAGES
+// deep; the neighbour ids themselves are read HUB_ID_AHEAD stages earlier), and the first four
+// lanes of warp 0 add the rows in CSR order, four features per lane, with the next eight rows'
+// shared-memory loads in flight, so the chain runs at the FP32 add latency.
 template <int MODE>
 __global__ void __launch_bounds__(HUB_THREADS) k_gnn_hub(const uint32_t *__restrict__ V, const uint32_t *__restrict__ E,
-                                                         uint32_t N, const uint32_t *__restrict__ hubs,
+                                                         const uint32_t *__restrict__ hubs,
                                                          const float2 *__restrict__ t01, const float *__restrict__ x,
                                                          float *__restrict__ y, uint32_t *__restrict__ key,
                                                          const float *__restrict__ Wb) {
-    // stage buffers: hidden rows are 16 floats, input rows 2 floats (deg/md, id/N)
-    constexpr int ROW = (MODE == MODE_INPUT) ? 2 : FEAT;
-    extern __shared__ __align__(16) float smem[];
-    float *stage = smem;  // HUB_STAGES * HUB_ROWS * ROW floats
+    constexpr int ROW = (MODE == MODE_INPUT) ? 2 : FEAT;  // floats per staged row
+    extern __shared__ __align__(16) float stage[];         // HUB_STAGES * HUB_ROWS * ROW floats
+    __shared__ __align__(16) float sW[LAYER_PARAMS];
+    for (int i = threadIdx.x; i < LAYER_PARAMS; i += blockDim.x) sW[i] = Wb[i];
     const uint32_t u = hubs[blockIdx.x];
     const uint32_t beg = V[u], end = V[u + 1], d = end - beg;
     const uint32_t nchunks = (d + HUB_ROWS - 1) / HUB_ROWS;
     const int tid = threadIdx.x;
 
-    auto issue = [&](uint32_t c) {
-        if (c < nchunks) {
-            uint32_t i = beg + c * HUB_ROWS + tid;
-            float *dst = stage + (size_t)(c % HUB_STAGES) * HUB_ROWS * ROW + (size_t)tid * ROW;
-            if (i < end) {
-                uint32_t v = ld_stream(E + i);
-                if (MODE == MODE_INPUT) {
-                    cp_async_8(dst, t01 + v);
-                } else {
-                    const float *src = x + (size_t)v * FEAT;
+    auto load_id = [&](uint32_t c) -> uint32_t {
+        const uint32_t i = beg + c * HUB_ROWS + tid;
+        return (c < nchunks && i < end) ? ld_stream(E + i) : 0xffffffffu;
+    };
+    auto issue = [&](uint32_t c, uint32_t v) {
+        if (v != 0xffffffffu) {
+            float *dst = stage + ((size_t)(c % HUB_STAGES) * HUB_ROWS + tid) * ROW;
+            if (MODE == MODE_INPUT) {
+                cp_async_8(dst, t01 + v);
+            } else {
+                const float *src = x + (size_t)v * FEAT;
 #pragma unroll
-                    for (int q = 0; q < 4; q++) cp_async_16(dst + 4 * q, src + 4 * q);
-                }
+                for (int k = 0; k < 4; k++) cp_async_16(dst + 4 * k, src + 4 * k);
             }
         }
         cp_async_commit();  // empty groups keep the group count uniform
     };
 
-    for (int c = 0; c < HUB_STAGES - 1; c++) issue(c);
-    float s = 0.0f, s1 = 0.0f;  // feature chain (lane), and the second layer-0 chain
-    const int lane = tid & 31;
+    // ids of the stages to be issued next, oldest first
+    uint32_t id0, id1, id2, id3;
+    for (int c = 0; c < HUB_STAGES - 1; c++) issue(c, load_id(c));
+    id0 = load_id(HUB_STAGES - 1);
+    id1 = load_id(HUB_STAGES);
+    id2 = load_id(HUB_STAGES + 1);
+    id3 = load_id(HUB_STAGES + 2);
+    static_assert(HUB_ID_AHEAD == 4, "the id ring below holds four stages");
+
+    const int q = tid & 3;
+    float4 s = make_float4(0.0f, 0.0f, 0.0f, 0.0f);  // hidden: features 4q..4q+3; input: (deg, id) in .x/.y
     for (uint32_t c = 0; c < nchunks; c++) {
-        issue(c + HUB_STAGES - 1);
+        issue(c + HUB_STAGES - 1, id0);
+        id0 = id1;
+        id1 = id2;
+        id2 = id3;
+        id3 = load_id(c + HUB_STAGES - 1 + HUB_ID_AHEAD);
         cp_async_wait<HUB_STAGES - 1>();
         __syncthreads();
-        if (tid < 16) {
+        if (tid < 4) {
             const float *buf = stage + (size_t)(c % HUB_STAGES) * HUB_ROWS * ROW;
             const uint32_t cnt = min((uint32_t)HUB_ROWS, end - (beg + c * HUB_ROWS));
             if (MODE == MODE_INPUT) {
-                // lane 0 sums deg/md, lane 1 sums id/N
-                if (lane < 2)
-                    for (uint32_t r = 0; r < cnt; r++) s = __fadd_rn(s, buf[2 * r + lane]);
+                const float2 *b2 = reinterpret_cast<const float2 *>(buf);
+                uint32_t r = 0;
+                for (; r + 8 <= cnt; r += 8) {
+                    float2 t[8];
+#pragma unroll
+                    for (int k = 0; k < 8; k++) t[k] = b2[r + k];
+#pragma unroll
+                    for (int k = 0; k < 8; k++) {
+                        s.x = __fadd_rn(s.x, t[k].x);
+                        s.y = __fadd_rn(s.y, t[k].y);
+                    }
+                }
+                for (; r < cnt; r++) {
+                    const float2 t = b2[r];
+                    s.x = __fadd_rn(s.x, t.x);
+                    s.y = __fadd_rn(s.y, t.y);
+                }
             } else {
-                for (uint32_t r = 0; r < cnt; r++) s = __fadd_rn(s, buf[r * FEAT + lane]);
+                const float4 *b4 = reinterpret_cast<const float4 *>(buf);
+                uint32_t r = 0;
+                if (cnt >= 8) {
+                    float4 t[8];
+#pragma unroll
+                    for (int k = 0; k < 8; k++) t[k] = b4[k * 4 + q];
+                    for (r = 8; r + 8 <= cnt; r += 8) {
+                        float4 nx[8];
+#pragma unroll
+                        for (int k = 0; k < 8; k++) nx[k] = b4[(r + k) * 4 + q];
+#pragma unroll
+                        for (int k = 0; k < 8; k++) s = add4(s, t[k]);
+#pragma unroll
+                        for (int k = 0; k < 8; k++) t[k] = nx[k];
+                    }
+#pragma unroll
+                    for (int k = 0; k < 8; k++) s = add4(s, t[k]);
+                }
+                for (; r < cnt; r++) s = add4(s, b4[r * 4 + q]);
             }
         }
         __syncthreads();
     }
     cp_async_wait<0>();
-    if (tid >= 16) return;
-    (void)s1;
-    const unsigned int hmask = 0xffffu;
-    __shared__ float sW[LAYER_PARAMS];
-    for (int i = tid; i < LAYER_PARAMS; i += 16) sW[i] = Wb[i];
-    __syncwarp(hmask);
-    float w[32];
-#pragma unroll
-    for (int i = 0; i < 32; i++) w[i] = sW[i * FEAT + lane];
-    const float bias = sW[2 * FEAT * FEAT + lane];
+    if (tid >= 4) return;
+    const unsigned int mask = 0xfu;
+    const float4 *W4 = reinterpret_cast<const float4 *>(sW);
+    const float4 b4 = reinterpret_cast<const float4 *>(sW + 2 * FEAT * FEAT)[q];
     const float fd = __uint2float_rn(d);
-    float out;
+    const float4 zero4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    float4 out;
     if (MODE == MODE_INPUT) {
-        float s0 = __shfl_sync(hmask, s, 0, 16), sid = __shfl_sync(hmask, s, 1, 16);
+        float s0 = s.x, s1 = s.y;  // every lane of the quad ran the same two chains
         if (fd > 0.0f) {
             s0 = __fdiv_rn(s0, fd);
-            sid = __fdiv_rn(sid, fd);
+            s1 = __fdiv_rn(s1, fd);
         }
         const float2 self = t01[u];
-        out = dense_relu<MODE_INPUT>(w, bias, 0.0f, 0.0f, s0, sid, self.x, self.y, hmask);
+        out = dense_quad<MODE_INPUT>(W4, b4, q, 0, mask, zero4, zero4, s0, s1, self.x, self.y);
     } else {
-        if (fd > 0.0f) s = __fdiv_rn(s, fd);
-        const float self = x[(size_t)u * FEAT + lane];
-        out = dense_relu<MODE>(w, bias, s, self, 0.0f, 0.0f, 0.0f, 0.0f, hmask);
+        if (fd > 0.0f) s = make_float4(__fdiv_rn(s.x, fd), __fdiv_rn(s.y, fd), __fdiv_rn(s.z, fd), __fdiv_rn(s.w, fd));
+        const float4 self = reinterpret_cast<const float4 *>(x)[(size_t)u * 4 + q];
+        out = dense_quad<MODE>(W4, b4, q, 0, mask, s, self, 0.0f, 0.0f, 0.0f, 0.0f);
     }
     if (MODE == MODE_OUTPUT) {
-        float sum = output_tree(out, hmask);
-        if (lane == 0) key[u] = __float_as_uint(sum);
+        const float sum = output_sum(out, mask);
+        if (q == 0) key[u] = __float_as_uint(sum);
     } else {
-        y[(size_t)u * FEAT + lane] = out;
+        reinterpret_cast<float4 *>(y)[(size_t)u * 4 + q] = out;
     }
 }
 
@@ -254,19 +422,28 @@ gc_status launch_layer(gc_graph *g, const float *Wb, const float *x, float *y, c
         if ((s = gc_check_cuda(ctx, cudaFuncSetAttribute(k_gnn_hub<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                          (int)smem), "hub smem")) != GC_OK)
             return s;
+        if (ctx->gnn_serial) side = ctx->stream;  // hubs first, then the bulk, on one stream
         if ((s = gc_check_cuda(ctx, cudaEventRecord(fork, ctx->stream), "fork")) != GC_OK) return s;
         if ((s = gc_check_cuda(ctx, cudaStreamWaitEvent(side, fork, 0), "fork")) != GC_OK) return s;
         ProfScope ps(ctx, MODE == MODE_INPUT ? "gnn_hub_input" : (MODE == MODE_HIDDEN ? "gnn_hub_hidden" : "gnn_hub_output"),
                      side);
-        k_gnn_hub<MODE><<<g->n_hubs, HUB_THREADS, smem, side>>>(g->V, g->E, g->N, g->hubs, g->t01, x, y, g->key, Wb);
+        k_gnn_hub<MODE><<<g->n_hubs, HUB_THREADS, smem, side>>>(g->V, g->E, g->hubs, g->t01, x, y, g->key, Wb);
         ctx->launches++;
         if ((s = gc_check_launch(ctx, "gnn hub layer")) != GC_OK) return s;
     }
-    int grid = ctx->num_sms * 8;
-    {
+    int &blocks = ctx->gnn_blocks_per_sm[MODE];
+    if (!blocks) {
+        if ((s = gc_check_cuda(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_gnn_layer<MODE>,
+                                                                                  GNN_THREADS, 0),
+                               "occupancy")) != GC_OK)
+            return s;
+        if (blocks < 1) blocks = 1;
+    }
+    if (g->n_vorder) {
         ProfScope ps(ctx, MODE == MODE_INPUT ? "gnn_input" : (MODE == MODE_HIDDEN ? "gnn_hidden" : "gnn_output"),
                      ctx->stream);
-        k_gnn_layer<MODE><<<grid, 256, 0, ctx->stream>>>(g->V, g->E, g->N, g->t01, x, y, g->key, Wb, GC_GNN_HUB_DEGREE);
+        k_gnn_layer<MODE><<<ctx->num_sms * blocks, GNN_THREADS, 0, ctx->stream>>>(
+            g->V, g->E, g->vorder, g->n_wide, g->n_vorder, g->t01, x, y, g->key, Wb);
     }
     ctx->launches++;
     if ((s = gc_check_launch(ctx, "gnn layer")) != GC_OK) return s;
@@ -289,7 +466,11 @@ gc_status gc_priority_gnn(gc_graph *g, const gc_model *m) {
     if ((s = gc_alloc(ctx, &g->y, rows * FEAT, "gnn features")) != GC_OK) return s;
     if ((s = gc_alloc(ctx, &g->t01, rows, "gnn input table")) != GC_OK) return s;
     if (ctx->side_stream == nullptr) {
-        if ((s = gc_check_cuda(ctx, cudaStreamCreateWithFlags(&ctx->side_stream, cudaStreamNonBlocking), "stream")) != GC_OK)
+        int lo = 0, hi = 0;
+        cudaDeviceGetStreamPriorityRange(&lo, &hi);
+        // hub CTAs carry the longest FP32 chains: schedule them ahead of the bulk
+        if ((s = gc_check_cuda(ctx, cudaStreamCreateWithPriority(&ctx->side_stream, cudaStreamNonBlocking, hi),
+                               "stream")) != GC_OK)
             return s;
         if ((s = gc_check_cuda(ctx, cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming), "event")) != GC_OK)
             return s;

@@ -36,8 +36,24 @@ __global__ void k_degree_classes(const uint32_t *__restrict__ V, uint32_t N, uin
         if (d > hub_deg) {
             uint32_t at = atomicAdd(&st->count2, 1u);
             if (hubs && at < hub_cap) hubs[at] = u;
+        } else if (d > GC_GNN_WARP_DEGREE) {
+            atomicAdd(&st->min_deg, 1u);  // counts the GNN warp tier
         }
     }
+}
+
+__global__ void k_degree_keys(const uint32_t *__restrict__ V, uint32_t N, uint32_t *__restrict__ out) {
+    for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < N; u += gridDim.x * blockDim.x)
+        out[u] = V[u + 1] - V[u];
+}
+
+int bits_of(uint32_t x) {
+    int b = 0;
+    while (x) {
+        b++;
+        x >>= 1;
+    }
+    return b;
 }
 
 __global__ void k_hub_degrees(const uint32_t *__restrict__ V, const uint32_t *__restrict__ hubs, uint32_t n,
@@ -58,6 +74,7 @@ gc_status gc_graph_prepare(gc_graph *g) {
         g->max_deg = 0;
         g->n_big_tasks = 0;
         g->n_hubs = 0;
+        g->n_vorder = 0;
         return GC_OK;
     }
     int grid = ctx->num_sms * 8;
@@ -70,6 +87,7 @@ gc_status gc_graph_prepare(gc_graph *g) {
     if ((s = gc_read_state(ctx)) != GC_OK) return s;
     g->max_deg = ctx->hstate->max_color;
     uint32_t n_tasks = ctx->hstate->count, n_hubs = ctx->hstate->count2;
+    g->n_wide = ctx->hstate->min_deg;
     // (re)allocate lists
     if (g->big) cudaFree(g->big);
     if (g->hubs) cudaFree(g->hubs);
@@ -112,5 +130,21 @@ gc_status gc_graph_prepare(gc_graph *g) {
             return s;
         if ((s = gc_check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "hub list")) != GC_OK) return s;
     }
+    // GNN schedule: every non-hub vertex by descending degree (ties by id), so that the vertices a
+    // warp handles together have nearly equal neighbour counts.  The key buffer is free here (no
+    // priorities exist right after an upload).
+    if (g->vorder) cudaFree(g->vorder);
+    g->vorder = nullptr;
+    if ((s = gc_alloc(ctx, &g->vorder, (size_t)g->cap_N, "degree order")) != GC_OK) return s;
+    k_degree_keys<<<ctx->num_sms * 4, 256, 0, ctx->stream>>>(g->V, g->N, g->key);
+    ctx->launches++;
+    if ((s = gc_reset_state(ctx)) != GC_OK) return s;
+    const uint32_t top = g->max_deg < GC_GNN_HUB_DEGREE ? g->max_deg : GC_GNN_HUB_DEGREE;
+    if ((s = gc_sort_vertices(g, g->key, bits_of(top), SORT_KEEP_DEG_AT_MOST, GC_GNN_HUB_DEGREE, g->vorder,
+                              &ctx->dstate->count)) != GC_OK)
+        return s;
+    if ((s = gc_read_state(ctx)) != GC_OK) return s;
+    g->n_vorder = ctx->hstate->count;
+    if (g->n_vorder + g->n_hubs != g->N) return gc_fail(ctx, GC_ERR_DEVICE, "degree order lost vertices");
     return GC_OK;
 }

@@ -88,7 +88,6 @@ constexpr int COLOR_WARPS = COLOR_THREADS / 32;
 constexpr uint32_t WINDOW = 1024;   // colors covered by one pass over the predecessors
 constexpr int TRACK = 64;           // per lane: predecessors whose wait is tracked in a bitmask
 constexpr int LOADS = 4;            // predecessor colors in flight per lane
-constexpr uint32_t CORE_TICKETS = 1u << 16;  // first tickets handed out one at a time
 
 __device__ __forceinline__ void mark(uint32_t *fb, int c, uint32_t window) {
     const uint32_t idx = (uint32_t)(c - 1) - window * WINDOW;
@@ -179,35 +178,117 @@ __device__ int color_one(const uint32_t *__restrict__ list, uint32_t cnt, const 
     }
 }
 
-// The ordered vertices (neither sources nor leaves), one warp each, in ticket order.  Tickets are
-// taken one at a time for the first CORE_TICKETS (the deep, narrow part of the DAG), then in
-// batches of 8 that the warp colors in order.
-__global__ void __launch_bounds__(COLOR_THREADS, 6) k_jp_color(const uint32_t *__restrict__ V, const uint32_t *__restrict__ P,
-                                                            const uint32_t *__restrict__ pc,
-                                                            const uint32_t *__restrict__ order, int *color,
-                                                            DevState *st, unsigned int spin_limit) {
-    __shared__ uint32_t forbid[COLOR_WARPS][32];
+constexpr int COLOR_WARPS_PER_CTA = 8;
+constexpr int PENDING = 128;  // per warp: uncolored predecessors remembered for polling
+
+// Colors one ordered vertex whose predecessors are list[0..cnt): the smallest color >= 1 none of
+// them has.  Every predecessor color is read first without waiting (LOADS per lane in flight);
+// the ids of uncolored ones go to the warp's pending list in shared memory, and only those are
+// re-read (one global load each) until colored: back to back at first, then with growing sleeps.
+// Pending-list overflow (more than PENDING uncolored predecessors) waits in place.  Returns -1
+// when a wait exceeded spin_limit rounds or another warp raised the error flag.
+__device__ int color_one_v(const uint32_t *__restrict__ list, uint32_t cnt, const int *color, uint32_t *fb,
+                           uint32_t *pend, int lane, DevState *st, unsigned int spin_limit, unsigned int tight,
+                           unsigned int nap) {
+    for (uint32_t window = 0;; window++) {
+        fb[lane] = 0;
+        __syncwarp();
+        uint32_t npend = 0;  // warp-uniform
+        bool gave_up = false;
+        for (uint32_t j0 = 0; j0 < cnt; j0 += 32 * LOADS) {
+            uint32_t v[LOADS];
+            int c[LOADS];
+#pragma unroll
+            for (int q = 0; q < LOADS; q++) {
+                const uint32_t j = j0 + q * 32 + lane;
+                v[q] = j < cnt ? list[j] : 0xffffffffu;
+            }
+#pragma unroll
+            for (int q = 0; q < LOADS; q++) c[q] = v[q] != 0xffffffffu ? ld_relaxed(color + v[q]) : -1;
+#pragma unroll
+            for (int q = 0; q < LOADS; q++) {
+                if (c[q] > 0) mark(fb, c[q], window);
+                const unsigned int zero = __ballot_sync(0xffffffffu, c[q] == 0);
+                if (zero) {
+                    const uint32_t slot = npend + __popc(zero & ((1u << lane) - 1u));
+                    if (c[q] == 0) {
+                        if (slot < PENDING) {
+                            pend[slot] = v[q];
+                        } else {  // list full: wait in place
+                            unsigned int spins = 0;
+                            int cc;
+                            while ((cc = ld_relaxed(color + v[q])) == 0) {
+                                if (++spins > spin_limit || ((spins & 255u) == 0 && ld_relaxed_u32(&st->err))) {
+                                    gave_up = true;
+                                    break;
+                                }
+                                __nanosleep(64);
+                            }
+                            if (!gave_up) mark(fb, cc, window);
+                        }
+                    }
+                    npend = min((uint32_t)PENDING, npend + __popc(zero));
+                }
+            }
+        }
+        __syncwarp();
+        // poll the pending list: lane l re-reads entries l, l + 32, ...
+        unsigned int spins = 0;
+        for (;;) {
+            bool left = false, progress = false;
+            for (uint32_t i = lane; i < npend && !gave_up; i += 32) {
+                const uint32_t v = pend[i];
+                if (v == 0xffffffffu) continue;
+                const int cc = ld_relaxed(color + v);
+                if (cc) {
+                    mark(fb, cc, window);
+                    pend[i] = 0xffffffffu;
+                    progress = true;
+                } else {
+                    left = true;
+                }
+            }
+            if (!__any_sync(0xffffffffu, left && !gave_up)) break;
+            if (!__any_sync(0xffffffffu, progress)) {
+                if (++spins > spin_limit || ((spins & 255u) == 0 && ld_relaxed_u32(&st->err))) gave_up = true;
+                else if (spins > tight) __nanosleep(spins > 16 * tight + 64 ? 4 * nap : nap);
+            }
+        }
+        if (__any_sync(0xffffffffu, gave_up)) return -1;
+        __syncwarp();
+        const int m = window_mex(fb, lane, window);
+        __syncwarp();
+        if (m) return m;
+    }
+}
+
+// The ordered vertices (neither sources nor leaves), one warp each, tickets taken one at a time
+// in order.  A warp waits only on vertices with smaller tickets, which are held by running warps
+// or done, so the oldest unfinished ticket always progresses.
+__global__ void __launch_bounds__(COLOR_WARPS_PER_CTA * 32) k_jp_color(const uint32_t *__restrict__ V,
+                                                                       const uint32_t *__restrict__ P,
+                                                                       const uint32_t *__restrict__ pc,
+                                                                       const uint32_t *__restrict__ order, int *color,
+                                                                       DevState *st, unsigned int spin_limit,
+                                                                       unsigned int tight, unsigned int nap) {
+    __shared__ uint32_t forbid[COLOR_WARPS_PER_CTA][32];
+    __shared__ uint32_t pending[COLOR_WARPS_PER_CTA][PENDING];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    uint32_t *fb = forbid[warp];
     const uint32_t n = ld_relaxed_u32(&st->ordered);
     for (;;) {
-        uint32_t t = 0, b = 1;
-        if (lane == 0) {
-            b = ld_relaxed_u32(&st->ticket) < CORE_TICKETS ? 1u : 8u;
-            t = atomicAdd(&st->ticket, b);
-        }
+        uint32_t t = 0;
+        if (lane == 0) t = atomicAdd(&st->ticket, 1u);
         t = __shfl_sync(0xffffffffu, t, 0);
-        b = __shfl_sync(0xffffffffu, b, 0);
         if (t >= n) break;
-        const uint32_t t_end = min(n, t + b);
-        for (; t < t_end; t++) {
-            const uint32_t u = order[t];
-            const int c = color_one(P + V[u], pc[u], color, fb, lane, st, spin_limit);
-            if (c < 0 && lane == 0) raise_error(st, ERR_WAIT_EXPIRED, u);
+        const uint32_t u = order[t];
+        const int c = color_one_v(P + V[u], pc[u], color, forbid[warp], pending[warp], lane, st, spin_limit, tight,
+                                  nap);
+        if (lane == 0) {
+            if (c < 0) raise_error(st, ERR_WAIT_EXPIRED, u);
             // -1 on error is non-zero, so successors stop waiting; the host reports the error
-            if (lane == 0) st_relaxed(color + u, c);
-            __syncwarp();
+            st_relaxed(color + u, c);
         }
+        __syncwarp();
     }
 }
 
@@ -326,25 +407,21 @@ gc_status gc_jp_color(gc_graph *g) {
     if ((s = gc_sort_order_bits(g, bits, true, &ctx->dstate->ordered)) != GC_OK) return s;
 
     // 3. ordered coloring
-    int &blocks_per_sm = ctx->color_blocks_per_sm;
-    if (!blocks_per_sm) {
-        if ((s = gc_check_cuda(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_jp_color,
-                                                                                  COLOR_THREADS, 0),
+    int &blocks = ctx->color_blocks_per_sm;
+    if (!blocks) {
+        if ((s = gc_check_cuda(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_jp_color,
+                                                                                  COLOR_WARPS_PER_CTA * 32, 0),
                                "occupancy")) != GC_OK)
             return s;
-        if (blocks_per_sm < 1) blocks_per_sm = 1;
-        if (const char *e = getenv("GC_JP_BLOCKS_PER_SM")) {
-            int b = atoi(e);
-            if (b >= 1 && b < blocks_per_sm) blocks_per_sm = b;
-        }
+        if (blocks < 1) blocks = 1;
+        if (ctx->jp_ctas_per_sm > 0 && ctx->jp_ctas_per_sm < blocks) blocks = ctx->jp_ctas_per_sm;
     }
     k_reset_ticket<<<1, 1, 0, ctx->stream>>>(ctx->dstate);
     ctx->launches++;
     {
         ProfScope ps(ctx, "jp_color", ctx->stream);
-        k_jp_color<<<ctx->num_sms * blocks_per_sm, COLOR_THREADS, 0, ctx->stream>>>(g->V, g->P, g->pc, g->order,
-                                                                                    g->color, ctx->dstate,
-                                                                                    ctx->spin_limit);
+        k_jp_color<<<ctx->num_sms * blocks, COLOR_WARPS_PER_CTA * 32, 0, ctx->stream>>>(
+            g->V, g->P, g->pc, g->order, g->color, ctx->dstate, ctx->spin_limit, ctx->jp_tight, ctx->jp_nap);
         ctx->launches++;
     }
     // 4. leaves

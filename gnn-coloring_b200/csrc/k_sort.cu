@@ -28,18 +28,21 @@ constexpr int RADIX = 256;
 struct SortIn {
     const uint32_t *kin, *vin;  // previous pass (later passes)
     const uint32_t *key;        // keys by vertex (first pass)
-    const uint32_t *V, *pc;     // filter: keep u when 0 < pc[u] < deg(u)
+    const uint32_t *V, *pc;     // filter inputs
     const uint32_t *d_n;        // element count of later passes
     uint32_t N;
+    uint32_t max_deg;           // SORT_KEEP_DEG_AT_MOST: largest degree kept
     int first, filter;
 };
 
 __device__ __forceinline__ bool sort_elem(const SortIn &in, uint32_t j, uint32_t n, uint32_t &k, uint32_t &v) {
     if (in.first) {
         if (j >= in.N) return false;
-        if (in.filter) {
+        if (in.filter == SORT_KEEP_INNER) {
             const uint32_t p = in.pc[j], d = in.V[j + 1] - in.V[j];
             if (p == 0 || p >= d) return false;
+        } else if (in.filter == SORT_KEEP_DEG_AT_MOST) {
+            if (in.V[j + 1] - in.V[j] > in.max_deg) return false;
         }
         k = in.key[j];
         v = j;
@@ -154,11 +157,11 @@ __global__ void __launch_bounds__(SORT_THREADS) k_sort_scatter(SortIn in, int sh
 
 }  // namespace
 
-// Sorts into g->order.  key_bits: number of low key bits that may be non-zero; 0 means "all keys
-// equal" (a stable compaction by id).  With `filter`, only vertices with 0 < pc < deg take part
-// (the inner vertices of the coloring DAG) and their number is left in *d_count; otherwise
-// *d_count = N.
-gc_status gc_sort_order_bits(gc_graph *g, int key_bits, bool filter, uint32_t *d_count) {
+// Sorts vertex ids by descending key (ascending id on ties) into `out`.  key_bits: number of low
+// key bits that may be non-zero; 0 means "all keys equal" (a stable compaction by id).  `filter`
+// selects which vertices take part (SORT_KEEP_*); their number is left in *d_count.
+gc_status gc_sort_vertices(gc_graph *g, const uint32_t *keys, int key_bits, int filter, uint32_t max_deg,
+                           uint32_t *out, uint32_t *d_count) {
     gc_ctx *ctx = g->ctx;
     gc_status s;
     const uint32_t N = g->N;
@@ -175,19 +178,20 @@ gc_status gc_sort_order_bits(gc_graph *g, int key_bits, bool filter, uint32_t *d
     uint32_t *k0 = g->sort_buf, *v0 = g->sort_buf + g->cap_N;
     uint32_t *k1 = g->sort_buf + 2 * (size_t)g->cap_N, *v1 = g->sort_buf + 3 * (size_t)g->cap_N;
     SortIn in{};
-    in.key = g->key;
+    in.key = keys;
     in.V = g->V;
     in.pc = g->pc;
     in.d_n = d_count;
     in.N = N;
-    in.filter = filter ? 1 : 0;
+    in.max_deg = max_deg;
+    in.filter = filter;
     ProfScope ps(ctx, "sort", ctx->stream);
     for (int p = 0; p < passes; p++) {
         const int shift = 8 * p;
         const uint32_t mask = key_bits <= 0 ? 0u : (uint32_t)(RADIX - 1);
         in.first = (p == 0);
         uint32_t *kout = (p & 1) ? k1 : k0, *vout = (p & 1) ? v1 : v0;
-        if (p == passes - 1) vout = g->order;  // last pass writes the ticket order directly
+        if (p == passes - 1) vout = out;  // last pass writes the result directly
         k_sort_hist<<<ntiles, SORT_THREADS, 0, ctx->stream>>>(in, shift, mask, g->sort_hist, ntiles);
         k_sort_scan<<<1, 1024, 0, ctx->stream>>>(g->sort_hist, RADIX * ntiles, p == 0 ? d_count : nullptr);
         k_sort_scatter<<<ntiles, SORT_THREADS, 0, ctx->stream>>>(in, shift, mask, g->sort_hist, ntiles, kout, vout);
@@ -197,4 +201,8 @@ gc_status gc_sort_order_bits(gc_graph *g, int key_bits, bool filter, uint32_t *d
         in.vin = vout;
     }
     return GC_OK;
+}
+
+gc_status gc_sort_order_bits(gc_graph *g, int key_bits, bool filter, uint32_t *d_count) {
+    return gc_sort_vertices(g, g->key, key_bits, filter ? SORT_KEEP_INNER : SORT_KEEP_ALL, 0, g->order, d_count);
 }
