@@ -139,6 +139,27 @@ gc_status gc_download_colors(gc_ctx *ctx, gc_graph *g, int32_t *color);
  * after Culberson the colors. */
 gc_status gc_download_priority(gc_ctx *ctx, gc_graph *g, double *p);
 
+/* ---- GraphSAGE priorities without device allocation ------------------------------------------- */
+
+/* No counterpart in the reference: an extra entry point of this library.
+ *
+ * The same FP32 GraphSAGE-16 priorities as gc_priority(GC_GNN) -- the reference's fast_gnn.c
+ * arithmetic, bit for bit -- for callers that may not allocate device memory: a serving loop that
+ * reserved its HBM budget up front, a host framework that owns all device memory and passes only
+ * its own buffers, or a latency-critical path that cannot take cudaMalloc's implicit device
+ * synchronisation.  The caller passes the CSR (dV[N+1], dE[dV[N]]), the model (dparam: params
+ * floats, params = L * 528, L >= 2; md its degree normaliser) and the output dp[N] (one float per
+ * vertex), all in device memory, plus a cudaStream_t as void* (NULL: the default stream).  The call
+ * is asynchronous on that stream and allocates nothing: its scratch is a fixed device array in the
+ * library, sized for GC_NOALLOC_MAX_VERTICES vertices, held by every device that loads the library
+ * until the process exits.  Larger graphs return GC_ERR_INVALID (use gc_priority).  All calls
+ * share that array: calls whose kernels overlap on one device (other streams, other host threads)
+ * race.  The first call on a device looks up the array's address with that device current; make
+ * that first call before any stream capture. */
+#define GC_NOALLOC_MAX_VERTICES 65536u
+gc_status gc_gnn_priority_noalloc(uint32_t N, const uint32_t *dV, const uint32_t *dE, int params, int md,
+                                  const float *dparam, float *dp, void *stream);
+
 /* ---- host-side graph preparation (no device involved) --------------------------------------- */
 
 /* Reads a Matrix Market file into a simple, symmetric, sorted CSR with the reference's rules:
