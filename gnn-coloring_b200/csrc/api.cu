@@ -93,6 +93,11 @@ __global__ void k_check_csr(const uint32_t *__restrict__ V, const uint32_t *__re
         if (E[i] >= N) gc::raise_error(st, gc::ERR_BOUND, i);
 }
 
+__global__ void k_keys_to_double(const uint32_t *__restrict__ key, uint32_t N, int float_bits, double *__restrict__ p) {
+    for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < N; u += gridDim.x * blockDim.x)
+        p[u] = float_bits ? (double)__uint_as_float(key[u]) : (double)key[u];
+}
+
 void free_graph_buffers(gc_graph *g) {
     if (g->owns_csr) {
         cudaFree(g->V);
@@ -100,7 +105,7 @@ void free_graph_buffers(gc_graph *g) {
     }
     void *bufs[] = {g->key,     g->color,    g->P,       g->pc,      g->order,    g->sort_buf, g->sort_hist,
                     g->big,     g->hubs,     g->x,       g->y,       g->t01,      g->deg_rem,  g->frontier,
-                    g->frontier2, g->removed, g->leaf_list, g->vorder, g->rank};
+                    g->frontier2, g->removed, g->leaf_list, g->vorder, g->rank, g->p64};
     for (void *p : bufs)
         if (p) cudaFree(p);
 }
@@ -582,22 +587,17 @@ gc_status gc_download_priority(gc_ctx *ctx, gc_graph *g, double *p) {
         memcpy(p, g->user_p.data(), sizeof(double) * N);
         return GC_OK;
     }
-    std::vector<uint32_t> k(N);
+    if (N == 0) return GC_OK;
+    // widen on the device, then one copy into the caller's buffer
     gc_status s;
-    if (N && (s = gc_check_cuda(ctx, cudaMemcpyAsync(k.data(), g->key, sizeof(uint32_t) * N, cudaMemcpyDeviceToHost,
-                                                     ctx->stream), "download priorities")) != GC_OK)
+    if ((s = gc_alloc(ctx, &g->p64, (size_t)g->cap_N, "priority staging")) != GC_OK) return s;
+    k_keys_to_double<<<ctx->num_sms * 4, 256, 0, ctx->stream>>>(g->key, N, g->key_kind == GC_GNN ? 1 : 0, g->p64);
+    ctx->launches++;
+    if ((s = gc_check_launch(ctx, "priority widening")) != GC_OK) return s;
+    if ((s = gc_check_cuda(ctx, cudaMemcpyAsync(p, g->p64, sizeof(double) * N, cudaMemcpyDeviceToHost, ctx->stream),
+                           "download priorities")) != GC_OK)
         return s;
-    if ((s = gc_check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "download priorities")) != GC_OK) return s;
-    if (g->key_kind == GC_GNN) {
-        for (uint32_t u = 0; u < N; u++) {
-            float f;
-            memcpy(&f, &k[u], sizeof f);
-            p[u] = (double)f;
-        }
-    } else {
-        for (uint32_t u = 0; u < N; u++) p[u] = (double)k[u];
-    }
-    return GC_OK;
+    return gc_check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "download priorities");
 }
 
 }  // extern "C"

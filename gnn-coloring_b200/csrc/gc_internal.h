@@ -55,9 +55,9 @@ struct ProfScope {
 // GC_GNN_WARP_DEGREE, four lanes otherwise.
 constexpr uint32_t GC_GNN_HUB_DEGREE = 16384;
 constexpr uint32_t GC_GNN_WARP_DEGREE = 256;
-// Vertices with more neighbours than this are split across several warps in the JP split pass.
-constexpr uint32_t GC_SPLIT_BIG_DEGREE = 32;
-constexpr uint32_t GC_SPLIT_CHUNK = 2048;
+// Hubs (more than GC_GNN_HUB_DEGREE neighbours) are split across several warps in the JP split
+// pass, this many edges per warp task.
+constexpr uint32_t GC_SPLIT_CHUNK = 1024;  // edges per warp task (shared-memory buffer per warp)
 
 struct gc_graph {
     gc_ctx *ctx = nullptr;
@@ -81,8 +81,9 @@ struct gc_graph {
     uint32_t *sort_hist = nullptr;
     uint32_t sort_hist_cap = 0;
     // degree classes (depend on the graph only; rebuilt on upload)
-    uint32_t *big = nullptr;         // split tasks: (vertex, first edge) pairs for deg > GC_SPLIT_BIG_DEGREE
+    uint32_t *big = nullptr;         // split tasks of the hubs: (vertex, first edge) pairs
     uint32_t n_big_tasks = 0;
+    size_t big_cap = 0;              // words allocated for `big`
     uint32_t *hubs = nullptr;        // vertices with deg > GC_GNN_HUB_DEGREE
     uint32_t n_hubs = 0;
     uint32_t *vorder = nullptr;      // the other vertices by descending degree (GNN schedule)
@@ -96,6 +97,7 @@ struct gc_graph {
     // stats of the last coloring
     int colors_used = 0;
     std::vector<double> user_p;  // priorities given by gc_priority_set, returned unchanged
+    double *p64 = nullptr;       // device staging for gc_download_priority
 };
 
 struct gc_model {

@@ -80,7 +80,7 @@ gc_status gc_graph_prepare(gc_graph *g) {
     int grid = ctx->num_sms * 8;
     // pass 1: counts
     if ((s = gc_reset_state(ctx)) != GC_OK) return s;
-    k_degree_classes<<<grid, 256, 0, ctx->stream>>>(g->V, g->N, GC_SPLIT_BIG_DEGREE, GC_SPLIT_CHUNK,
+    k_degree_classes<<<grid, 256, 0, ctx->stream>>>(g->V, g->N, GC_GNN_HUB_DEGREE, GC_SPLIT_CHUNK,
                                                     GC_GNN_HUB_DEGREE, ctx->dstate, nullptr, 0, nullptr, 0);
     ctx->launches++;
     if ((s = gc_check_launch(ctx, "degree classes")) != GC_OK) return s;
@@ -88,16 +88,17 @@ gc_status gc_graph_prepare(gc_graph *g) {
     g->max_deg = ctx->hstate->max_color;
     uint32_t n_tasks = ctx->hstate->count, n_hubs = ctx->hstate->count2;
     g->n_wide = ctx->hstate->min_deg;
-    // (re)allocate lists
-    if (g->big) cudaFree(g->big);
-    if (g->hubs) cudaFree(g->hubs);
-    g->big = nullptr;
-    g->hubs = nullptr;
-    if ((s = gc_alloc(ctx, &g->big, 2 * (size_t)n_tasks, "split task list")) != GC_OK) return s;
-    if ((s = gc_alloc(ctx, &g->hubs, (size_t)n_hubs, "hub list")) != GC_OK) return s;
+    // lists: the hub list and the degree order fit in cap_N; the task list grows when needed
+    if (2 * (size_t)n_tasks > g->big_cap) {
+        if (g->big) cudaFree(g->big);
+        g->big = nullptr;
+        if ((s = gc_alloc(ctx, &g->big, 2 * (size_t)n_tasks, "split task list")) != GC_OK) return s;
+        g->big_cap = 2 * (size_t)n_tasks;
+    }
+    if ((s = gc_alloc(ctx, &g->hubs, (size_t)g->cap_N, "hub list")) != GC_OK) return s;
     // pass 2: fill
     if ((s = gc_reset_state(ctx)) != GC_OK) return s;
-    k_degree_classes<<<grid, 256, 0, ctx->stream>>>(g->V, g->N, GC_SPLIT_BIG_DEGREE, GC_SPLIT_CHUNK,
+    k_degree_classes<<<grid, 256, 0, ctx->stream>>>(g->V, g->N, GC_GNN_HUB_DEGREE, GC_SPLIT_CHUNK,
                                                     GC_GNN_HUB_DEGREE, ctx->dstate, g->big, n_tasks,
                                                     g->hubs, n_hubs);
     ctx->launches++;
@@ -133,8 +134,6 @@ gc_status gc_graph_prepare(gc_graph *g) {
     // GNN schedule: every non-hub vertex by descending degree (ties by id), so that the vertices a
     // warp handles together have nearly equal neighbour counts.  The key buffer is free here (no
     // priorities exist right after an upload).
-    if (g->vorder) cudaFree(g->vorder);
-    g->vorder = nullptr;
     if ((s = gc_alloc(ctx, &g->vorder, (size_t)g->cap_N, "degree order")) != GC_OK) return s;
     k_degree_keys<<<ctx->num_sms * 4, 256, 0, ctx->stream>>>(g->V, g->N, g->key);
     ctx->launches++;

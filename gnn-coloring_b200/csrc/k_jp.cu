@@ -27,53 +27,102 @@ gc_status gc_sort_order_bits(gc_graph *g, int key_bits, bool filter, uint32_t *d
 namespace {
 using namespace gc;
 
-// Vertices with at most GC_SPLIT_BIG_DEGREE neighbours: one thread each.
-__global__ void k_jp_split_small(const uint32_t *__restrict__ V, const uint32_t *__restrict__ E,
-                                 const uint32_t *__restrict__ key, uint32_t N, uint32_t *__restrict__ P,
-                                 uint32_t *__restrict__ pc) {
-    for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < N; u += gridDim.x * blockDim.x) {
-        const uint32_t beg = V[u], end = V[u + 1];
-        if (end - beg > GC_SPLIT_BIG_DEGREE) {
-            pc[u] = 0;  // filled by k_jp_split_big
+// Split in the GNN's degree order (built at upload): the first n_wide vertices (more than
+// GC_GNN_WARP_DEGREE neighbours) one per warp, the rest eight per warp with four lanes each.  A
+// vertex is owned by one warp or quad, so its predecessors are packed with ballots alone.  Hubs
+// (not in the degree order) are split by k_jp_split_big.
+__global__ void __launch_bounds__(256) k_jp_split(const uint32_t *__restrict__ V, const uint32_t *__restrict__ E,
+                                                  const uint32_t *__restrict__ key, const uint32_t *__restrict__ vorder,
+                                                  uint32_t n_wide, uint32_t n_vorder, uint32_t *__restrict__ P,
+                                                  uint32_t *__restrict__ pc) {
+    const int lane = threadIdx.x & 31, q = lane & 3, qbase = lane & ~3;
+    const unsigned int lt = (1u << lane) - 1u;
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    const uint32_t n_items = n_wide + (n_vorder - n_wide + 7) / 8;
+    for (uint32_t it = warp; it < n_items; it += nwarps) {
+        if (it < n_wide) {
+            const uint32_t u = vorder[it];
+            const uint32_t beg = V[u], d = V[u + 1] - beg, ku = key[u];
+            uint32_t cnt = 0;
+            for (uint32_t c = 0; c < d; c += 64) {
+                const uint32_t ia = c + lane, ib = c + 32 + lane;
+                const uint32_t va = ia < d ? ld_stream(E + beg + ia) : 0u, vb = ib < d ? ld_stream(E + beg + ib) : 0u;
+                const bool pa = ia < d && precedes(key[va], va, ku, u);
+                const bool pb = ib < d && precedes(key[vb], vb, ku, u);
+                const unsigned int ma = __ballot_sync(0xffffffffu, pa);
+                if (pa) P[beg + cnt + __popc(ma & lt)] = va;
+                cnt += __popc(ma);
+                const unsigned int mb = __ballot_sync(0xffffffffu, pb);
+                if (pb) P[beg + cnt + __popc(mb & lt)] = vb;
+                cnt += __popc(mb);
+            }
+            if (lane == 0) pc[u] = cnt;
             continue;
         }
-        const uint32_t ku = key[u];
-        uint32_t w = beg;
-        for (uint32_t i = beg; i < end; i++) {
-            uint32_t v = ld_stream(E + i);
-            if (precedes(key[v], v, ku, u)) P[w++] = v;
+        const uint32_t slot = n_wide + (it - n_wide) * 8 + (lane >> 2);
+        const bool valid = slot < n_vorder;
+        const uint32_t u = valid ? vorder[slot] : 0u;
+        const uint32_t beg = valid ? V[u] : 0u, d = valid ? V[u + 1] - beg : 0u;
+        const uint32_t ku = valid ? key[u] : 0u;
+        const uint32_t dmax = __reduce_max_sync(0xffffffffu, d);
+        const unsigned int qlt = (1u << q) - 1u;
+        uint32_t cnt = 0;
+        for (uint32_t c = 0; c < dmax; c += 4) {
+            const uint32_t i = c + q;
+            const uint32_t v = i < d ? ld_stream(E + beg + i) : 0u;
+            const bool p = i < d && precedes(key[v], v, ku, u);
+            const unsigned int qm = (__ballot_sync(0xffffffffu, p) >> qbase) & 0xfu;
+            if (p) P[beg + cnt + __popc(qm & qlt)] = v;
+            cnt += __popc(qm);
         }
-        pc[u] = w - beg;
+        if (valid && q == 0) pc[u] = cnt;
     }
 }
 
-// Larger vertices: one warp per GC_SPLIT_CHUNK-edge chunk, slots reserved with atomics.
-__global__ void k_jp_split_big(const uint32_t *__restrict__ V, const uint32_t *__restrict__ E,
-                               const uint32_t *__restrict__ key, const uint32_t *__restrict__ tasks,
-                               uint32_t n_tasks, uint32_t *__restrict__ P, uint32_t *__restrict__ pc) {
+__global__ void k_zero_hub_counts(const uint32_t *__restrict__ hubs, uint32_t n, uint32_t *__restrict__ pc) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) pc[hubs[i]] = 0;
+}
+
+// Hubs: one warp per GC_SPLIT_CHUNK-edge chunk.  The warp gathers its chunk's
+// predecessors in shared memory, reserves their slots with one atomic on pc[u], then writes them
+// out coalesced (predecessor order within P does not matter).
+constexpr int SPLIT_WARPS = 8;
+__global__ void __launch_bounds__(SPLIT_WARPS * 32) k_jp_split_big(const uint32_t *__restrict__ V,
+                                                                   const uint32_t *__restrict__ E,
+                                                                   const uint32_t *__restrict__ key,
+                                                                   const uint32_t *__restrict__ tasks, uint32_t n_tasks,
+                                                                   uint32_t *__restrict__ P, uint32_t *__restrict__ pc) {
+    __shared__ uint32_t buf[SPLIT_WARPS][GC_SPLIT_CHUNK];
     const int lane = threadIdx.x & 31;
+    uint32_t *mine = buf[threadIdx.x >> 5];
     const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
     const unsigned int lt = (1u << lane) - 1u;
     for (uint32_t t = warp; t < n_tasks; t += nwarps) {
         const uint32_t u = tasks[2 * t], e0 = tasks[2 * t + 1];
         const uint32_t end = min(V[u + 1], e0 + GC_SPLIT_CHUNK);
-        const uint32_t ku = key[u], beg = V[u];
-        for (uint32_t i0 = e0; i0 < end; i0 += 32) {
-            const uint32_t i = i0 + lane;
-            bool is_pred = false;
-            uint32_t v = 0;
-            if (i < end) {
-                v = ld_stream(E + i);
-                is_pred = precedes(key[v], v, ku, u);
-            }
-            unsigned int m = __ballot_sync(0xffffffffu, is_pred);
-            if (!m) continue;
-            uint32_t slot = 0;
-            if (lane == 0) slot = atomicAdd(&pc[u], (uint32_t)__popc(m));
-            slot = __shfl_sync(0xffffffffu, slot, 0);
-            if (is_pred) P[beg + slot + __popc(m & lt)] = v;
+        const uint32_t ku = key[u];
+        uint32_t cnt = 0;
+        for (uint32_t i0 = e0; i0 < end; i0 += 64) {
+            const uint32_t ia = i0 + lane, ib = i0 + 32 + lane;
+            const uint32_t va = ia < end ? ld_stream(E + ia) : 0u, vb = ib < end ? ld_stream(E + ib) : 0u;
+            const bool pa = ia < end && precedes(key[va], va, ku, u);
+            const bool pb = ib < end && precedes(key[vb], vb, ku, u);
+            const unsigned int ma = __ballot_sync(0xffffffffu, pa);
+            if (pa) mine[cnt + __popc(ma & lt)] = va;
+            cnt += __popc(ma);
+            const unsigned int mb = __ballot_sync(0xffffffffu, pb);
+            if (pb) mine[cnt + __popc(mb & lt)] = vb;
+            cnt += __popc(mb);
         }
+        __syncwarp();
+        uint32_t slot = 0;
+        if (lane == 0 && cnt) slot = atomicAdd(&pc[u], cnt);
+        slot = __shfl_sync(0xffffffffu, slot, 0);
+        uint32_t *out = P + V[u] + slot;
+        for (uint32_t j = lane; j < cnt; j += 32) out[j] = mine[j];
+        __syncwarp();
     }
 }
 
@@ -387,11 +436,15 @@ gc_status gc_jp_color(gc_graph *g) {
     // 1. split, and color the sources
     {
         ProfScope ps(ctx, "jp_split", ctx->stream);
-        k_jp_split_small<<<grid, 256, 0, ctx->stream>>>(g->V, g->E, g->key, N, g->P, g->pc);
-        ctx->launches++;
-        if (g->n_big_tasks) {
-            k_jp_split_big<<<grid, 256, 0, ctx->stream>>>(g->V, g->E, g->key, g->big, g->n_big_tasks, g->P, g->pc);
+        if (g->n_vorder) {
+            k_jp_split<<<grid, 256, 0, ctx->stream>>>(g->V, g->E, g->key, g->vorder, g->n_wide, g->n_vorder, g->P, g->pc);
             ctx->launches++;
+        }
+        if (g->n_big_tasks) {
+            k_zero_hub_counts<<<ctx->num_sms, 256, 0, ctx->stream>>>(g->hubs, g->n_hubs, g->pc);
+            k_jp_split_big<<<grid, SPLIT_WARPS * 32, 0, ctx->stream>>>(g->V, g->E, g->key, g->big, g->n_big_tasks, g->P,
+                                                                      g->pc);
+            ctx->launches += 2;
         }
         k_jp_init_colors<<<ctx->num_sms * 4, 256, 0, ctx->stream>>>(g->pc, N, g->color);
         ctx->launches++;

@@ -8,7 +8,8 @@
 // up by ascending id.  Passes over digits that no key can have set are skipped: the caller
 // passes the key's bit width (known per heuristic: degree bound, color bound, 32 for floats).
 //
-// Per pass: tile histograms -> one exclusive scan in digit-major order -> stable scatter.
+// Per pass: tile histograms (and digit totals) -> scan of the digit totals -> one CTA per digit
+// scans that digit's tile counts -> stable scatter.
 // Stability inside a tile: each warp walks its own contiguous run of the tile in order, ranking
 // equal digits with __match_any_sync; per-digit warp totals are then prefixed across warps.
 #include "gc_internal.h"
@@ -59,7 +60,8 @@ __device__ __forceinline__ uint32_t digit_of(uint32_t k, int shift, uint32_t mas
 __device__ __forceinline__ uint32_t pass_len(const SortIn &in) { return in.first ? in.N : min(in.N, *in.d_n); }
 
 __global__ void __launch_bounds__(SORT_THREADS) k_sort_hist(SortIn in, int shift, uint32_t mask,
-                                                            uint32_t *__restrict__ counts, uint32_t ntiles) {
+                                                            uint32_t *__restrict__ counts, uint32_t ntiles,
+                                                            uint32_t *__restrict__ digit_total) {
     __shared__ uint32_t hist[RADIX];
     for (int i = threadIdx.x; i < RADIX; i += SORT_THREADS) hist[i] = 0;
     __syncthreads();
@@ -77,33 +79,54 @@ __global__ void __launch_bounds__(SORT_THREADS) k_sort_hist(SortIn in, int shift
         }
     }
     __syncthreads();
-    for (int d = threadIdx.x; d < RADIX; d += SORT_THREADS) counts[(size_t)d * ntiles + tile] = hist[d];
+    for (int d = threadIdx.x; d < RADIX; d += SORT_THREADS) {
+        counts[(size_t)d * ntiles + tile] = hist[d];
+        if (hist[d]) atomicAdd(&digit_total[d], hist[d]);
+    }
 }
 
-// Exclusive scan of `total` counters in place by one CTA of 1024 threads; the grand total (the
-// number of sorted elements) goes to *d_total when given.
-__global__ void __launch_bounds__(1024) k_sort_scan(uint32_t *__restrict__ counts, uint32_t total, uint32_t *d_total) {
-    __shared__ uint32_t part[1024];
-    const uint32_t per = (total + 1023) / 1024;
-    const uint32_t b = threadIdx.x * per, e = min(total, b + per);
-    uint32_t sum = 0;
-    for (uint32_t i = b; i < e; i++) sum += counts[i];
-    part[threadIdx.x] = sum;
+// Exclusive scan of the 256 digit totals (one CTA); the grand total -- the number of sorted
+// elements -- goes to *d_total when given.
+__global__ void __launch_bounds__(RADIX) k_sort_scan_digits(const uint32_t *__restrict__ digit_total,
+                                                            uint32_t *__restrict__ digit_base, uint32_t *d_total) {
+    __shared__ uint32_t part[RADIX];
+    part[threadIdx.x] = digit_total[threadIdx.x];
     __syncthreads();
-    // Hillis-Steele inclusive scan over the 1024 partial sums
-    for (int off = 1; off < 1024; off <<= 1) {
-        uint32_t v = threadIdx.x >= (unsigned)off ? part[threadIdx.x - off] : 0;
+    for (int off = 1; off < RADIX; off <<= 1) {
+        const uint32_t v = threadIdx.x >= (unsigned)off ? part[threadIdx.x - off] : 0;
         __syncthreads();
         part[threadIdx.x] += v;
         __syncthreads();
     }
-    uint32_t run = threadIdx.x ? part[threadIdx.x - 1] : 0;
+    digit_base[threadIdx.x] = threadIdx.x ? part[threadIdx.x - 1] : 0;
+    if (d_total && threadIdx.x == RADIX - 1) *d_total = part[RADIX - 1];
+}
+
+// One CTA per digit: exclusive scan of that digit's tile counts, offset by the digit's base, so
+// counts[d][t] becomes the first output position of digit d in tile t.
+constexpr int SCAN_THREADS = 512;
+__global__ void __launch_bounds__(SCAN_THREADS) k_sort_scan_tiles(uint32_t *__restrict__ counts, uint32_t ntiles,
+                                                                  const uint32_t *__restrict__ digit_base) {
+    __shared__ uint32_t part[SCAN_THREADS];
+    uint32_t *row = counts + (size_t)blockIdx.x * ntiles;
+    const uint32_t per = (ntiles + SCAN_THREADS - 1) / SCAN_THREADS;
+    const uint32_t b = threadIdx.x * per, e = min(ntiles, b + per);
+    uint32_t sum = 0;
+    for (uint32_t i = b; i < e; i++) sum += row[i];
+    part[threadIdx.x] = sum;
+    __syncthreads();
+    for (int off = 1; off < SCAN_THREADS; off <<= 1) {
+        const uint32_t v = threadIdx.x >= (unsigned)off ? part[threadIdx.x - off] : 0;
+        __syncthreads();
+        part[threadIdx.x] += v;
+        __syncthreads();
+    }
+    uint32_t run = digit_base[blockIdx.x] + (threadIdx.x ? part[threadIdx.x - 1] : 0);
     for (uint32_t i = b; i < e; i++) {
-        uint32_t c = counts[i];
-        counts[i] = run;
+        const uint32_t c = row[i];
+        row[i] = run;
         run += c;
     }
-    if (d_total && threadIdx.x == 1023) *d_total = part[1023];
 }
 
 __global__ void __launch_bounds__(SORT_THREADS) k_sort_scatter(SortIn in, int shift, uint32_t mask,
@@ -168,12 +191,18 @@ gc_status gc_sort_vertices(gc_graph *g, const uint32_t *keys, int key_bits, int 
     if (N == 0) return GC_OK;
     if ((s = gc_alloc(ctx, &g->sort_buf, 4 * (size_t)g->cap_N, "sort buffers")) != GC_OK) return s;
     const uint32_t ntiles = (N + SORT_TILE - 1) / SORT_TILE;
-    if (g->sort_hist_cap < (size_t)RADIX * ntiles) {
+    // tile counts, then per pass: digit totals and digit bases (4 passes at most)
+    const size_t hist_words = (size_t)RADIX * ntiles + 4 * 2 * RADIX;
+    if (g->sort_hist_cap < hist_words) {
         if (g->sort_hist) cudaFree(g->sort_hist);
         g->sort_hist = nullptr;
-        if ((s = gc_alloc(ctx, &g->sort_hist, (size_t)RADIX * ntiles, "sort histogram")) != GC_OK) return s;
-        g->sort_hist_cap = RADIX * ntiles;
+        if ((s = gc_alloc(ctx, &g->sort_hist, hist_words, "sort histogram")) != GC_OK) return s;
+        g->sort_hist_cap = (uint32_t)hist_words;
     }
+    uint32_t *digit_words = g->sort_hist + (size_t)RADIX * ntiles;
+    if ((s = gc_check_cuda(ctx, cudaMemsetAsync(digit_words, 0, sizeof(uint32_t) * 4 * 2 * RADIX, ctx->stream),
+                           "sort digit totals")) != GC_OK)
+        return s;
     const int passes = key_bits <= 0 ? 1 : (key_bits + 7) / 8;
     uint32_t *k0 = g->sort_buf, *v0 = g->sort_buf + g->cap_N;
     uint32_t *k1 = g->sort_buf + 2 * (size_t)g->cap_N, *v1 = g->sort_buf + 3 * (size_t)g->cap_N;
@@ -192,10 +221,12 @@ gc_status gc_sort_vertices(gc_graph *g, const uint32_t *keys, int key_bits, int 
         in.first = (p == 0);
         uint32_t *kout = (p & 1) ? k1 : k0, *vout = (p & 1) ? v1 : v0;
         if (p == passes - 1) vout = out;  // last pass writes the result directly
-        k_sort_hist<<<ntiles, SORT_THREADS, 0, ctx->stream>>>(in, shift, mask, g->sort_hist, ntiles);
-        k_sort_scan<<<1, 1024, 0, ctx->stream>>>(g->sort_hist, RADIX * ntiles, p == 0 ? d_count : nullptr);
+        uint32_t *digit_total = digit_words + 2 * RADIX * p, *digit_base = digit_total + RADIX;
+        k_sort_hist<<<ntiles, SORT_THREADS, 0, ctx->stream>>>(in, shift, mask, g->sort_hist, ntiles, digit_total);
+        k_sort_scan_digits<<<1, RADIX, 0, ctx->stream>>>(digit_total, digit_base, p == 0 ? d_count : nullptr);
+        k_sort_scan_tiles<<<RADIX, SCAN_THREADS, 0, ctx->stream>>>(g->sort_hist, ntiles, digit_base);
         k_sort_scatter<<<ntiles, SORT_THREADS, 0, ctx->stream>>>(in, shift, mask, g->sort_hist, ntiles, kout, vout);
-        ctx->launches += 3;
+        ctx->launches += 4;
         if ((s = gc_check_launch(ctx, "radix sort")) != GC_OK) return s;
         in.kin = kout;
         in.vin = vout;
