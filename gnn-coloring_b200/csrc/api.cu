@@ -187,7 +187,7 @@ gc_status gc_ctx_create(int device, gc_ctx **out) {
     if (const char *e = getenv("GC_JP_CTAS_PER_SM")) ctx->jp_ctas_per_sm = atoi(e);
     if (const char *e = getenv("GC_JP_TIGHT")) ctx->jp_tight = (unsigned int)strtoul(e, nullptr, 10);
     if (const char *e = getenv("GC_JP_NAP")) ctx->jp_nap = (unsigned int)strtoul(e, nullptr, 10);
-    if (const char *e = getenv("GC_GNN_SERIAL")) ctx->gnn_serial = atoi(e) != 0;
+    if (const char *e = getenv("GC_GNN_SERIAL")) ctx->gnn_serial = atoi(e) != 0;  // 0: overlap hubs and bulk
     if (s != GC_OK) {
         gc_ctx_destroy(ctx);
         return s;

@@ -102,8 +102,10 @@ __device__ __forceinline__ void warp_vertex(uint32_t u, const uint32_t *__restri
     const int q = lane & 3;
     const float4 zero4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     float s = 0.0f, s1 = 0.0f;  // lane l < 16: feature l (input layer: lane 0 sums deg/md, lane 1 id/N)
+    uint32_t nxt = lane < d ? ld_stream(E + beg + lane) : 0u;  // ids one step ahead
     for (uint32_t c = 0; c < d; c += 32) {
-        const uint32_t e = c + lane < d ? ld_stream(E + beg + c + lane) : 0u;
+        const uint32_t e = nxt;
+        nxt = c + 32 + lane < d ? ld_stream(E + beg + c + 32 + lane) : 0u;
         if (MODE == MODE_INPUT) {
             const float2 t = c + lane < d ? t01[e] : make_float2(0.0f, 0.0f);
             reinterpret_cast<float2 *>(slab)[lane] = t;
@@ -233,10 +235,14 @@ __global__ void __launch_bounds__(GNN_THREADS, 4) k_gnn_layer(const uint32_t *__
             out = dense_quad<MODE_INPUT>(W4, b4, q, qbase, FULL, zero4, zero4, s0, s1, self.x, self.y);
         } else {
             float4 s = zero4;
+            // neighbour ids one step ahead, so the row loads never wait for them
+            uint32_t n0 = q < d ? ld_stream(E + beg + q) : 0u;
+            uint32_t n1 = 4 + q < d ? ld_stream(E + beg + 4 + q) : 0u;
             for (uint32_t c = 0; c < dmax; c += 8) {
                 // two groups of four neighbours in flight per quad
-                const uint32_t e0 = c + q < d ? ld_stream(E + beg + c + q) : 0u;
-                const uint32_t e1 = c + 4 + q < d ? ld_stream(E + beg + c + 4 + q) : 0u;
+                const uint32_t e0 = n0, e1 = n1;
+                n0 = c + 8 + q < d ? ld_stream(E + beg + c + 8 + q) : 0u;
+                n1 = c + 12 + q < d ? ld_stream(E + beg + c + 12 + q) : 0u;
                 float4 r[8];
 #pragma unroll
                 for (int k = 0; k < 8; k++) {
@@ -262,128 +268,147 @@ __global__ void __launch_bounds__(GNN_THREADS, 4) k_gnn_layer(const uint32_t *__
 
 // ---- hub vertices: one CTA each --------------------------------------------------------------
 
-constexpr int HUB_THREADS = 128;  // one neighbour row per thread per stage
-constexpr int HUB_ROWS = HUB_THREADS;
-constexpr int HUB_STAGES = 8;      // rows in flight: 7 stages ahead of the adder
-constexpr int HUB_ID_AHEAD = 4;    // neighbour ids are loaded this many stages before their rows
+// Hub CTAs: a producer warp streams the hub's neighbour rows into a shared-memory ring with
+// cp.async, each stage completing on its own mbarrier; a consumer quad adds the rows in CSR
+// order, four features per lane.  No CTA-wide barrier: the producer runs up to HUB_STAGES stages
+// ahead and refills a stage as soon as the consumer releases it.  Every mbarrier wait is bounded:
+// on expiry the kernel raises ERR_WAIT_EXPIRED and returns.
+constexpr int HUB_THREADS = 64;    // warp 0 adds, warp 1 loads
+constexpr int HUB_ROWS = 128;      // rows per stage: 4 per producer lane
+constexpr int HUB_STAGES = 12;
+constexpr int HUB_ID_AHEAD = 4;    // the producer reads neighbour ids this many stages early
+constexpr unsigned int HUB_WAIT_LIMIT = 1u << 20;  // each try_wait may also suspend briefly
 
+__device__ __forceinline__ unsigned int smem_u32(const void *p) { return (unsigned int)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned int count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+    asm volatile("{\n .reg .b64 st;\n mbarrier.arrive.shared::cta.b64 st, [%0];\n}" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_on_copies(uint64_t *bar) {
+    asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned int parity) {
+    unsigned int ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Waits for the phase of `parity` to complete; false if the wait gave up (error raised).
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned int parity, DevState *st) {
+    for (unsigned int i = 0; i < HUB_WAIT_LIMIT; i++) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if ((i & 1023u) == 1023u && ld_relaxed_u32(&st->err)) return false;
+    }
+    raise_error(st, ERR_WAIT_EXPIRED, 0xffffffffu);
+    return false;
+}
 __device__ __forceinline__ void cp_async_16(void *smem, const void *gmem) {
-    unsigned int sa = (unsigned int)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(gmem) : "memory");
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(smem)), "l"(gmem) : "memory");
 }
 __device__ __forceinline__ void cp_async_8(void *smem, const void *gmem) {
-    unsigned int sa = (unsigned int)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(sa), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(smem)), "l"(gmem) : "memory");
 }
 
-// All threads stream the hub's neighbour rows into a shared-memory ring (cp.async, HUB_STAGES
-// deep; the neighbour ids themselves are read HUB_ID_AHEAD stages earlier), and the first four
-// lanes of warp 0 add the rows in CSR order, four features per lane, with the next eight rows'
-// shared-memory loads in flight, so the chain runs at the FP32 add latency.
 template <int MODE>
 __global__ void __launch_bounds__(HUB_THREADS) k_gnn_hub(const uint32_t *__restrict__ V, const uint32_t *__restrict__ E,
                                                          const uint32_t *__restrict__ hubs,
                                                          const float2 *__restrict__ t01, const float *__restrict__ x,
                                                          float *__restrict__ y, uint32_t *__restrict__ key,
-                                                         const float *__restrict__ Wb) {
+                                                         const float *__restrict__ Wb, DevState *st) {
     constexpr int ROW = (MODE == MODE_INPUT) ? 2 : FEAT;  // floats per staged row
     extern __shared__ __align__(16) float stage[];         // HUB_STAGES * HUB_ROWS * ROW floats
     __shared__ __align__(16) float sW[LAYER_PARAMS];
+    __shared__ __align__(8) uint64_t full[HUB_STAGES], empty[HUB_STAGES];
     for (int i = threadIdx.x; i < LAYER_PARAMS; i += blockDim.x) sW[i] = Wb[i];
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < HUB_STAGES; i++) {
+            mbar_init(&full[i], 32);  // one copy-completion arrival per producer lane
+            mbar_init(&empty[i], 1);  // the consumer's release
+        }
+    }
+    __syncthreads();
     const uint32_t u = hubs[blockIdx.x];
     const uint32_t beg = V[u], end = V[u + 1], d = end - beg;
     const uint32_t nchunks = (d + HUB_ROWS - 1) / HUB_ROWS;
-    const int tid = threadIdx.x;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
-    auto load_id = [&](uint32_t c) -> uint32_t {
-        const uint32_t i = beg + c * HUB_ROWS + tid;
-        return (c < nchunks && i < end) ? ld_stream(E + i) : 0xffffffffu;
-    };
-    auto issue = [&](uint32_t c, uint32_t v) {
-        if (v != 0xffffffffu) {
-            float *dst = stage + ((size_t)(c % HUB_STAGES) * HUB_ROWS + tid) * ROW;
-            if (MODE == MODE_INPUT) {
-                cp_async_8(dst, t01 + v);
-            } else {
-                const float *src = x + (size_t)v * FEAT;
+    if (warp == 1) {
+        // producer: ids HUB_ID_AHEAD stages ahead in registers, rows via cp.async
+        uint32_t ids[HUB_ID_AHEAD][4];
+        auto load_ids = [&](uint32_t c, uint32_t (&out)[4]) {
 #pragma unroll
-                for (int k = 0; k < 4; k++) cp_async_16(dst + 4 * k, src + 4 * k);
+            for (int k = 0; k < 4; k++) {
+                const uint32_t i = beg + c * HUB_ROWS + k * 32 + lane;
+                out[k] = (c < nchunks && i < end) ? ld_stream(E + i) : 0xffffffffu;
             }
-        }
-        cp_async_commit();  // empty groups keep the group count uniform
-    };
-
-    // ids of the stages to be issued next, oldest first
-    uint32_t id0, id1, id2, id3;
-    for (int c = 0; c < HUB_STAGES - 1; c++) issue(c, load_id(c));
-    id0 = load_id(HUB_STAGES - 1);
-    id1 = load_id(HUB_STAGES);
-    id2 = load_id(HUB_STAGES + 1);
-    id3 = load_id(HUB_STAGES + 2);
-    static_assert(HUB_ID_AHEAD == 4, "the id ring below holds four stages");
-
-    const int q = tid & 3;
-    float4 s = make_float4(0.0f, 0.0f, 0.0f, 0.0f);  // hidden: features 4q..4q+3; input: (deg, id) in .x/.y
-    for (uint32_t c = 0; c < nchunks; c++) {
-        issue(c + HUB_STAGES - 1, id0);
-        id0 = id1;
-        id1 = id2;
-        id2 = id3;
-        id3 = load_id(c + HUB_STAGES - 1 + HUB_ID_AHEAD);
-        cp_async_wait<HUB_STAGES - 1>();
-        __syncthreads();
-        if (tid < 4) {
-            const float *buf = stage + (size_t)(c % HUB_STAGES) * HUB_ROWS * ROW;
-            const uint32_t cnt = min((uint32_t)HUB_ROWS, end - (beg + c * HUB_ROWS));
-            if (MODE == MODE_INPUT) {
-                const float2 *b2 = reinterpret_cast<const float2 *>(buf);
-                uint32_t r = 0;
-                for (; r + 8 <= cnt; r += 8) {
-                    float2 t[8];
+        };
 #pragma unroll
-                    for (int k = 0; k < 8; k++) t[k] = b2[r + k];
+        for (int a = 0; a < HUB_ID_AHEAD; a++) load_ids(a, ids[a]);
+        for (uint32_t c = 0; c < nchunks; c++) {
+            const uint32_t s = c % HUB_STAGES;
+            if (c >= HUB_STAGES && !mbar_wait(&empty[s], ((c / HUB_STAGES) - 1) & 1u, st)) {
+                asm volatile("cp.async.wait_all;" ::: "memory");
+                return;
+            }
+            float *buf = stage + (size_t)s * HUB_ROWS * ROW;
 #pragma unroll
-                    for (int k = 0; k < 8; k++) {
-                        s.x = __fadd_rn(s.x, t[k].x);
-                        s.y = __fadd_rn(s.y, t[k].y);
+            for (int k = 0; k < 4; k++) {
+                const uint32_t v = ids[0][k];
+                if (v != 0xffffffffu) {
+                    float *dst = buf + (size_t)(k * 32 + lane) * ROW;
+                    if (MODE == MODE_INPUT) {
+                        cp_async_8(dst, t01 + v);
+                    } else {
+                        const float *src = x + (size_t)v * FEAT;
+#pragma unroll
+                        for (int w = 0; w < 4; w++) cp_async_16(dst + 4 * w, src + 4 * w);
                     }
                 }
-                for (; r < cnt; r++) {
-                    const float2 t = b2[r];
-                    s.x = __fadd_rn(s.x, t.x);
-                    s.y = __fadd_rn(s.y, t.y);
-                }
-            } else {
-                const float4 *b4 = reinterpret_cast<const float4 *>(buf);
-                uint32_t r = 0;
-                if (cnt >= 8) {
-                    float4 t[8];
-#pragma unroll
-                    for (int k = 0; k < 8; k++) t[k] = b4[k * 4 + q];
-                    for (r = 8; r + 8 <= cnt; r += 8) {
-                        float4 nx[8];
-#pragma unroll
-                        for (int k = 0; k < 8; k++) nx[k] = b4[(r + k) * 4 + q];
-#pragma unroll
-                        for (int k = 0; k < 8; k++) s = add4(s, t[k]);
-#pragma unroll
-                        for (int k = 0; k < 8; k++) t[k] = nx[k];
-                    }
-#pragma unroll
-                    for (int k = 0; k < 8; k++) s = add4(s, t[k]);
-                }
-                for (; r < cnt; r++) s = add4(s, b4[r * 4 + q]);
             }
+            mbar_arrive_on_copies(&full[s]);
+#pragma unroll
+            for (int a = 0; a + 1 < HUB_ID_AHEAD; a++)
+#pragma unroll
+                for (int k = 0; k < 4; k++) ids[a][k] = ids[a + 1][k];
+            load_ids(c + HUB_ID_AHEAD, ids[HUB_ID_AHEAD - 1]);
         }
-        __syncthreads();
+        asm volatile("cp.async.wait_all;" ::: "memory");  // leave no copy of ours in flight
+        return;
     }
-    cp_async_wait<0>();
-    if (tid >= 4) return;
+
+    // consumer: warp 0.  Lane l < 16 owns feature l (input layer: lane 0 sums deg/md, lane 1 id/N):
+    // one shared-memory load and one add per row per lane, so the chain runs at the add latency.
+    float acc = 0.0f;
+    for (uint32_t c = 0; c < nchunks; c++) {
+        const uint32_t s = c % HUB_STAGES;
+        if (!mbar_wait(&full[s], (c / HUB_STAGES) & 1u, st)) return;
+        const float *buf = stage + (size_t)s * HUB_ROWS * ROW;
+        const uint32_t cnt = min((uint32_t)HUB_ROWS, end - (beg + c * HUB_ROWS));
+        if (lane < ROW) {
+            if (cnt == HUB_ROWS) {
+#pragma unroll 32
+                for (uint32_t r = 0; r < HUB_ROWS; r++) acc = __fadd_rn(acc, buf[r * ROW + lane]);
+            } else {
+                for (uint32_t r = 0; r < cnt; r++) acc = __fadd_rn(acc, buf[r * ROW + lane]);
+            }
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[s]);
+    }
+    // hand the 16 feature sums (or the two input sums) to the quad that runs the dense part
+    const int q = lane & 3;
+    float4 nb;
+    nb.x = __shfl_sync(0xffffffffu, acc, 4 * q + 0);
+    nb.y = __shfl_sync(0xffffffffu, acc, 4 * q + 1);
+    nb.z = __shfl_sync(0xffffffffu, acc, 4 * q + 2);
+    nb.w = __shfl_sync(0xffffffffu, acc, 4 * q + 3);
+    const float in0 = __shfl_sync(0xffffffffu, acc, 0), in1 = __shfl_sync(0xffffffffu, acc, 1);
+    if (lane >= 4) return;
     const unsigned int mask = 0xfu;
     const float4 *W4 = reinterpret_cast<const float4 *>(sW);
     const float4 b4 = reinterpret_cast<const float4 *>(sW + 2 * FEAT * FEAT)[q];
@@ -391,7 +416,7 @@ __global__ void __launch_bounds__(HUB_THREADS) k_gnn_hub(const uint32_t *__restr
     const float4 zero4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     float4 out;
     if (MODE == MODE_INPUT) {
-        float s0 = s.x, s1 = s.y;  // every lane of the quad ran the same two chains
+        float s0 = in0, s1 = in1;
         if (fd > 0.0f) {
             s0 = __fdiv_rn(s0, fd);
             s1 = __fdiv_rn(s1, fd);
@@ -399,9 +424,9 @@ __global__ void __launch_bounds__(HUB_THREADS) k_gnn_hub(const uint32_t *__restr
         const float2 self = t01[u];
         out = dense_quad<MODE_INPUT>(W4, b4, q, 0, mask, zero4, zero4, s0, s1, self.x, self.y);
     } else {
-        if (fd > 0.0f) s = make_float4(__fdiv_rn(s.x, fd), __fdiv_rn(s.y, fd), __fdiv_rn(s.z, fd), __fdiv_rn(s.w, fd));
+        if (fd > 0.0f) nb = make_float4(__fdiv_rn(nb.x, fd), __fdiv_rn(nb.y, fd), __fdiv_rn(nb.z, fd), __fdiv_rn(nb.w, fd));
         const float4 self = reinterpret_cast<const float4 *>(x)[(size_t)u * 4 + q];
-        out = dense_quad<MODE>(W4, b4, q, 0, mask, s, self, 0.0f, 0.0f, 0.0f, 0.0f);
+        out = dense_quad<MODE>(W4, b4, q, 0, mask, nb, self, 0.0f, 0.0f, 0.0f, 0.0f);
     }
     if (MODE == MODE_OUTPUT) {
         const float sum = output_sum(out, mask);
@@ -427,7 +452,8 @@ gc_status launch_layer(gc_graph *g, const float *Wb, const float *x, float *y, c
         if ((s = gc_check_cuda(ctx, cudaStreamWaitEvent(side, fork, 0), "fork")) != GC_OK) return s;
         ProfScope ps(ctx, MODE == MODE_INPUT ? "gnn_hub_input" : (MODE == MODE_HIDDEN ? "gnn_hub_hidden" : "gnn_hub_output"),
                      side);
-        k_gnn_hub<MODE><<<g->n_hubs, HUB_THREADS, smem, side>>>(g->V, g->E, g->hubs, g->t01, x, y, g->key, Wb);
+        k_gnn_hub<MODE><<<g->n_hubs, HUB_THREADS, smem, side>>>(g->V, g->E, g->hubs, g->t01, x, y, g->key, Wb,
+                                                                ctx->dstate);
         ctx->launches++;
         if ((s = gc_check_launch(ctx, "gnn hub layer")) != GC_OK) return s;
     }
