@@ -37,6 +37,10 @@ gc_status gc_read_state(gc_ctx *ctx) {
         "read device state");
     if (s != GC_OK) return s;
     if ((s = gc_check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "kernel execution")) != GC_OK) return s;
+    return gc_check_hstate(ctx);
+}
+
+gc_status gc_check_hstate(gc_ctx *ctx) {
     unsigned int err = ctx->hstate->err;
     if (err) {
         char buf[160];
@@ -76,12 +80,6 @@ ProfScope::~ProfScope() {
 
 namespace {
 
-struct DeviceGuard {
-    explicit DeviceGuard(const gc_ctx *ctx) {
-        if (ctx) cudaSetDevice(ctx->device);
-    }
-};
-
 __global__ void k_check_csr(const uint32_t *__restrict__ V, const uint32_t *__restrict__ E, uint32_t N, uint32_t M,
                             gc::DevState *st) {
     const uint32_t stride = gridDim.x * blockDim.x;
@@ -98,19 +96,22 @@ __global__ void k_keys_to_double(const uint32_t *__restrict__ key, uint32_t N, i
         p[u] = float_bits ? (double)__uint_as_float(key[u]) : (double)key[u];
 }
 
-void free_graph_buffers(gc_graph *g) {
+}  // namespace
+
+void gc_graph_free_buffers(gc_graph *g) {
+    gc_ctx *ctx = g->ctx;
     if (g->owns_csr) {
-        cudaFree(g->V);
-        cudaFree(g->E);
+        gc_dev_free(ctx, g->V);
+        gc_dev_free(ctx, g->E);
     }
-    void *bufs[] = {g->key,     g->color,    g->P,       g->pc,      g->order,    g->sort_buf, g->sort_hist,
-                    g->big,     g->hubs,     g->x,       g->y,       g->t01,      g->deg_rem,  g->frontier,
-                    g->frontier2, g->removed, g->leaf_list, g->vorder, g->rank, g->p64};
-    for (void *p : bufs)
-        if (p) cudaFree(p);
+    void *bufs[] = {g->key,       g->color,  g->P,        g->pc,       g->order,    g->sort_buf, g->sort_hist,
+                    g->big,       g->hubs,   g->x,        g->y,        g->t01,      g->deg_rem,  g->frontier,
+                    g->frontier2, g->removed, g->leaf_list, g->vorder, g->rank,     g->p64,      g->seg_voff,
+                    g->seg_stat};
+    for (void *p : bufs) gc_dev_free(ctx, p);
 }
 
-gc_status alloc_graph(gc_ctx *ctx, gc_graph *g, uint32_t N, uint32_t M, bool csr) {
+gc_status gc_graph_alloc(gc_ctx *ctx, gc_graph *g, uint32_t N, uint32_t M, bool csr) {
     gc_status s;
     g->cap_N = N;
     g->cap_M = M;
@@ -123,6 +124,8 @@ gc_status alloc_graph(gc_ctx *ctx, gc_graph *g, uint32_t N, uint32_t M, bool csr
     return GC_OK;
 }
 
+namespace {
+
 gc_status check_host_csr(gc_ctx *ctx, uint32_t N, const uint32_t *V, const uint32_t *E) {
     if (!V) return gc_fail(ctx, GC_ERR_INVALID, "V is NULL");
     if (V[0] != 0) return gc_fail(ctx, GC_ERR_INVALID, "V[0] must be 0");
@@ -130,7 +133,9 @@ gc_status check_host_csr(gc_ctx *ctx, uint32_t N, const uint32_t *V, const uint3
     return GC_OK;
 }
 
-gc_status finish_upload(gc_graph *g) {
+}  // namespace
+
+gc_status gc_graph_finish_upload(gc_graph *g) {
     gc_ctx *ctx = g->ctx;
     gc_status s;
     g->has_keys = g->has_colors = false;
@@ -145,7 +150,6 @@ gc_status finish_upload(gc_graph *g) {
     return gc_graph_prepare(g);
 }
 
-}  // namespace
 
 extern "C" {
 
@@ -294,7 +298,7 @@ gc_status gc_graph_upload(gc_ctx *ctx, uint32_t N, const uint32_t *V, const uint
     gc_graph *g = new gc_graph();
     g->ctx = ctx;
     ctx_retain(ctx);
-    if ((s = alloc_graph(ctx, g, N, V[N], true)) != GC_OK) {
+    if ((s = gc_graph_alloc(ctx, g, N, V[N], true)) != GC_OK) {
         gc_graph_free(g);
         return s;
     }
@@ -313,7 +317,7 @@ gc_status gc_graph_create(gc_ctx *ctx, uint32_t cap_N, uint32_t cap_M, gc_graph 
     gc_graph *g = new gc_graph();
     g->ctx = ctx;
     ctx_retain(ctx);
-    gc_status s = alloc_graph(ctx, g, cap_N, cap_M, true);
+    gc_status s = gc_graph_alloc(ctx, g, cap_N, cap_M, true);
     if (s != GC_OK) {
         gc_graph_free(g);
         return s;
@@ -337,7 +341,7 @@ gc_status gc_graph_reupload(gc_ctx *ctx, gc_graph *g, uint32_t N, const uint32_t
     if (M && (s = gc_check_cuda(ctx, cudaMemcpyAsync(g->E, E, sizeof(uint32_t) * (size_t)M, cudaMemcpyHostToDevice,
                                                      ctx->stream), "upload E")) != GC_OK)
         return s;
-    return finish_upload(g);
+    return gc_graph_finish_upload(g);
 }
 
 gc_status gc_graph_wrap_device(gc_ctx *ctx, uint32_t N, uint32_t M, const uint32_t *dV, const uint32_t *dE,
@@ -351,11 +355,11 @@ gc_status gc_graph_wrap_device(gc_ctx *ctx, uint32_t N, uint32_t M, const uint32
     g->owns_csr = false;
     g->V = const_cast<uint32_t *>(dV);
     g->E = const_cast<uint32_t *>(dE);
-    gc_status s = alloc_graph(ctx, g, N, M, false);
+    gc_status s = gc_graph_alloc(ctx, g, N, M, false);
     if (s == GC_OK) {
         g->N = N;
         g->M = M;
-        s = finish_upload(g);
+        s = gc_graph_finish_upload(g);
     }
     if (s != GC_OK) {
         gc_graph_free(g);
@@ -371,7 +375,7 @@ void gc_graph_free(gc_graph *g) {
     {
         DeviceGuard dg(ctx);
         if (ctx) cudaStreamSynchronize(ctx->stream);
-        free_graph_buffers(g);
+        gc_graph_free_buffers(g);
     }
     delete g;
     if (ctx) ctx_release(ctx);
@@ -451,8 +455,11 @@ gc_status gc_priority(gc_ctx *ctx, gc_graph *g, gc_heuristic h, const gc_model *
         case GC_FF:
         case GC_LF:
         case GC_LLF: s = gc_priority_simple(g, h); break;
-        case GC_SL: s = gc_priority_peel(g, false); break;
-        case GC_SLL: s = gc_priority_peel(g, true); break;
+        case GC_SL:
+        case GC_SLL:
+            if (g->n_seg > 1) return gc_fail(ctx, GC_ERR_INVALID, "SL / SLL peel each graph on its own: not offered on batches");
+            s = gc_priority_peel(g, h == GC_SLL);
+            break;
         case GC_GNN:
             if (!model) return gc_fail(ctx, GC_ERR_INVALID, "GNN priorities need a model");
             s = gc_priority_gnn(g, model);

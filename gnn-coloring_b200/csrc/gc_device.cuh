@@ -60,4 +60,16 @@ __device__ __forceinline__ bool precedes(uint32_t kv, uint32_t v, uint32_t ku, u
     return kv > ku || (kv == ku && v < u);
 }
 
+// Segment of vertex u in a segmented CSR: the s with voff[s] <= u < voff[s + 1] (empty segments
+// are skipped).  Requires voff[0] = 0 <= u < voff[nseg].
+__device__ __forceinline__ uint32_t seg_of(const uint32_t *__restrict__ voff, uint32_t nseg, uint32_t u) {
+    uint32_t lo = 0, hi = nseg;  // voff[lo] <= u < voff[hi]
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (__ldg(voff + mid) <= u) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
 }  // namespace gc

@@ -24,11 +24,13 @@ struct gc_ctx {
     cudaStream_t side_stream = nullptr;  // GNN hub CTAs run here, overlapping the bulk of a layer
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     int color_blocks_per_sm = 0;         // resident CTAs of the coloring kernel (occupancy query)
-    int jp_ctas_per_sm = 2;              // cap on the above: fewer pollers beat more lookahead (measured)
+    int jp_ctas_per_sm = 2;              // CTAs per SM of the coloring kernel: fewer pollers beat more lookahead (measured)
     unsigned int jp_tight = 32;          // coloring: unproductive polling rounds before sleeping
     unsigned int jp_nap = 32;            // coloring: first sleep between polling rounds (ns)
     int gnn_blocks_per_sm[3] = {0, 0, 0};  // resident CTAs of each GNN layer kernel
     bool gnn_serial = true;              // hub CTAs before the bulk (measured faster than beside it)
+    bool hub_smem_set[3] = {false, false, false};  // hub kernels' shared-memory limit raised
+    cudaMemPool_t pool = nullptr;        // when set, graph buffers are stream-ordered allocations from this pool
     gc::DevState *dstate = nullptr;      // device status block
     gc::DevState *hstate = nullptr;      // pinned host mirror for read-back
     uint64_t launches = 0;
@@ -94,6 +96,18 @@ struct gc_graph {
     float2 *t01 = nullptr;
     // SL/SLL scratch (allocated on first use)
     uint32_t *deg_rem = nullptr, *frontier = nullptr, *frontier2 = nullptr, *removed = nullptr;
+    // tier thresholds and vertex schedule of the split and GNN kernels (gc_graph_prepare applies them)
+    uint32_t warp_deg = GC_GNN_WARP_DEGREE, hub_deg = GC_GNN_HUB_DEGREE;
+    int sched = GC_SCHEDULE_DEGREE;
+    // coloring-kernel overrides (0 = the context's value)
+    int jp_ctas = 0;
+    unsigned int jp_tight = 0, jp_nap = 0;
+    // segments: n_seg independent graphs in one CSR (0 = a single graph).  Segment s owns the
+    // vertices [seg_voff[s], seg_voff[s + 1]); E holds global ids after the upload.
+    uint32_t n_seg = 0, seg_cap = 0;
+    uint32_t *seg_voff = nullptr;    // device copy of the vertex offsets
+    int32_t *seg_stat = nullptr;     // device, 2 * seg_cap: largest color, improper flag per segment
+    std::vector<uint32_t> h_seg_voff;
     // stats of the last coloring
     int colors_used = 0;
     std::vector<double> user_p;  // priorities given by gc_priority_set, returned unchanged
@@ -107,21 +121,41 @@ struct gc_model {
     float *h_param = nullptr;  // host copy
 };
 
+// Makes the context's device current for the scope of a call.
+struct DeviceGuard {
+    explicit DeviceGuard(const gc_ctx *ctx) {
+        if (ctx) cudaSetDevice(ctx->device);
+    }
+};
+
 // ---- helpers (api.cu) ----
+gc_status gc_graph_alloc(gc_ctx *ctx, gc_graph *g, uint32_t N, uint32_t M, bool csr);  // CSR, keys, colors
+gc_status gc_graph_finish_upload(gc_graph *g);  // CSR checks, then gc_graph_prepare
+void gc_graph_free_buffers(gc_graph *g);
 gc_status gc_fail(gc_ctx *ctx, gc_status s, const std::string &msg);
 gc_status gc_check_cuda(gc_ctx *ctx, cudaError_t e, const char *what);
 gc_status gc_check_launch(gc_ctx *ctx, const char *what);
 gc_status gc_read_state(gc_ctx *ctx);  // syncs, copies DevState, reports device errors
+gc_status gc_check_hstate(gc_ctx *ctx);  // reports device errors of an already copied DevState
 gc_status gc_reset_state(gc_ctx *ctx);
 template <typename T>
 gc_status gc_alloc(gc_ctx *ctx, T **p, size_t count, const char *what) {
     if (*p) return GC_OK;
-    cudaError_t e = cudaMalloc((void **)p, sizeof(T) * (count ? count : 1));
+    const size_t bytes = sizeof(T) * (count ? count : 1);
+    cudaError_t e = ctx->pool ? cudaMallocFromPoolAsync((void **)p, bytes, ctx->pool, ctx->stream)
+                              : cudaMalloc((void **)p, bytes);
     if (e != cudaSuccess) {
         *p = nullptr;
         return gc_check_cuda(ctx, e, what);
     }
     return GC_OK;
+}
+
+// Frees a device buffer of a graph owned by ctx (stream-ordered when the context allocates from a pool).
+inline void gc_dev_free(gc_ctx *ctx, void *p) {
+    if (!p) return;
+    if (ctx && ctx->pool) cudaFreeAsync(p, ctx->stream);
+    else cudaFree(p);
 }
 
 // ---- kernel drivers ----
@@ -137,3 +171,5 @@ enum { SORT_KEEP_ALL = 0, SORT_KEEP_INNER = 1, SORT_KEEP_DEG_AT_MOST = 2 };
 gc_status gc_sort_vertices(gc_graph *g, const uint32_t *keys, int key_bits, int filter, uint32_t max_deg,
                            uint32_t *out, uint32_t *d_count);
 gc_status gc_sort_order_bits(gc_graph *g, int key_bits, bool filter, uint32_t *d_count);
+// Segments (batch.cu): per-segment largest color and improper flag into g->seg_stat.
+gc_status gc_segment_stats(gc_graph *g);

@@ -61,11 +61,21 @@ gc_status gc_csr_build(uint32_t N, uint64_t L, const uint32_t *I, const uint32_t
         free(V);
         return GC_ERR_NOMEM;
     }
+    // Inside an enclosing parallel region (many graphs built at once) or for small inputs the
+    // passes run on this thread alone, without atomics.
+    const bool par = !omp_in_parallel() && L >= (1u << 16);
     // degree count
+    if (par) {
 #pragma omp parallel for schedule(static)
-    for (uint64_t k = 0; k < L; k++) {
-        __atomic_add_fetch(&off[I[k] + 1], 1, __ATOMIC_RELAXED);
-        __atomic_add_fetch(&off[J[k] + 1], 1, __ATOMIC_RELAXED);
+        for (uint64_t k = 0; k < L; k++) {
+            __atomic_add_fetch(&off[I[k] + 1], 1, __ATOMIC_RELAXED);
+            __atomic_add_fetch(&off[J[k] + 1], 1, __ATOMIC_RELAXED);
+        }
+    } else {
+        for (uint64_t k = 0; k < L; k++) {
+            off[I[k] + 1]++;
+            off[J[k] + 1]++;
+        }
     }
     for (uint32_t u = 0; u < N; u++) off[u + 1] += off[u];
     uint64_t M2 = off[N];
@@ -79,12 +89,19 @@ gc_status gc_csr_build(uint32_t N, uint64_t L, const uint32_t *I, const uint32_t
         return GC_ERR_NOMEM;
     }
     memcpy(cur, off, sizeof(uint64_t) * ((size_t)N + 1));
+    if (par) {
 #pragma omp parallel for schedule(static)
-    for (uint64_t k = 0; k < L; k++) {
-        uint64_t a = __atomic_fetch_add(&cur[I[k]], 1, __ATOMIC_RELAXED);
-        tmp[a] = J[k];
-        uint64_t b = __atomic_fetch_add(&cur[J[k]], 1, __ATOMIC_RELAXED);
-        tmp[b] = I[k];
+        for (uint64_t k = 0; k < L; k++) {
+            uint64_t a = __atomic_fetch_add(&cur[I[k]], 1, __ATOMIC_RELAXED);
+            tmp[a] = J[k];
+            uint64_t b = __atomic_fetch_add(&cur[J[k]], 1, __ATOMIC_RELAXED);
+            tmp[b] = I[k];
+        }
+    } else {
+        for (uint64_t k = 0; k < L; k++) {
+            tmp[cur[I[k]]++] = J[k];
+            tmp[cur[J[k]]++] = I[k];
+        }
     }
     free(cur);
     // sort + simplify each list in place; record the kept count
@@ -95,11 +112,20 @@ gc_status gc_csr_build(uint32_t N, uint64_t L, const uint32_t *I, const uint32_t
         free(tmp);
         return GC_ERR_NOMEM;
     }
-#pragma omp parallel for schedule(dynamic, 1024)
+#pragma omp parallel for schedule(dynamic, 1024) if (par)
     for (uint32_t u = 0; u < N; u++) {
         uint32_t *a = tmp + off[u];
         uint64_t d = off[u + 1] - off[u];
-        std::sort(a, a + d);
+        if (d <= 24) {  // short lists: insertion sort
+            for (uint64_t i = 1; i < d; i++) {
+                const uint32_t x = a[i];
+                uint64_t j = i;
+                for (; j > 0 && a[j - 1] > x; j--) a[j] = a[j - 1];
+                a[j] = x;
+            }
+        } else {
+            std::sort(a, a + d);
+        }
         uint64_t w = 0;
         for (uint64_t i = 0; i < d; i++) {
             uint32_t v = a[i];
@@ -119,7 +145,7 @@ gc_status gc_csr_build(uint32_t N, uint64_t L, const uint32_t *I, const uint32_t
         free(tmp);
         return GC_ERR_NOMEM;
     }
-#pragma omp parallel for schedule(dynamic, 1024)
+#pragma omp parallel for schedule(dynamic, 1024) if (par)
     for (uint32_t u = 0; u < N; u++)
         memcpy(E + V[u], tmp + off[u], sizeof(uint32_t) * (V[u + 1] - V[u]));
     free(tmp);
@@ -489,6 +515,95 @@ gc_status gc_gen_stencil27(uint32_t nx, uint32_t ny, uint32_t nz, uint32_t **V_o
                             E[w++] = (uint32_t)((Z * ny + Y) * nx + X);
                         }
             }
+    *V_out = V;
+    *E_out = E;
+    return GC_OK;
+}
+
+gc_status gc_gen_mixed(uint64_t seed, uint32_t n_min, uint32_t n_max, uint32_t *n_out, int *kind_out,
+                       double *param_out, uint32_t **V, uint32_t **E) {
+    if (!V || !E || n_min < 2 || n_max < n_min) return GC_ERR_INVALID;
+    uint64_t s = stream_state(seed, 0x6d69786564ULL);
+    const double lo = std::log((double)n_min), hi = std::log((double)n_max);
+    double nf = std::exp(lo + uniform01(s) * (hi - lo));
+    uint32_t n = (uint32_t)std::llround(nf);
+    n = std::min(std::max(n, n_min), n_max);
+    const int kind = (int)(seed & 1);
+    double param;
+    gc_status st;
+    if (kind == 0) {
+        param = 8.0 + 24.0 * uniform01(s);
+        uint64_t m = (uint64_t)std::llround((double)n * param / 2.0);
+        m = std::min<uint64_t>(m, (uint64_t)n * (n - 1) / 2);
+        st = gc_gen_er(n, m, seed, V, E);
+    } else {
+        param = 8.0;
+        st = gc_gen_rmat(n, param, 0.57, 0.19, 0.19, seed, V, E);
+    }
+    if (st != GC_OK) return st;
+    if (n_out) *n_out = n;
+    if (kind_out) *kind_out = kind;
+    if (param_out) *param_out = param;
+    return GC_OK;
+}
+
+gc_status gc_gen_mixed_batch(uint32_t G, uint64_t seed0, uint32_t n_min, uint32_t n_max, uint32_t **voff_out,
+                             uint32_t **V_out, uint32_t **E_out) {
+    if (!voff_out || !V_out || !E_out || n_min < 2 || n_max < n_min) return GC_ERR_INVALID;
+    std::vector<uint32_t *> Vs(G, nullptr), Es(G, nullptr);
+    std::vector<uint32_t> ns(G, 0);
+    int failed = 0;
+    // graphs in parallel; each generator's own parallel loops run single-threaded inside
+#pragma omp parallel for schedule(dynamic, 1) reduction(| : failed)
+    for (uint32_t i = 0; i < G; i++)
+        if (gc_gen_mixed(seed0 + i, n_min, n_max, &ns[i], nullptr, nullptr, &Vs[i], &Es[i]) != GC_OK) failed = 1;
+    auto release = [&]() {
+        for (uint32_t i = 0; i < G; i++) {
+            free(Vs[i]);
+            free(Es[i]);
+        }
+    };
+    if (failed) {
+        release();
+        return GC_ERR_NOMEM;
+    }
+    uint32_t *voff = (uint32_t *)malloc(sizeof(uint32_t) * ((size_t)G + 1));
+    std::vector<uint64_t> eoff((size_t)G + 1, 0);
+    if (!voff) {
+        release();
+        return GC_ERR_NOMEM;
+    }
+    uint64_t nv = 0;
+    voff[0] = 0;
+    for (uint32_t i = 0; i < G; i++) {
+        nv += ns[i];
+        eoff[i + 1] = eoff[i] + Vs[i][ns[i]];
+        if (nv >= 0xffffffffULL || eoff[i + 1] > 0xffffffffULL) {
+            release();
+            free(voff);
+            return GC_ERR_INVALID;
+        }
+        voff[i + 1] = (uint32_t)nv;
+    }
+    uint32_t *V = (uint32_t *)malloc(sizeof(uint32_t) * (nv + 1));
+    uint32_t *E = (uint32_t *)malloc(sizeof(uint32_t) * (eoff[G] ? eoff[G] : 1));
+    if (!V || !E) {
+        release();
+        free(voff);
+        free(V);
+        free(E);
+        return GC_ERR_NOMEM;
+    }
+#pragma omp parallel for schedule(dynamic, 1)
+    for (uint32_t i = 0; i < G; i++) {
+        for (uint32_t r = 0; r < ns[i]; r++) V[voff[i] + r] = (uint32_t)eoff[i] + Vs[i][r];
+        memcpy(E + eoff[i], Es[i], sizeof(uint32_t) * (eoff[i + 1] - eoff[i]));
+        free(Vs[i]);
+        free(Es[i]);
+        Vs[i] = Es[i] = nullptr;
+    }
+    V[nv] = (uint32_t)eoff[G];
+    *voff_out = voff;
     *V_out = V;
     *E_out = E;
     return GC_OK;

@@ -28,11 +28,19 @@ using namespace gc;
 
 enum : int { MODE_INPUT = 0, MODE_HIDDEN = 1, MODE_OUTPUT = 2 };
 
-__global__ void k_gnn_table0(const uint32_t *__restrict__ V, uint32_t N, float fmd, float2 *__restrict__ t01) {
+// In a segmented CSR the id feature is (local id) / (the graph's own N).
+__global__ void k_gnn_table0(const uint32_t *__restrict__ V, uint32_t N, float fmd, const uint32_t *__restrict__ voff,
+                             uint32_t nseg, float2 *__restrict__ t01) {
     for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < N; u += gridDim.x * blockDim.x) {
         uint32_t d = V[u + 1] - V[u];
+        uint32_t base = 0, n = N;
+        if (nseg) {
+            const uint32_t s = seg_of(voff, nseg, u);
+            base = __ldg(voff + s);
+            n = __ldg(voff + s + 1) - base;
+        }
         float deg_feat = __fdiv_rn(__uint2float_rn(d), fmd);
-        float id_feat = __double2float_rn(__ddiv_rn((double)u, (double)N));
+        float id_feat = __double2float_rn(__ddiv_rn((double)(u - base), (double)n));
         t01[u] = make_float2(deg_feat, id_feat);
     }
 }
@@ -444,9 +452,13 @@ gc_status launch_layer(gc_graph *g, const float *Wb, const float *x, float *y, c
     if (g->n_hubs) {
         constexpr int ROW = (MODE == MODE_INPUT) ? 2 : FEAT;
         const size_t smem = (size_t)HUB_STAGES * HUB_ROWS * ROW * sizeof(float);
-        if ((s = gc_check_cuda(ctx, cudaFuncSetAttribute(k_gnn_hub<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                         (int)smem), "hub smem")) != GC_OK)
-            return s;
+        if (!ctx->hub_smem_set[MODE]) {  // once per context: keeps the call out of captured sequences
+            if ((s = gc_check_cuda(ctx, cudaFuncSetAttribute(k_gnn_hub<MODE>,
+                                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                                   "hub smem")) != GC_OK)
+                return s;
+            ctx->hub_smem_set[MODE] = true;
+        }
         if (ctx->gnn_serial) side = ctx->stream;  // hubs first, then the bulk, on one stream
         if ((s = gc_check_cuda(ctx, cudaEventRecord(fork, ctx->stream), "fork")) != GC_OK) return s;
         if ((s = gc_check_cuda(ctx, cudaStreamWaitEvent(side, fork, 0), "fork")) != GC_OK) return s;
@@ -505,7 +517,8 @@ gc_status gc_priority_gnn(gc_graph *g, const gc_model *m) {
     }
     {
         ProfScope ps(ctx, "gnn_table0", ctx->stream);
-        k_gnn_table0<<<ctx->num_sms * 4, 256, 0, ctx->stream>>>(g->V, g->N, (float)m->md, g->t01);
+        k_gnn_table0<<<ctx->num_sms * 4, 256, 0, ctx->stream>>>(g->V, g->N, (float)m->md, g->seg_voff, g->n_seg,
+                                                                 g->t01);
     }
     ctx->launches++;
     if ((s = gc_check_launch(ctx, "gnn input table")) != GC_OK) return s;

@@ -9,7 +9,7 @@
 namespace {
 
 __global__ void k_degree_classes(const uint32_t *__restrict__ V, uint32_t N, uint32_t big_deg,
-                                 uint32_t chunk, uint32_t hub_deg, gc::DevState *st,
+                                 uint32_t chunk, uint32_t hub_deg, uint32_t warp_deg, gc::DevState *st,
                                  uint32_t *__restrict__ tasks, uint32_t task_cap,
                                  uint32_t *__restrict__ hubs, uint32_t hub_cap) {
     const uint32_t stride = gridDim.x * blockDim.x;
@@ -36,7 +36,7 @@ __global__ void k_degree_classes(const uint32_t *__restrict__ V, uint32_t N, uin
         if (d > hub_deg) {
             uint32_t at = atomicAdd(&st->count2, 1u);
             if (hubs && at < hub_cap) hubs[at] = u;
-        } else if (d > GC_GNN_WARP_DEGREE) {
+        } else if (d > warp_deg) {
             atomicAdd(&st->min_deg, 1u);  // counts the GNN warp tier
         }
     }
@@ -45,6 +45,20 @@ __global__ void k_degree_classes(const uint32_t *__restrict__ V, uint32_t N, uin
 __global__ void k_degree_keys(const uint32_t *__restrict__ V, uint32_t N, uint32_t *__restrict__ out) {
     for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < N; u += gridDim.x * blockDim.x)
         out[u] = V[u + 1] - V[u];
+}
+
+// Graph-major schedule keys: the warp tier first, then graph by graph (in order), then degree class
+// (bit length of the degree) descending.  The sort's ascending-id tie rule keeps each graph's
+// vertices of one class in id order.
+__global__ void k_segment_keys(const uint32_t *__restrict__ V, uint32_t N, const uint32_t *__restrict__ voff,
+                               uint32_t nseg, uint32_t warp_deg, uint32_t *__restrict__ out) {
+    for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < N; u += gridDim.x * blockDim.x) {
+        const uint32_t d = V[u + 1] - V[u];
+        const uint32_t s = nseg ? gc::seg_of(voff, nseg, u) : 0u;
+        const uint32_t cls = d ? 32u - (uint32_t)__clz(d) : 0u;  // 0 .. 32
+        const uint32_t rank = (nseg ? nseg - 1u - s : 0u);      // earlier graphs get larger keys
+        out[u] = (d > warp_deg ? 0x80000000u : 0u) | (rank << 6) | cls;
+    }
 }
 
 int bits_of(uint32_t x) {
@@ -80,8 +94,8 @@ gc_status gc_graph_prepare(gc_graph *g) {
     int grid = ctx->num_sms * 8;
     // pass 1: counts
     if ((s = gc_reset_state(ctx)) != GC_OK) return s;
-    k_degree_classes<<<grid, 256, 0, ctx->stream>>>(g->V, g->N, GC_GNN_HUB_DEGREE, GC_SPLIT_CHUNK,
-                                                    GC_GNN_HUB_DEGREE, ctx->dstate, nullptr, 0, nullptr, 0);
+    k_degree_classes<<<grid, 256, 0, ctx->stream>>>(g->V, g->N, g->hub_deg, GC_SPLIT_CHUNK, g->hub_deg,
+                                                    g->warp_deg, ctx->dstate, nullptr, 0, nullptr, 0);
     ctx->launches++;
     if ((s = gc_check_launch(ctx, "degree classes")) != GC_OK) return s;
     if ((s = gc_read_state(ctx)) != GC_OK) return s;
@@ -90,7 +104,7 @@ gc_status gc_graph_prepare(gc_graph *g) {
     g->n_wide = ctx->hstate->min_deg;
     // lists: the hub list and the degree order fit in cap_N; the task list grows when needed
     if (2 * (size_t)n_tasks > g->big_cap) {
-        if (g->big) cudaFree(g->big);
+        gc_dev_free(ctx, g->big);
         g->big = nullptr;
         if ((s = gc_alloc(ctx, &g->big, 2 * (size_t)n_tasks, "split task list")) != GC_OK) return s;
         g->big_cap = 2 * (size_t)n_tasks;
@@ -98,9 +112,8 @@ gc_status gc_graph_prepare(gc_graph *g) {
     if ((s = gc_alloc(ctx, &g->hubs, (size_t)g->cap_N, "hub list")) != GC_OK) return s;
     // pass 2: fill
     if ((s = gc_reset_state(ctx)) != GC_OK) return s;
-    k_degree_classes<<<grid, 256, 0, ctx->stream>>>(g->V, g->N, GC_GNN_HUB_DEGREE, GC_SPLIT_CHUNK,
-                                                    GC_GNN_HUB_DEGREE, ctx->dstate, g->big, n_tasks,
-                                                    g->hubs, n_hubs);
+    k_degree_classes<<<grid, 256, 0, ctx->stream>>>(g->V, g->N, g->hub_deg, GC_SPLIT_CHUNK, g->hub_deg,
+                                                    g->warp_deg, ctx->dstate, g->big, n_tasks, g->hubs, n_hubs);
     ctx->launches++;
     if ((s = gc_check_launch(ctx, "degree classes")) != GC_OK) return s;
     if ((s = gc_read_state(ctx)) != GC_OK) return s;
@@ -117,7 +130,7 @@ gc_status gc_graph_prepare(gc_graph *g) {
         s = gc_check_cuda(ctx, cudaMemcpyAsync(hp.data(), pairs, 8 * (size_t)n_hubs, cudaMemcpyDeviceToHost,
                                                ctx->stream), "hub degrees");
         if (s == GC_OK) s = gc_check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "hub degrees");
-        cudaFree(pairs);
+        gc_dev_free(ctx, pairs);
         if (s != GC_OK) return s;
         std::vector<uint32_t> idx(n_hubs);
         for (uint32_t i = 0; i < n_hubs; i++) idx[i] = i;
@@ -131,15 +144,26 @@ gc_status gc_graph_prepare(gc_graph *g) {
             return s;
         if ((s = gc_check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "hub list")) != GC_OK) return s;
     }
-    // GNN schedule: every non-hub vertex by descending degree (ties by id), so that the vertices a
-    // warp handles together have nearly equal neighbour counts.  The key buffer is free here (no
+    // GNN schedule.  By degree: every non-hub vertex by descending degree (ties by id), so that the
+    // vertices a warp handles together have nearly equal neighbour counts.  Graph-major (segmented
+    // CSRs): the warp tier, then graph by graph, by degree class inside, so that one graph's
+    // feature rows stay in L2 while its vertices are processed.  The key buffer is free here (no
     // priorities exist right after an upload).
     if ((s = gc_alloc(ctx, &g->vorder, (size_t)g->cap_N, "degree order")) != GC_OK) return s;
-    k_degree_keys<<<ctx->num_sms * 4, 256, 0, ctx->stream>>>(g->V, g->N, g->key);
+    int key_bits;
+    if (g->sched == GC_SCHEDULE_SEGMENT) {
+        if (g->n_seg >= (1u << 25)) return gc_fail(ctx, GC_ERR_INVALID, "graph-major schedule: too many graphs");
+        k_segment_keys<<<ctx->num_sms * 4, 256, 0, ctx->stream>>>(g->V, g->N, g->seg_voff, g->n_seg, g->warp_deg,
+                                                                  g->key);
+        key_bits = 32;
+    } else {
+        k_degree_keys<<<ctx->num_sms * 4, 256, 0, ctx->stream>>>(g->V, g->N, g->key);
+        const uint32_t top = g->max_deg < g->hub_deg ? g->max_deg : g->hub_deg;
+        key_bits = bits_of(top);
+    }
     ctx->launches++;
     if ((s = gc_reset_state(ctx)) != GC_OK) return s;
-    const uint32_t top = g->max_deg < GC_GNN_HUB_DEGREE ? g->max_deg : GC_GNN_HUB_DEGREE;
-    if ((s = gc_sort_vertices(g, g->key, bits_of(top), SORT_KEEP_DEG_AT_MOST, GC_GNN_HUB_DEGREE, g->vorder,
+    if ((s = gc_sort_vertices(g, g->key, key_bits, SORT_KEEP_DEG_AT_MOST, g->hub_deg, g->vorder,
                               &ctx->dstate->count)) != GC_OK)
         return s;
     if ((s = gc_read_state(ctx)) != GC_OK) return s;

@@ -378,26 +378,90 @@ __global__ void __launch_bounds__(COLOR_THREADS, 6) k_jp_big_leaves(const uint32
     }
 }
 
-// One warp per vertex: colors positive and no monochrome edge; largest color.
-__global__ void k_validate(const uint32_t *__restrict__ V, const uint32_t *__restrict__ E, uint32_t N,
-                           const int *__restrict__ color, DevState *st) {
-    const int lane = threadIdx.x & 31;
+// Coloring statistics: every color positive, no monochrome edge, largest color -- per segment of
+// a segmented CSR (stat[2s] largest color, stat[2s + 1] improper flag), or for the whole graph
+// into DevState when nseg = 0.  Work items, heaviest first, one warp each: the hubs' split tasks
+// (GC_SPLIT_CHUNK edges), the warp-tier vertices (vorder[0, n_wide)), then blocks of 32
+// consecutive vertices, which a warp takes 8 at a time with 4 lanes per vertex.  Vertices above
+// warp_deg have their edges checked by the first two kinds of item only.
+__device__ __forceinline__ void stats_record(int *stat, DevState *st, uint32_t nseg, uint32_t s, int cmax, bool bad) {
+    if (nseg) {
+        atomicMax(stat + 2 * s, cmax);
+        if (bad) atomicOr(stat + 2 * s + 1, 1);
+    } else {
+        atomicMax(&st->max_color, (unsigned int)max(cmax, 0));
+        if (bad) atomicOr(&st->invalid, 1u);
+    }
+}
+
+__global__ void __launch_bounds__(256) k_color_stats(const uint32_t *__restrict__ V, const uint32_t *__restrict__ E,
+                                                     const int *__restrict__ color, const uint32_t *__restrict__ vorder,
+                                                     uint32_t n_wide, const uint32_t *__restrict__ tasks,
+                                                     uint32_t n_tasks, const uint32_t *__restrict__ voff,
+                                                     uint32_t nseg, uint32_t N, uint32_t warp_deg, int *stat,
+                                                     DevState *st) {
+    const int lane = threadIdx.x & 31, q = lane & 3;
     const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-    int cmax = 0;
-    bool bad = false;
-    for (uint32_t u = warp; u < N; u += nwarps) {
-        const int cu = color[u];
-        if (cu <= 0) bad = true;
-        if (cu > cmax) cmax = cu;
-        for (uint32_t j = V[u] + lane; j < V[u + 1]; j += 32)
-            if (color[ld_stream(E + j)] == cu) bad = true;
-    }
-    bad = __any_sync(0xffffffffu, bad);
-    cmax = __reduce_max_sync(0xffffffffu, cmax);
-    if (lane == 0) {
-        if (bad) atomicOr(&st->invalid, 1u);
-        atomicMax(&st->max_color, (unsigned int)cmax);
+    const uint32_t n_blocks = (N + 31) / 32;
+    const uint32_t n_items = n_tasks + n_wide + n_blocks;
+    for (uint32_t it = warp; it < n_items; it += nwarps) {
+        if (it < n_tasks + n_wide) {
+            uint32_t u, b, e;
+            if (it < n_tasks) {
+                u = tasks[2 * it];
+                b = tasks[2 * it + 1];
+                e = min(V[u + 1], b + GC_SPLIT_CHUNK);
+            } else {
+                u = vorder[it - n_tasks];
+                b = V[u];
+                e = V[u + 1];
+            }
+            const int cu = color[u];
+            bool hit = false;
+            for (uint32_t j = b + lane; j < e; j += 32) hit |= color[ld_stream(E + j)] == cu;
+            if (__any_sync(0xffffffffu, hit) && lane == 0)
+                stats_record(stat, st, nseg, nseg ? seg_of(voff, nseg, u) : 0u, 0, true);
+            continue;
+        }
+        const uint32_t base = (it - n_tasks - n_wide) * 32;
+        const uint32_t last = min(base + 31, N - 1);
+        const uint32_t s0 = nseg ? seg_of(voff, nseg, base) : 0u;
+        const bool uniform = !nseg || last < __ldg(voff + s0 + 1);
+        int bmax = 0;
+        bool bbad = false;
+#pragma unroll 1
+        for (int sub = 0; sub < 4; sub++) {
+            const uint32_t u = base + 8 * sub + (lane >> 2);
+            const bool valid = u < N;
+            const uint32_t b = valid ? V[u] : 0u, e = valid ? V[u + 1] : 0u;
+            const int cu = valid ? color[u] : 0;
+            bool bad = valid && cu <= 0;
+            if (valid && e - b <= warp_deg) {
+                uint32_t j = b + q;
+                for (; j + 12 < e; j += 16) {
+                    const uint32_t v0 = ld_stream(E + j), v1 = ld_stream(E + j + 4);
+                    const uint32_t v2 = ld_stream(E + j + 8), v3 = ld_stream(E + j + 12);
+                    bad |= (color[v0] == cu) | (color[v1] == cu) | (color[v2] == cu) | (color[v3] == cu);
+                }
+                for (; j < e; j += 4) bad |= color[ld_stream(E + j)] == cu;
+            }
+            if (uniform) {
+                bmax = max(bmax, cu);
+                bbad |= bad;
+            } else {
+                const uint32_t s = valid ? seg_of(voff, nseg, u) : 0xffffffffu;
+                const unsigned int peers = __match_any_sync(0xffffffffu, s);
+                const int m = __reduce_max_sync(peers, cu);
+                const unsigned int anybad = __reduce_or_sync(peers, bad ? 1u : 0u);
+                if (valid && lane == __ffs(peers) - 1) stats_record(stat, st, nseg, s, m, anybad != 0);
+            }
+        }
+        if (uniform) {
+            const int m = __reduce_max_sync(0xffffffffu, bmax);
+            const unsigned int anybad = __reduce_or_sync(0xffffffffu, bbad ? 1u : 0u);
+            if (lane == 0) stats_record(stat, st, nseg, s0, m, anybad != 0);
+        }
     }
 }
 
@@ -426,7 +490,10 @@ gc_status gc_jp_color(gc_graph *g) {
     gc_ctx *ctx = g->ctx;
     gc_status s;
     const uint32_t N = g->N;
-    if (N == 0) return GC_OK;
+    if (N == 0) {
+        g->has_colors = true;
+        return GC_OK;
+    }
     if ((s = gc_alloc(ctx, &g->P, g->cap_M, "predecessor lists")) != GC_OK) return s;
     if ((s = gc_alloc(ctx, &g->pc, g->cap_N, "predecessor counts")) != GC_OK) return s;
     if ((s = gc_alloc(ctx, &g->order, g->cap_N, "ticket order")) != GC_OK) return s;
@@ -460,21 +527,24 @@ gc_status gc_jp_color(gc_graph *g) {
     if ((s = gc_sort_order_bits(g, bits, true, &ctx->dstate->ordered)) != GC_OK) return s;
 
     // 3. ordered coloring
-    int &blocks = ctx->color_blocks_per_sm;
-    if (!blocks) {
-        if ((s = gc_check_cuda(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_jp_color,
+    int &occupancy = ctx->color_blocks_per_sm;
+    if (!occupancy) {
+        if ((s = gc_check_cuda(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occupancy, k_jp_color,
                                                                                   COLOR_WARPS_PER_CTA * 32, 0),
                                "occupancy")) != GC_OK)
             return s;
-        if (blocks < 1) blocks = 1;
-        if (ctx->jp_ctas_per_sm > 0 && ctx->jp_ctas_per_sm < blocks) blocks = ctx->jp_ctas_per_sm;
+        if (occupancy < 1) occupancy = 1;
     }
+    const int want = g->jp_ctas > 0 ? g->jp_ctas : ctx->jp_ctas_per_sm;
+    const int blocks = (want > 0 && want < occupancy) ? want : occupancy;
+    const unsigned int tight = g->jp_ctas > 0 ? g->jp_tight : ctx->jp_tight;
+    const unsigned int nap = g->jp_ctas > 0 ? g->jp_nap : ctx->jp_nap;
     k_reset_ticket<<<1, 1, 0, ctx->stream>>>(ctx->dstate);
     ctx->launches++;
     {
         ProfScope ps(ctx, "jp_color", ctx->stream);
         k_jp_color<<<ctx->num_sms * blocks, COLOR_WARPS_PER_CTA * 32, 0, ctx->stream>>>(
-            g->V, g->P, g->pc, g->order, g->color, ctx->dstate, ctx->spin_limit, ctx->jp_tight, ctx->jp_nap);
+            g->V, g->P, g->pc, g->order, g->color, ctx->dstate, ctx->spin_limit, tight, nap);
         ctx->launches++;
     }
     // 4. leaves
@@ -500,6 +570,20 @@ gc_status gc_keys_from_colors(gc_graph *g) {
     return gc_check_launch(ctx, "culberson keys");
 }
 
+namespace {
+
+gc_status launch_color_stats(gc_graph *g, int *stat, uint32_t nseg) {
+    gc_ctx *ctx = g->ctx;
+    ProfScope ps(ctx, "color_stats", ctx->stream);
+    k_color_stats<<<ctx->num_sms * 8, 256, 0, ctx->stream>>>(g->V, g->E, g->color, g->vorder, g->n_wide, g->big,
+                                                             g->n_big_tasks, g->seg_voff, nseg, g->N, g->warp_deg,
+                                                             stat, ctx->dstate);
+    ctx->launches++;
+    return gc_check_launch(ctx, "color statistics");
+}
+
+}  // namespace
+
 gc_status gc_validate_device(gc_graph *g, int *max_color) {
     gc_ctx *ctx = g->ctx;
     gc_status s;
@@ -508,15 +592,21 @@ gc_status gc_validate_device(gc_graph *g, int *max_color) {
         return GC_OK;
     }
     if ((s = gc_reset_state(ctx)) != GC_OK) return s;
-    {
-        ProfScope ps(ctx, "validate", ctx->stream);
-        k_validate<<<ctx->num_sms * 8, 256, 0, ctx->stream>>>(g->V, g->E, g->N, g->color, ctx->dstate);
-    }
-    ctx->launches++;
-    if ((s = gc_check_launch(ctx, "validate")) != GC_OK) return s;
+    if ((s = launch_color_stats(g, nullptr, 0)) != GC_OK) return s;
     if ((s = gc_read_state(ctx)) != GC_OK) return s;
     int C = (int)ctx->hstate->max_color;
     if (C < 1) C = 1;
     *max_color = ctx->hstate->invalid ? 0 : C;
     return GC_OK;
+}
+
+gc_status gc_segment_stats(gc_graph *g) {
+    gc_ctx *ctx = g->ctx;
+    gc_status s;
+    if (!g->n_seg) return GC_OK;
+    if ((s = gc_check_cuda(ctx, cudaMemsetAsync(g->seg_stat, 0, sizeof(int32_t) * 2 * g->n_seg, ctx->stream),
+                           "segment statistics")) != GC_OK)
+        return s;
+    if (g->N == 0) return GC_OK;
+    return launch_color_stats(g, g->seg_stat, g->n_seg);
 }

@@ -12,11 +12,13 @@
 namespace {
 using gc::ld_stream;
 
-__global__ void k_simple_keys(const uint32_t *__restrict__ V, uint32_t N, int h, uint32_t *__restrict__ key) {
+// FF in a segmented CSR: N - u with the graph's own N and local u, i.e. (end of u's graph) - u.
+__global__ void k_simple_keys(const uint32_t *__restrict__ V, uint32_t N, int h, const uint32_t *__restrict__ voff,
+                              uint32_t nseg, uint32_t *__restrict__ key) {
     for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < N; u += gridDim.x * blockDim.x) {
         uint32_t k;
         if (h == GC_FF) {
-            k = N - u;
+            k = (nseg ? __ldg(voff + gc::seg_of(voff, nseg, u) + 1) : N) - u;
         } else {
             uint32_t d = V[u + 1] - V[u];
             k = (h == GC_LF) ? d : (d ? 32u - (uint32_t)__clz(d) : 0u);
@@ -163,7 +165,7 @@ gc_status gc_priority_simple(gc_graph *g, gc_heuristic h) {
     if (g->N == 0) return GC_OK;
     int grid = ctx->num_sms * 4;
     ProfScope ps(ctx, "priority_keys", ctx->stream);
-    k_simple_keys<<<grid, 256, 0, ctx->stream>>>(g->V, g->N, (int)h, g->key);
+    k_simple_keys<<<grid, 256, 0, ctx->stream>>>(g->V, g->N, (int)h, g->seg_voff, g->n_seg, g->key);
     ctx->launches++;
     return gc_check_launch(ctx, "priority keys");
 }

@@ -194,7 +194,7 @@ gc_status gc_sort_vertices(gc_graph *g, const uint32_t *keys, int key_bits, int 
     // tile counts, then per pass: digit totals and digit bases (4 passes at most)
     const size_t hist_words = (size_t)RADIX * ntiles + 4 * 2 * RADIX;
     if (g->sort_hist_cap < hist_words) {
-        if (g->sort_hist) cudaFree(g->sort_hist);
+        gc_dev_free(ctx, g->sort_hist);
         g->sort_hist = nullptr;
         if ((s = gc_alloc(ctx, &g->sort_hist, hist_words, "sort histogram")) != GC_OK) return s;
         g->sort_hist_cap = (uint32_t)hist_words;

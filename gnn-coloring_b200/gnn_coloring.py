@@ -97,6 +97,41 @@ _sig("gc_gen_rmat", C.c_int, C.c_uint32, C.c_double, C.c_double, C.c_double, C.c
      C.POINTER(u32p), C.POINTER(u32p))
 _sig("gc_gen_rgg2d", C.c_int, C.c_uint32, C.c_double, C.c_uint64, C.POINTER(u32p), C.POINTER(u32p))
 _sig("gc_gen_stencil27", C.c_int, C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(u32p), C.POINTER(u32p))
+_sig("gc_gen_mixed", C.c_int, C.c_uint64, C.c_uint32, C.c_uint32, u32p, C.POINTER(C.c_int), f64p,
+     C.POINTER(u32p), C.POINTER(u32p))
+_sig("gc_gen_mixed_batch", C.c_int, C.c_uint32, C.c_uint64, C.c_uint32, C.c_uint32, C.POINTER(u32p),
+     C.POINTER(u32p), C.POINTER(u32p))
+
+
+class Tuning(C.Structure):
+    """gc_tuning: what the batch autotuner may change (never a color or priority bit)."""
+    _fields_ = [("warp_degree", C.c_uint32), ("hub_degree", C.c_uint32), ("schedule", C.c_int),
+                ("jp_ctas_per_sm", C.c_int), ("jp_tight", C.c_uint), ("jp_nap", C.c_uint)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+GC_SCHEDULE_DEGREE, GC_SCHEDULE_SEGMENT = 0, 1
+SCHEDULES = {"degree": GC_SCHEDULE_DEGREE, "segment": GC_SCHEDULE_SEGMENT}
+
+# batches
+_sig("gc_batch_upload", C.c_int, vp, C.c_uint32, u32p, u32p, u32p, C.POINTER(vp))
+_sig("gc_batch_upload_graphs", C.c_int, vp, C.c_uint32, u32p, C.POINTER(u32p), C.POINTER(u32p), C.POINTER(vp))
+_sig("gc_batch_create", C.c_int, vp, C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(vp))
+_sig("gc_batch_reupload_graphs", C.c_int, vp, vp, C.c_uint32, u32p, C.POINTER(u32p), C.POINTER(u32p))
+_sig("gc_batch_free", None, vp)
+_sig("gc_batch_num_graphs", C.c_uint32, vp)
+_sig("gc_batch_num_vertices", C.c_uint32, vp)
+_sig("gc_batch_num_edges", C.c_uint32, vp)
+_sig("gc_batch_device_bytes", C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int)
+_sig("gc_batch_graph", vp, vp)
+_sig("gc_batch_color", C.c_int, vp, vp, C.c_int, vp, C.c_int, i32p)
+_sig("gc_batch_download_colors", C.c_int, vp, vp, i32p)
+_sig("gc_batch_autotune", C.c_int, vp, vp, C.c_int, vp, C.c_int, C.c_int, C.POINTER(Tuning), f64p)
+_sig("gc_batch_set_tuning", C.c_int, vp, vp, C.POINTER(Tuning))
+_sig("gc_batch_get_tuning", C.c_int, vp, C.POINTER(Tuning))
+_sig("gc_tuning_default", None, C.POINTER(Tuning))
 
 
 def _ptr(a: np.ndarray, t):
@@ -155,6 +190,36 @@ def csr_from_pairs(n: int, I: np.ndarray, J: np.ndarray):
     _check(lib.gc_csr_from_pairs(n, len(I), _ptr(I, u32p), _ptr(J, u32p), C.byref(Vp), C.byref(Ep)),
            what="csr_from_pairs")
     return _take_csr(n, Vp, Ep)
+
+
+def gen_mixed(seed: int, n_min: int = 1000, n_max: int = 200000):
+    """One graph of a mixed batch (gc_gen_mixed): (N, V, E, kind, param), kind 0 = ER, 1 = R-MAT."""
+    Vp, Ep = u32p(), u32p()
+    n, kind, param = C.c_uint32(), C.c_int(), C.c_double()
+    _check(lib.gc_gen_mixed(seed, n_min, n_max, C.byref(n), C.byref(kind), C.byref(param), C.byref(Vp), C.byref(Ep)),
+           what="gen_mixed")
+    N, V, E = _take_csr(n.value, Vp, Ep)
+    return N, V, E, kind.value, param.value
+
+
+def gen_mixed_batch(G: int, seed0: int, n_min: int = 1000, n_max: int = 200000):
+    """G mixed graphs as one segmented CSR: (voff, V with global row offsets, E with local ids)."""
+    Op, Vp, Ep = u32p(), u32p(), u32p()
+    _check(lib.gc_gen_mixed_batch(G, seed0, n_min, n_max, C.byref(Op), C.byref(Vp), C.byref(Ep)),
+           what="gen_mixed_batch")
+    voff = np.ctypeslib.as_array(Op, shape=(G + 1,)).copy()
+    N = int(voff[G])
+    _, V, E = _take_csr(N, Vp, Ep)
+    lib.gc_host_free(C.cast(Op, vp))
+    return voff, V, E
+
+
+def split_batch(voff: np.ndarray, V: np.ndarray, E: np.ndarray, g: int):
+    """Graph g of a segmented CSR as its own (N, V, E) with local ids."""
+    a, b = int(voff[g]), int(voff[g + 1])
+    Vg = (V[a:b + 1] - V[a]).astype(np.uint32)
+    Eg = E[int(V[a]):int(V[b])].copy()
+    return b - a, Vg, Eg
 
 
 def mtx_read(path: str):
@@ -359,6 +424,111 @@ class Graph:
             self.close()
         except Exception:
             pass
+
+
+class Batch:
+    """G independent graphs in one segmented CSR on the device (gc_batch).
+
+    Build it from a segmented CSR (``voff``, global row offsets ``V``, local ids ``E``) or from a list
+    of (N, V, E) graphs.  ``color()`` runs priorities + JP (+ Culberson) for all graphs in one CUDA
+    graph launch and returns each graph's color count."""
+
+    def __init__(self, ctx: Context, voff: np.ndarray = None, V: np.ndarray = None, E: np.ndarray = None,
+                 graphs=None):
+        self.ctx = ctx
+        h = vp()
+        if graphs is not None:
+            self._keep = [(np.ascontiguousarray(Vg, np.uint32),
+                           np.ascontiguousarray(Eg, np.uint32) if len(Eg) else np.zeros(1, np.uint32))
+                          for _, Vg, Eg in graphs]
+            G = len(graphs)
+            ns = np.array([int(n) for n, _, _ in graphs], np.uint32)
+            Vs = (u32p * max(G, 1))(*[_ptr(v, u32p) for v, _ in self._keep])
+            Es = (u32p * max(G, 1))(*[_ptr(e, u32p) for _, e in self._keep])
+            ctx.check(lib.gc_batch_upload_graphs(ctx.h, G, _ptr(ns, u32p), Vs, Es, C.byref(h)), "batch upload")
+            self.voff = np.concatenate([[0], np.cumsum(ns, dtype=np.uint64)]).astype(np.uint32)
+            self._keep = None
+        else:
+            self.voff = np.ascontiguousarray(voff, np.uint32)
+            Vc = np.ascontiguousarray(V, np.uint32)
+            Ec = np.ascontiguousarray(E, np.uint32) if len(E) else np.zeros(1, np.uint32)
+            G = len(self.voff) - 1
+            ctx.check(lib.gc_batch_upload(ctx.h, G, _ptr(self.voff, u32p), _ptr(Vc, u32p), _ptr(Ec, u32p),
+                                          C.byref(h)), "batch upload")
+        self.h = h
+        self.G = G
+        _live_objects.add(self)
+
+    @property
+    def N(self) -> int:
+        return int(lib.gc_batch_num_vertices(self.h))
+
+    @property
+    def M(self) -> int:
+        return int(lib.gc_batch_num_edges(self.h))
+
+    def color(self, heuristic, model: Optional[Model] = None, recolor: int = 0) -> np.ndarray:
+        h = HEURISTICS[heuristic] if isinstance(heuristic, str) else int(heuristic)
+        out = np.zeros(max(self.G, 1), np.int32)
+        self.ctx.check(lib.gc_batch_color(self.ctx.h, self.h, h, model.h if model else None, recolor,
+                                          _ptr(out, i32p)), "batch color")
+        return out[: self.G]
+
+    def colors(self) -> np.ndarray:
+        out = np.empty(max(self.N, 1), np.int32)
+        self.ctx.check(lib.gc_batch_download_colors(self.ctx.h, self.h, _ptr(out, i32p)), "batch colors")
+        return out[: self.N]
+
+    def graph_colors(self, g: int, all_colors: Optional[np.ndarray] = None) -> np.ndarray:
+        c = self.colors() if all_colors is None else all_colors
+        return c[int(self.voff[g]):int(self.voff[g + 1])]
+
+    def priorities(self) -> np.ndarray:
+        """Keys of all vertices as doubles (the union graph's gc_download_priority)."""
+        out = np.empty(max(self.N, 1), np.float64)
+        gh = lib.gc_batch_graph(self.h)
+        self.ctx.check(lib.gc_download_priority(self.ctx.h, gh, _ptr(out, f64p)), "batch priorities")
+        return out[: self.N]
+
+    def autotune(self, heuristic, model: Optional[Model] = None, recolor: int = 0, effort: int = 1):
+        h = HEURISTICS[heuristic] if isinstance(heuristic, str) else int(heuristic)
+        t = Tuning()
+        ms = C.c_double(0.0)
+        self.ctx.check(lib.gc_batch_autotune(self.ctx.h, self.h, h, model.h if model else None, recolor, effort,
+                                             C.byref(t), C.byref(ms)), "autotune")
+        return t, ms.value
+
+    @property
+    def tuning(self) -> Tuning:
+        t = Tuning()
+        _check(lib.gc_batch_get_tuning(self.h, C.byref(t)), what="get tuning")
+        return t
+
+    @tuning.setter
+    def tuning(self, t: Tuning):
+        self.ctx.check(lib.gc_batch_set_tuning(self.ctx.h, self.h, C.byref(t)), "set tuning")
+
+    def close(self):
+        if self.h:
+            lib.gc_batch_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def default_tuning() -> Tuning:
+    t = Tuning()
+    lib.gc_tuning_default(C.byref(t))
+    return t
+
+
+def batch_device_bytes(G: int, N: int, M: int, heuristic) -> int:
+    h = HEURISTICS[heuristic] if isinstance(heuristic, str) else int(heuristic)
+    return int(lib.gc_batch_device_bytes(G, N, M, h))
 
 
 # ---- the reference-named drop-in functions ------------------------------------------------------

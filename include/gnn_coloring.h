@@ -160,6 +160,79 @@ gc_status gc_download_priority(gc_ctx *ctx, gc_graph *g, double *p);
 gc_status gc_gnn_priority_noalloc(uint32_t N, const uint32_t *dV, const uint32_t *dE, int params, int md,
                                   const float *dparam, float *dp, void *stream);
 
+/* ---- batches: many independent graphs in one segmented CSR ---------------------------------- */
+
+/* No counterpart in the reference, whose runner colors one graph per process (src/runner.c:105-153).
+ *
+ * A batch holds G graphs as one segmented CSR in device memory.  Graph g owns the global vertex
+ * range [voff[g], voff[g+1]); V holds global row offsets (voff[G] + 1 entries, V[0] = 0), and E
+ * holds each graph's LOCAL neighbour ids (0 .. n_g - 1), as a concatenation of G ordinary CSRs
+ * would.  Every graph's priorities, colors and color count equal those of the same graph colored
+ * alone by gc_priority + gc_color: the segments share no edge, ties still break by id inside a
+ * graph, FF keys and the GNN id feature use the graph's own n and local ids.  SL and SLL are not
+ * offered on batches (their peeling thresholds are per graph; color such graphs one at a time). */
+typedef struct gc_batch gc_batch;
+
+/* Vertex schedules of the split and GNN kernels. */
+typedef enum gc_schedule {
+    GC_SCHEDULE_DEGREE = 0,  /* all vertices by descending degree: even work per warp on skewed graphs */
+    GC_SCHEDULE_SEGMENT = 1  /* graph by graph, by degree class inside: one graph's rows stay in L2 */
+} gc_schedule;
+
+/* What an autotuner may change; none of it changes a single color or priority bit. */
+typedef struct gc_tuning {
+    uint32_t warp_degree;   /* above this many neighbours a vertex gets a whole warp (else 4 lanes) */
+    uint32_t hub_degree;    /* above this many neighbours a vertex gets a whole CTA (GNN) or split tasks */
+    int schedule;           /* gc_schedule */
+    int jp_ctas_per_sm;     /* resident CTAs per SM of the ordered coloring kernel */
+    unsigned int jp_tight;  /* polling rounds before a coloring warp starts to sleep */
+    unsigned int jp_nap;    /* first sleep of a coloring warp (ns) */
+} gc_tuning;
+
+/* Uploads G graphs given as one segmented CSR (layout above). */
+gc_status gc_batch_upload(gc_ctx *ctx, uint32_t G, const uint32_t *voff, const uint32_t *V, const uint32_t *E,
+                          gc_batch **b);
+/* Uploads G separate host CSRs: graph g has n[g] vertices, row offsets Vs[g] (n[g] + 1 entries
+ * from 0) and local neighbour ids Es[g].  Pinned host memory makes the copies asynchronous. */
+gc_status gc_batch_upload_graphs(gc_ctx *ctx, uint32_t G, const uint32_t *n, const uint32_t *const *Vs,
+                                 const uint32_t *const *Es, gc_batch **b);
+/* An empty batch with room for cap_G graphs, cap_N vertices and cap_M directed edges, refilled by
+ * gc_batch_reupload_graphs without new device allocations. */
+gc_status gc_batch_create(gc_ctx *ctx, uint32_t cap_G, uint32_t cap_N, uint32_t cap_M, gc_batch **b);
+gc_status gc_batch_reupload_graphs(gc_ctx *ctx, gc_batch *b, uint32_t G, const uint32_t *n,
+                                   const uint32_t *const *Vs, const uint32_t *const *Es);
+void gc_batch_free(gc_batch *b);
+uint32_t gc_batch_num_graphs(const gc_batch *b);
+uint32_t gc_batch_num_vertices(const gc_batch *b);
+uint32_t gc_batch_num_edges(const gc_batch *b);
+/* Device bytes a batch (or a single graph: G = 1) of this size holds once colored with heuristic
+ * h: the figure admission control charges. */
+uint64_t gc_batch_device_bytes(uint32_t G, uint32_t N, uint32_t M, gc_heuristic h);
+/* The union of the batch's graphs as one gc_graph (global ids), for gc_download_priority,
+ * gc_download_colors and gc_validate over all graphs at once.  Owned by the batch. */
+gc_graph *gc_batch_graph(gc_batch *b);
+
+/* Priorities by heuristic h (GC_FF, GC_LF, GC_LLF or GC_GNN), Jones-Plassmann, then `recolor`
+ * Culberson iterations, for every graph of the batch.  The first call for a given (h, model,
+ * recolor) runs the stages directly and captures them into a CUDA graph; later calls replay that
+ * graph: one launch for all stages of all graphs.  colors (host, G entries, may be NULL) receives
+ * each graph's color count as validate_coloring_par reports it: 0 for an improper coloring. */
+gc_status gc_batch_color(gc_ctx *ctx, gc_batch *b, gc_heuristic h, const gc_model *model, int recolor,
+                         int32_t *colors);
+/* Colors of all vertices, graph by graph (voff[G] entries, local order inside each graph). */
+gc_status gc_batch_download_colors(gc_ctx *ctx, gc_batch *b, int32_t *color);
+
+/* Measures candidate tunings on this batch (each one a full gc_batch_color pass, timed with CUDA
+ * events) and keeps the fastest; `effort` 0 tries the tier thresholds only, 1 also the schedule and
+ * the coloring-kernel settings, 2 a wider grid.  *best (may be NULL) receives the tuning kept and
+ * *best_ms its time per pass. */
+gc_status gc_batch_autotune(gc_ctx *ctx, gc_batch *b, gc_heuristic h, const gc_model *model, int recolor,
+                            int effort, gc_tuning *best, double *best_ms);
+gc_status gc_batch_set_tuning(gc_ctx *ctx, gc_batch *b, const gc_tuning *t);
+gc_status gc_batch_get_tuning(const gc_batch *b, gc_tuning *t);
+/* The library's default tuning. */
+void gc_tuning_default(gc_tuning *t);
+
 /* ---- host-side graph preparation (no device involved) --------------------------------------- */
 
 /* Reads a Matrix Market file into a simple, symmetric, sorted CSR with the reference's rules:
@@ -186,6 +259,18 @@ gc_status gc_gen_rmat(uint32_t n, double ef, double a, double b, double c, uint6
 gc_status gc_gen_rgg2d(uint32_t n, double radius, uint64_t seed, uint32_t **V, uint32_t **E);
 /* 3D 27-point stencil on an nx * ny * nz grid (all 26 neighbours at Chebyshev distance 1). */
 gc_status gc_gen_stencil27(uint32_t nx, uint32_t ny, uint32_t nz, uint32_t **V, uint32_t **E);
+/* One graph of a mixed batch, drawn from `seed` alone: n log-uniform in [n_min, n_max] (rounded);
+ * even `seed`: Erdos-Renyi with average degree d uniform in [8, 32] (m = round(n d / 2) pairs);
+ * odd `seed`: R-MAT with edge factor 8 and (a, b, c) = (0.57, 0.19, 0.19) over 2^ceil(log2 n)
+ * ids, samples with an endpoint >= n dropped.  *kind is 0 for ER, 1 for R-MAT; *param the ER
+ * degree or the R-MAT edge factor. */
+gc_status gc_gen_mixed(uint64_t seed, uint32_t n_min, uint32_t n_max, uint32_t *n, int *kind, double *param,
+                       uint32_t **V, uint32_t **E);
+/* G graphs of gc_gen_mixed with seeds seed0 .. seed0 + G - 1, generated in parallel, as one
+ * segmented CSR (the layout of gc_batch_upload): voff (G + 1), V (voff[G] + 1, global row
+ * offsets), E (local ids).  All three malloc'd. */
+gc_status gc_gen_mixed_batch(uint32_t G, uint64_t seed0, uint32_t n_min, uint32_t n_max, uint32_t **voff,
+                             uint32_t **V, uint32_t **E);
 
 #ifdef __cplusplus
 }
