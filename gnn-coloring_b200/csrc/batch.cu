@@ -446,6 +446,34 @@ gc_status gc_batch_upload(gc_ctx *ctx, uint32_t G, const uint32_t *voff, const u
     return GC_OK;
 }
 
+gc_status gc_batch_reupload(gc_ctx *ctx, gc_batch *b, uint32_t G, const uint32_t *voff, const uint32_t *V,
+                            const uint32_t *E) {
+    if (!ctx || !b || b->ctx != ctx || !voff || !V) return GC_ERR_INVALID;
+    DeviceGuard dg(ctx);
+    if (voff[0] != 0) return gc_fail(ctx, GC_ERR_INVALID, "voff[0] must be 0");
+    for (uint32_t i = 0; i < G; i++)
+        if (voff[i + 1] < voff[i]) return gc_fail(ctx, GC_ERR_INVALID, "voff not monotone");
+    const uint32_t N = voff[G];
+    if (V[0] != 0) return gc_fail(ctx, GC_ERR_INVALID, "V[0] must be 0");
+    const uint32_t M = V[N];
+    if (M && !E) return gc_fail(ctx, GC_ERR_INVALID, "E is NULL");
+    gc_graph *g = b->g;
+    if (N > g->cap_N || M > g->cap_M || G > b->cap_G)
+        return gc_fail(ctx, GC_ERR_INVALID, "batch exceeds the allocated capacity");
+    g->N = N;
+    g->M = M;
+    gc_status s = gc_check_cuda(ctx, cudaMemcpyAsync(g->V, V, sizeof(uint32_t) * ((size_t)N + 1),
+                                                     cudaMemcpyHostToDevice, ctx->stream), "upload V");
+    if (s == GC_OK && M)
+        s = gc_check_cuda(ctx, cudaMemcpyAsync(g->E, E, sizeof(uint32_t) * (size_t)M, cudaMemcpyHostToDevice, ctx->stream),
+                          "upload E");
+    if (s == GC_OK)
+        s = gc_check_cuda(ctx, cudaMemcpyAsync(g->seg_voff, voff, sizeof(uint32_t) * ((size_t)G + 1),
+                                               cudaMemcpyHostToDevice, ctx->stream), "upload offsets");
+    if (s != GC_OK) return s;
+    return finish_batch_upload(b, G, voff);
+}
+
 void gc_batch_free(gc_batch *b) {
     if (!b) return;
     {
@@ -504,6 +532,25 @@ gc_status gc_batch_color(gc_ctx *ctx, gc_batch *b, gc_heuristic h, const gc_mode
     g->key_kind = (int)h;
     g->has_keys = g->has_colors = true;
     return finish_pipeline(b, colors);
+}
+
+gc_status gc_batch_color_once(gc_ctx *ctx, gc_batch *b, gc_heuristic h, const gc_model *m, int recolor,
+                              int32_t *colors) {
+    if (!ctx || !b || b->ctx != ctx || recolor < 0) return GC_ERR_INVALID;
+    DeviceGuard dg(ctx);
+    gc_status s = check_heuristic(ctx, h, m);
+    if (s != GC_OK) return s;
+    gc_graph *g = b->g;
+    if (g->N == 0) {
+        if (colors)
+            for (uint32_t i = 0; i < b->G; i++) colors[i] = 1;
+        g->has_colors = true;
+        return GC_OK;
+    }
+    if ((s = direct_pass(b, h, m, recolor, colors, nullptr)) != GC_OK) return s;
+    g->key_kind = (int)h;
+    g->has_keys = g->has_colors = true;
+    return GC_OK;
 }
 
 gc_status gc_batch_download_colors(gc_ctx *ctx, gc_batch *b, int32_t *color) {

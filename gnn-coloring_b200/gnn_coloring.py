@@ -133,6 +133,55 @@ _sig("gc_batch_set_tuning", C.c_int, vp, vp, C.POINTER(Tuning))
 _sig("gc_batch_get_tuning", C.c_int, vp, C.POINTER(Tuning))
 _sig("gc_tuning_default", None, C.POINTER(Tuning))
 
+_sig("gc_batch_reupload", C.c_int, vp, vp, C.c_uint32, u32p, u32p, u32p)
+_sig("gc_batch_color_once", C.c_int, vp, vp, C.c_int, vp, C.c_int, i32p)
+
+
+class ServeConfig(C.Structure):
+    """gc_serve_config."""
+    _fields_ = [("device", C.c_int), ("lanes", C.c_uint32), ("hbm_budget", C.c_uint64),
+                ("slot_graphs", C.c_uint32), ("slot_vertices", C.c_uint32), ("slot_edges", C.c_uint32),
+                ("batch_max_job_vertices", C.c_uint32)]
+
+
+class JobInfo(C.Structure):
+    """gc_job_info: outcome and timing of one served job."""
+    _fields_ = [("status", C.c_int), ("colors", C.c_int), ("N", C.c_uint32), ("M", C.c_uint32),
+                ("batch_jobs", C.c_uint32), ("lane", C.c_uint32), ("queue_ms", C.c_double),
+                ("run_ms", C.c_double), ("latency_ms", C.c_double)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class ServeStats(C.Structure):
+    """gc_serve_stats."""
+    _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("failed", C.c_uint64),
+                ("rejected", C.c_uint64), ("edges", C.c_uint64), ("launches", C.c_uint64),
+                ("batched_jobs", C.c_uint64), ("p50_ms", C.c_double), ("p99_ms", C.c_double),
+                ("mean_ms", C.c_double), ("max_ms", C.c_double), ("span_s", C.c_double),
+                ("edges_per_s", C.c_double), ("budget_bytes", C.c_uint64), ("reserved_bytes", C.c_uint64),
+                ("peak_reserved_bytes", C.c_uint64), ("pool_peak_bytes", C.c_uint64), ("lanes", C.c_uint32)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+_sig("gc_serve_config_default", None, C.POINTER(ServeConfig))
+_sig("gc_serve_create", C.c_int, C.POINTER(ServeConfig), C.POINTER(vp))
+_sig("gc_serve_add_model", C.c_int, vp, C.c_int, C.c_int, f32p)
+_sig("gc_serve_submit", C.c_int, vp, C.c_uint32, u32p, u32p, C.c_int, C.c_int, C.c_int, i32p,
+     C.POINTER(C.c_uint64))
+_sig("gc_serve_test", C.c_int, vp, C.c_uint64, C.POINTER(C.c_int))
+_sig("gc_serve_wait", C.c_int, vp, C.c_uint64, C.POINTER(JobInfo))
+_sig("gc_serve_drain", C.c_int, vp)
+_sig("gc_serve_replay", C.c_int, vp, C.c_uint32, f64p, u32p, C.POINTER(u32p), C.POINTER(u32p), C.POINTER(C.c_int),
+     C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(i32p), C.POINTER(JobInfo))
+_sig("gc_serve_read_stats", C.c_int, vp, C.POINTER(ServeStats))
+_sig("gc_serve_reset_stats", None, vp)
+_sig("gc_serve_last_error", C.c_char_p, vp)
+_sig("gc_serve_destroy", None, vp)
+
 
 def _ptr(a: np.ndarray, t):
     return a.ctypes.data_as(t)
@@ -518,6 +567,122 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+class Server:
+    """A coloring server on one GPU (gc_server): continuous batching over device-resident pools,
+    admission by HBM budget, per-job latency.  Each job's colors equal its graph colored alone.
+
+    ``submit`` keeps references to the job's arrays until ``wait`` returns, as the C API requires
+    the caller's buffers to stay valid until the job is done."""
+
+    def __init__(self, device: int = 0, lanes: int = 4, hbm_budget: int = 0, slot_graphs: int = 4096,
+                 slot_vertices: int = 1 << 22, slot_edges: int = 1 << 26, batch_max_job_vertices: int = 1 << 17,
+                 models=()):
+        cfg = ServeConfig()
+        lib.gc_serve_config_default(C.byref(cfg))
+        cfg.device, cfg.lanes, cfg.hbm_budget = device, lanes, hbm_budget
+        cfg.slot_graphs, cfg.slot_vertices, cfg.slot_edges = slot_graphs, slot_vertices, slot_edges
+        cfg.batch_max_job_vertices = batch_max_job_vertices
+        h = vp()
+        st = lib.gc_serve_create(C.byref(cfg), C.byref(h))
+        if st != 0:
+            raise GCError(st, "gc_serve_create")
+        self.h = h
+        self._held = {}
+        _live_objects.add(self)
+        for params, md in models:
+            self.add_model(params, md)
+
+    def _check(self, st, what):
+        if st != 0:
+            detail = lib.gc_serve_last_error(self.h) if self.h else b""
+            raise GCError(st, f"{what}: {detail.decode()}" if detail else what)
+
+    def add_model(self, params: np.ndarray, md: int):
+        p = np.ascontiguousarray(params, np.float32)
+        self._check(lib.gc_serve_add_model(self.h, len(p), md, _ptr(p, f32p)), "add model")
+
+    @staticmethod
+    def _job_arrays(N, V, E):
+        Vc = np.ascontiguousarray(V, np.uint32)
+        Ec = np.ascontiguousarray(E, np.uint32) if len(E) else np.zeros(1, np.uint32)
+        return Vc, Ec
+
+    def submit(self, N: int, V: np.ndarray, E: np.ndarray, heuristic="FF", layers: int = 0, recolor: int = 0,
+               want_colors: bool = True) -> int:
+        h = HEURISTICS[heuristic] if isinstance(heuristic, str) else int(heuristic)
+        Vc, Ec = self._job_arrays(N, V, E)
+        out = np.zeros(max(int(N), 1), np.int32) if want_colors else None
+        jid = C.c_uint64(0)
+        self._check(lib.gc_serve_submit(self.h, int(N), _ptr(Vc, u32p), _ptr(Ec, u32p), h, layers, recolor,
+                                        _ptr(out, i32p) if out is not None else None, C.byref(jid)), "submit")
+        self._held[jid.value] = (Vc, Ec, out, int(N))
+        return jid.value
+
+    def done(self, job: int) -> bool:
+        d = C.c_int(0)
+        self._check(lib.gc_serve_test(self.h, job, C.byref(d)), "test")
+        return bool(d.value)
+
+    def wait(self, job: int):
+        """(colors or None, JobInfo); raises GCError when the job failed."""
+        info = JobInfo()
+        st = lib.gc_serve_wait(self.h, job, C.byref(info))
+        Vc, Ec, out, N = self._held.pop(job, (None, None, None, 0))
+        self._check(st, f"job {job}")
+        return (out[:N] if out is not None else None), info
+
+    def drain(self):
+        self._check(lib.gc_serve_drain(self.h), "drain")
+
+    def replay(self, arrive_s, graphs, heuristics, layers=None, recolor=None, want_colors: bool = False):
+        """Open-loop load: graphs[i] = (N, V, E) arrives at arrive_s[i] seconds.  Returns
+        (list of colors or None, list of JobInfo dicts)."""
+        J = len(graphs)
+        keep = [self._job_arrays(*g) for g in graphs]
+        arr = np.ascontiguousarray(arrive_s, np.float64)
+        ns = np.array([int(g[0]) for g in graphs], np.uint32)
+        Vs = (u32p * max(J, 1))(*[_ptr(v, u32p) for v, _ in keep])
+        Es = (u32p * max(J, 1))(*[_ptr(e, u32p) for _, e in keep])
+        hs = np.array([HEURISTICS[x] if isinstance(x, str) else int(x) for x in heuristics], np.int32)
+        ls = np.array(layers if layers is not None else [0] * J, np.int32)
+        rs = np.array(recolor if recolor is not None else [0] * J, np.int32)
+        outs = [np.zeros(max(int(g[0]), 1), np.int32) for g in graphs] if want_colors else None
+        op = (i32p * max(J, 1))(*[_ptr(o, i32p) for o in outs]) if want_colors else None
+        infos = (JobInfo * max(J, 1))()
+        i32 = C.POINTER(C.c_int)
+        st = lib.gc_serve_replay(self.h, J, _ptr(arr, f64p), _ptr(ns, u32p), Vs, Es, hs.ctypes.data_as(i32),
+                                 ls.ctypes.data_as(i32), rs.ctypes.data_as(i32), op, infos)
+        self._check(st, "replay")
+        cols = [o[: int(g[0])] for o, g in zip(outs, graphs)] if want_colors else None
+        return cols, [infos[i].as_dict() for i in range(J)]
+
+    def stats(self) -> dict:
+        st = ServeStats()
+        self._check(lib.gc_serve_read_stats(self.h, C.byref(st)), "stats")
+        return st.as_dict()
+
+    def reset_stats(self):
+        lib.gc_serve_reset_stats(self.h)
+
+    def close(self):
+        if self.h:
+            lib.gc_serve_destroy(self.h)
+            self.h = None
+            self._held.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def serve_config_default() -> ServeConfig:
+    c = ServeConfig()
+    lib.gc_serve_config_default(C.byref(c))
+    return c
 
 
 def default_tuning() -> Tuning:

@@ -201,6 +201,10 @@ gc_status gc_batch_upload_graphs(gc_ctx *ctx, uint32_t G, const uint32_t *n, con
 gc_status gc_batch_create(gc_ctx *ctx, uint32_t cap_G, uint32_t cap_N, uint32_t cap_M, gc_batch **b);
 gc_status gc_batch_reupload_graphs(gc_ctx *ctx, gc_batch *b, uint32_t G, const uint32_t *n,
                                    const uint32_t *const *Vs, const uint32_t *const *Es);
+/* Refills an existing batch from a segmented CSR in host memory (the layout of gc_batch_upload)
+ * without new device allocations; pinned host memory makes the copies asynchronous. */
+gc_status gc_batch_reupload(gc_ctx *ctx, gc_batch *b, uint32_t G, const uint32_t *voff, const uint32_t *V,
+                            const uint32_t *E);
 void gc_batch_free(gc_batch *b);
 uint32_t gc_batch_num_graphs(const gc_batch *b);
 uint32_t gc_batch_num_vertices(const gc_batch *b);
@@ -219,6 +223,10 @@ gc_graph *gc_batch_graph(gc_batch *b);
  * each graph's color count as validate_coloring_par reports it: 0 for an improper coloring. */
 gc_status gc_batch_color(gc_ctx *ctx, gc_batch *b, gc_heuristic h, const gc_model *model, int recolor,
                          int32_t *colors);
+/* The same pipeline as gc_batch_color, run once without capturing it: for batches whose contents
+ * change on every call (a serving loop refilling one batch), where a capture would not be replayed. */
+gc_status gc_batch_color_once(gc_ctx *ctx, gc_batch *b, gc_heuristic h, const gc_model *model, int recolor,
+                              int32_t *colors);
 /* Colors of all vertices, graph by graph (voff[G] entries, local order inside each graph). */
 gc_status gc_batch_download_colors(gc_ctx *ctx, gc_batch *b, int32_t *color);
 
@@ -232,6 +240,95 @@ gc_status gc_batch_set_tuning(gc_ctx *ctx, gc_batch *b, const gc_tuning *t);
 gc_status gc_batch_get_tuning(const gc_batch *b, gc_tuning *t);
 /* The library's default tuning. */
 void gc_tuning_default(gc_tuning *t);
+
+/* ---- serving: a request loop with continuous batching ----------------------------------------- */
+
+/* No counterpart in the reference, whose runner colors one graph per process (src/runner.c:105-153).
+ *
+ * A server keeps device-resident pools on one GPU and colors jobs submitted from any host thread.
+ * Every job's colors and color count equal those of its graph colored alone by gc_priority +
+ * gc_color; only when and beside what it runs changes.
+ *
+ *   lanes      `lanes` worker threads, each with its own stream, a batch slot of fixed capacity
+ *              (slot_graphs graphs, slot_vertices vertices, slot_edges directed edges) and pinned
+ *              staging buffers; lanes run concurrently, so their device work overlaps.
+ *   batching   continuous: a free lane takes the oldest pending job and, when it is small (at most
+ *              batch_max_job_vertices vertices, heuristic FF, LF, LLF or GNN), every other pending
+ *              small job of the same heuristic, layer count and recolor count that fits its slot,
+ *              and colors them in one pass.  Jobs arriving while the lanes are busy join the next
+ *              free lane's batch, so batches grow with the load.
+ *   admission  by HBM budget: the slots are charged once at creation; a job that runs alone (large,
+ *              or SL / SLL) is charged gc_batch_device_bytes(1, N, M, h) while it runs and starts
+ *              only when that fits what is left.  Such jobs start in arrival order.  A job that
+ *              could never fit is refused at submission with GC_ERR_BUDGET.
+ *   isolation  a batch that fails is re-run job by job, so a malformed job fails alone.
+ *
+ * The caller's V, E and color_out buffers must stay valid and unchanged until the job is done. */
+typedef struct gc_server gc_server;
+
+typedef struct gc_serve_config {
+    int device;                       /* CUDA device */
+    uint32_t lanes;                   /* concurrent worker lanes (default 4) */
+    uint64_t hbm_budget;              /* device bytes the server may hold; 0 = 80% of the free memory */
+    uint32_t slot_graphs;             /* most jobs in one batch (default 4096) */
+    uint32_t slot_vertices;           /* vertex capacity of a lane's batch slot (default 2^22) */
+    uint32_t slot_edges;              /* directed-edge capacity of a lane's batch slot (default 2^26) */
+    uint32_t batch_max_job_vertices;  /* larger jobs run alone (default 2^17) */
+} gc_serve_config;
+
+typedef struct gc_job_info {
+    int status;           /* gc_status of the job */
+    int colors;           /* colors used (validate_coloring_par's figure: 0 = improper) */
+    uint32_t N, M;        /* vertices, directed edges */
+    uint32_t batch_jobs;  /* jobs colored in the same pass (1 = alone) */
+    uint32_t lane;        /* lane that ran it */
+    double queue_ms;      /* submission to start */
+    double run_ms;        /* start to completion (upload, coloring, read-back) */
+    double latency_ms;    /* submission to completion */
+} gc_job_info;
+
+typedef struct gc_serve_stats {
+    uint64_t submitted, completed, failed, rejected;
+    uint64_t edges;                /* directed edges of completed jobs */
+    uint64_t launches;             /* passes run: batches plus jobs run alone */
+    uint64_t batched_jobs;         /* completed jobs that shared their pass with others */
+    double p50_ms, p99_ms, mean_ms, max_ms;  /* submission-to-completion latency of completed jobs */
+    double span_s;                 /* first submission to last completion */
+    double edges_per_s;            /* edges / span_s */
+    uint64_t budget_bytes, reserved_bytes, peak_reserved_bytes;  /* admission accounting */
+    uint64_t pool_peak_bytes;      /* high-water mark of the lanes' device memory pool */
+    uint32_t lanes;
+} gc_serve_stats;
+
+void gc_serve_config_default(gc_serve_config *c);
+/* Starts the lanes; GC_ERR_BUDGET when the slots alone exceed the budget. */
+gc_status gc_serve_create(const gc_serve_config *cfg, gc_server **s);
+/* Adds the GraphSAGE-16 model GNN jobs with params / 528 layers use (before the first submission). */
+gc_status gc_serve_add_model(gc_server *s, int params, int md, const float *param);
+/* Queues a job: CSR (V[N+1], E[V[N]], the rules of gc_graph_upload), heuristic h (`layers` picks
+ * the model for GC_GNN), `recolor` Culberson iterations; color_out (N entries, may be NULL)
+ * receives the colors.  Returns at once with the job's id. */
+gc_status gc_serve_submit(gc_server *s, uint32_t N, const uint32_t *V, const uint32_t *E, gc_heuristic h, int layers,
+                          int recolor, int32_t *color_out, uint64_t *job);
+/* *done = 1 when the job has finished. */
+gc_status gc_serve_test(gc_server *s, uint64_t job, int *done);
+/* Blocks until the job has finished, fills *info (may be NULL), releases the job's id and returns
+ * the job's status. */
+gc_status gc_serve_wait(gc_server *s, uint64_t job, gc_job_info *info);
+/* Blocks until no job is pending or running. */
+gc_status gc_serve_drain(gc_server *s);
+/* Open-loop load from the calling thread: job i is submitted arrive_s[i] seconds after the call
+ * starts (non-decreasing), with the arguments of gc_serve_submit taken from the arrays (layers,
+ * recolor and color_out may be NULL); then waits for every job and fills info[i] (may be NULL).
+ * A job's latency counts from its scheduled arrival.  Returns the first failing job's status. */
+gc_status gc_serve_replay(gc_server *s, uint32_t J, const double *arrive_s, const uint32_t *N,
+                          const uint32_t *const *V, const uint32_t *const *E, const int *h, const int *layers,
+                          const int *recolor, int32_t *const *color_out, gc_job_info *info);
+gc_status gc_serve_read_stats(gc_server *s, gc_serve_stats *st);
+void gc_serve_reset_stats(gc_server *s);
+const char *gc_serve_last_error(gc_server *s);
+/* Waits for all jobs, stops the lanes and frees everything. */
+void gc_serve_destroy(gc_server *s);
 
 /* ---- host-side graph preparation (no device involved) --------------------------------------- */
 
