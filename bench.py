@@ -371,6 +371,10 @@ def run_ours(args):
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         result["cpu_baseline"] = cpu_baseline(N, V, E, params, md)
+    if world == 1 and not args.no_batch:
+        result["batched"] = run_batched(args, device)
+    if world == 1 and not args.no_serve:
+        result["serving"] = run_serving(args, device)
     if rank == 0:
         print(json.dumps(result))
     g.close()
@@ -379,6 +383,214 @@ def run_ours(args):
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+# ---- batched vs plain: many independent graphs in one launch ------------------------------------
+
+def run_batched(args, device):
+    """4,096 mixed graphs (n log-uniform in [1e3, 2e5]; even seeds Erdos-Renyi with average degree
+    U[8, 32], odd seeds R-MAT with edge factor 8; seeds 1000..5095) colored by GNN2 and by LF: one
+    autotuned, CUDA-graph-captured gc_batch_color pass over the device-resident segmented CSR against
+    one plain gc_priority + gc_color per graph (graphs device-resident too).  Both legs return each
+    graph's color count to the host; colors are compared vertex by vertex."""
+    import gnn_coloring as gcn
+    G = args.batch_graphs
+    t0 = time.perf_counter()
+    voff, V, E = gcn.gen_mixed_batch(G, 1000, 1000, 200000)
+    gen_s = time.perf_counter() - t0
+    N, M = int(voff[G]), int(V[int(voff[G])])
+    ctx = gcn.Context(device)
+    params2, md2 = gcn.synthetic_model(2, MODEL_SEED)
+    model = gcn.Model(ctx, params2, md2)
+    heurs = [("GNN2", "GNN", model), ("LF", "LF", None)]
+    out = {"workload": f"{G} mixed graphs: n log-uniform [1000, 200000]; even seeds Erdos-Renyi avg degree "
+                       f"U[8,32], odd seeds R-MAT ef 8; seeds 1000..{999 + G}",
+           "G": G, "N": N, "M": M, "host_generation_s": gen_s, "heuristics": {}}
+    b = gcn.Batch(ctx, voff, V, E)
+    batch_colors = {}
+    for name, h, m in heurs:
+        tuning, tuned_ms = b.autotune(h, m, 0, effort=1)
+        counts = b.color(h, m)          # first call runs directly and captures the pipeline
+        ctx.sync()
+        reps = max(3, min(args.steps, 10))
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            counts = b.color(h, m)      # one cudaGraphLaunch, per-graph counts read back
+        batch_s = (time.perf_counter() - t0) / reps
+        batch_colors[name] = (b.colors(), counts.copy())
+        out["heuristics"][name] = {"batched_ms": 1e3 * batch_s, "batched_edges_per_s": M / batch_s,
+                                   "autotuned": tuning.as_dict(), "autotune_best_ms": tuned_ms}
+    b.close()
+    # plain leg: the same graphs, one device-resident gc_graph each, one priority + color per graph
+    graphs = []
+    for g in range(G):
+        a, z = int(voff[g]), int(voff[g + 1])
+        ea, ez = int(V[a]), int(V[z])
+        graphs.append(gcn.Graph(ctx, z - a, (V[a:z + 1] - V[a]).astype(np.uint32), E[ea:ez]))
+    for name, h, m in heurs:
+        for gr in graphs[:16]:
+            gr.priority(h, m)
+            gr.color()
+        ctx.sync()
+        counts = np.zeros(G, np.int64)
+        t0 = time.perf_counter()
+        for i, gr in enumerate(graphs):
+            gr.priority(h, m)
+            counts[i] = gr.color()      # the color count, read back per graph
+        plain_s = time.perf_counter() - t0
+        bc, bcounts = batch_colors[name]
+        same = bool(np.array_equal(counts, bcounts))
+        for i, gr in enumerate(graphs):
+            if not same:
+                break
+            same = np.array_equal(gr.colors(), bc[int(voff[i]):int(voff[i + 1])])
+        r = out["heuristics"][name]
+        r.update({"plain_ms": 1e3 * plain_s, "plain_edges_per_s": M / plain_s,
+                  "speedup": plain_s / (r["batched_ms"] / 1e3), "colors_identical": same})
+    for gr in graphs:
+        gr.close()
+    model.close()
+    ctx.close()
+    return out
+
+
+# ---- serving: open-loop arrivals of mixed jobs ----------------------------------------------------
+
+SERVE_RATES = (100, 1000, 5000, 20000)
+
+
+def serving_pool(seed: int = 5):
+    """Graphs the jobs draw from: 48 Erdos-Renyi (n uniform in [1000, 50000], average degree 16),
+    2 R-MAT scale 20 and 1 R-MAT scale 24 (edge factor 16, a/b/c = 0.57/0.19/0.19)."""
+    import gnn_coloring as gcn
+    rng = np.random.default_rng(seed)
+    small = []
+    for i in range(48):
+        n = int(rng.integers(1000, 50001))
+        small.append(gcn.gen_er(n, 8 * n, 10_000 + i))
+    medium = [gcn.gen_rmat(1 << 20, 16, 20 + i) for i in range(2)]
+    large = [gcn.gen_rmat(1 << 24, 16, 24)]
+    return small, medium, large
+
+
+def serving_jobs(pool, J: int, seed: int):
+    """J jobs: 90% small, 9% medium, 1% large graphs; heuristic uniform over FF, LLF, GNN3."""
+    small, medium, large = pool
+    rng = np.random.default_rng(seed)
+    jobs = []
+    for _ in range(J):
+        r = rng.random()
+        cls = small if r < 0.90 else (medium if r < 0.99 else large)
+        k = int(rng.integers(len(cls)))
+        jobs.append((cls[k], ("FF", "LLF", "GNN")[int(rng.integers(3))]))
+    return jobs
+
+
+def _sweep(srv, pool, J, replay, alone_counts):
+    """Poisson arrivals at each rate of SERVE_RATES (J jobs each) through `replay`; per-rate latency
+    percentiles and throughput from the server's own statistics."""
+    sweep, same = [], True
+    for i, rate in enumerate(SERVE_RATES):
+        jobs = serving_jobs(pool, J, 1000 + i)
+        arrive = np.cumsum(np.random.default_rng(2000 + i).exponential(1.0 / rate, J))
+        srv.reset_stats()
+        infos = replay(arrive, jobs)
+        st = srv.stats()
+        for (gr, h), inf in zip(jobs, infos):
+            c = alone_counts.get((id(gr), h))
+            if c is not None and c != inf["colors"]:
+                same = False
+        sweep.append({"offered_jobs_per_s": rate, "jobs": J, "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
+                      "max_ms": st["max_ms"], "edges_per_s": st["edges_per_s"],
+                      "jobs_per_s": st["completed"] / st["span_s"] if st["span_s"] else None,
+                      "passes": st["launches"], "batched_jobs": st["batched_jobs"],
+                      "peak_reserved_gb": st["peak_reserved_bytes"] / 1e9, "pool_peak_gb": st["pool_peak_bytes"] / 1e9})
+    return sweep, same
+
+
+def _plain_sequential(jobs, run_one):
+    """The same jobs one after another through the plain path: throughput and per-job latency."""
+    lat, edges = [], 0
+    counts = {}
+    t0 = time.perf_counter()
+    for gr, h in jobs:
+        ta = time.perf_counter()
+        counts[(id(gr), h)] = run_one(gr, h)
+        lat.append(1e3 * (time.perf_counter() - ta))
+        edges += int(gr[1][-1])
+    dt = time.perf_counter() - t0
+    return ({"jobs": len(jobs), "edges_per_s": edges / dt, "jobs_per_s": len(jobs) / dt,
+             "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99))}, counts)
+
+
+def run_serving(args, device):
+    """The serving mix in two forms: jobs bringing their CSR in host memory (uploaded per job), and
+    jobs on CSRs registered once (device-resident).  Each against the same jobs run one at a time
+    through the plain path in the same form."""
+    import gnn_coloring as gcn
+    t0 = time.perf_counter()
+    pool = serving_pool()
+    gen_s = time.perf_counter() - t0
+    params3, md3 = gcn.synthetic_model(3, MODEL_SEED)
+    J = args.serve_jobs
+    base_jobs = serving_jobs(pool, J, 99)
+    ctx = gcn.Context(device)
+    model = gcn.Model(ctx, params3, md3)
+
+    def host_one(gr, h):
+        g = gcn.Graph(ctx, *gr)
+        g.priority(h, model if h == "GNN" else None)
+        c = g.color()
+        g.colors()
+        g.close()
+        return c
+
+    plain_host, counts = _plain_sequential(base_jobs, host_one)
+    resident = {id(gr): gcn.Graph(ctx, *gr) for cls in pool for gr in cls}
+
+    def resident_one(gr, h):
+        g = resident[id(gr)]
+        g.priority(h, model if h == "GNN" else None)
+        c = g.color()
+        g.colors()
+        return c
+
+    plain_res, counts_res = _plain_sequential(base_jobs, resident_one)
+    counts.update(counts_res)
+    for g in resident.values():
+        g.close()
+    model.close()
+    ctx.close()
+
+    srv = gcn.Server(device=device, models=[(params3, md3)])
+    lanes = int(gcn.serve_config_default().lanes)
+
+    def replay_host(arrive, jobs):
+        return srv.replay(arrive, [gr for gr, _ in jobs], [h for _, h in jobs],
+                          layers=[3 if h == "GNN" else 0 for _, h in jobs])[1]
+
+    sweep_host, same1 = _sweep(srv, pool, J, replay_host, counts)
+    reg = {id(gr): srv.register(*gr) for cls in pool for gr in cls}
+
+    def replay_res(arrive, jobs):
+        return srv.replay_registered(arrive, [reg[id(gr)] for gr, _ in jobs], [h for _, h in jobs],
+                                     layers=[3 if h == "GNN" else 0 for _, h in jobs])[1]
+
+    sweep_res, same2 = _sweep(srv, pool, J, replay_res, counts)
+    srv.close()
+
+    def form(plain, sweep):
+        best = max(sweep, key=lambda r: r["edges_per_s"])
+        best_j = max(r["jobs_per_s"] or 0 for r in sweep)
+        return {"plain_sequential": plain, "sweep": sweep,
+                "speedup_edges_per_s": best["edges_per_s"] / plain["edges_per_s"],
+                "speedup_jobs_per_s": best_j / plain["jobs_per_s"]}
+
+    return {"mix": "90% Erdos-Renyi n in [1000, 50000] avg degree 16, 9% R-MAT scale 20, 1% R-MAT scale 24 "
+                   "(ef 16); heuristic uniform over FF, LLF, GNN3; open-loop Poisson arrivals",
+            "pool_generation_s": gen_s, "jobs_per_rate": J, "lanes": lanes,
+            "host_csr": form(plain_host, sweep_host), "resident_csr": form(plain_res, sweep_res),
+            "color_counts_identical_to_alone": same1 and same2}
 
 
 def run_e2e(args, N, V, E, params, md, torch):
@@ -431,6 +643,10 @@ def main():
     ap.add_argument("--workload", default="rmat22", choices=["rmat22", "rmat18", "er65k"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched-vs-plain leg")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving sweep")
+    ap.add_argument("--batch-graphs", type=int, default=4096)
+    ap.add_argument("--serve-jobs", type=int, default=300)
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

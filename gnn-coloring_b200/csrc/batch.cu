@@ -23,6 +23,15 @@
 
 #include "gc_internal.h"
 
+// Where one device-resident graph goes in a batch's staging buffers.
+struct gc_seg_src {
+    const uint32_t *V;  // n + 1 local row offsets
+    const uint32_t *E;  // m local neighbour ids
+    uint32_t n, m;
+    uint32_t vdst;      // voff[g] + g: its first staged row offset
+    uint32_t edst;      // eoff[g]: its first edge
+};
+
 namespace {
 
 __global__ void k_check_rows(const uint32_t *__restrict__ V, uint32_t N, uint32_t M, gc::DevState *st) {
@@ -63,6 +72,17 @@ __global__ void k_seg_globalize(const uint32_t *__restrict__ V, uint32_t *__rest
     }
 }
 
+// Copies graph g's local row offsets to vloc[src.vdst ...] and its neighbour ids to E[src.edst ...],
+// one CTA per graph (the staging layout of fill_graphs, but from device-resident CSRs).
+__global__ void k_seg_gather(const gc_seg_src *__restrict__ src, uint32_t G, uint32_t *__restrict__ vloc,
+                             uint32_t *__restrict__ E) {
+    for (uint32_t gi = blockIdx.x; gi < G; gi += gridDim.x) {
+        const gc_seg_src s = src[gi];
+        for (uint32_t i = threadIdx.x; i <= s.n; i += blockDim.x) vloc[s.vdst + i] = __ldg(s.V + i);
+        for (uint32_t i = threadIdx.x; i < s.m; i += blockDim.x) E[s.edst + i] = __ldg(s.E + i);
+    }
+}
+
 // A captured pipeline and what it was captured for.
 struct BatchCapture {
     int h = -1;
@@ -76,6 +96,8 @@ struct BatchCapture {
 
 struct gc_batch {
     gc_ctx *ctx = nullptr;
+    gc_seg_src *d_src = nullptr;    // gather descriptors of gc_batch_reupload_device_graphs (cap_G)
+    gc_seg_src *h_src = nullptr;    // pinned staging of the same
     gc_graph *g = nullptr;          // the union of the graphs (owned)
     uint32_t G = 0, cap_G = 0;
     uint32_t *d_vloc = nullptr;     // staged per-graph row offsets
@@ -474,6 +496,68 @@ gc_status gc_batch_reupload(gc_ctx *ctx, gc_batch *b, uint32_t G, const uint32_t
     return finish_batch_upload(b, G, voff);
 }
 
+gc_status gc_batch_reupload_device_graphs(gc_ctx *ctx, gc_batch *b, uint32_t G, const uint32_t *n, const uint32_t *m,
+                                          const uint32_t *const *dVs, const uint32_t *const *dEs) {
+    if (!ctx || !b || b->ctx != ctx) return GC_ERR_INVALID;
+    if (G && (!n || !m || !dVs || !dEs)) return gc_fail(ctx, GC_ERR_INVALID, "null graph arrays");
+    DeviceGuard dg(ctx);
+    gc_graph *g = b->g;
+    std::vector<uint32_t> voff((size_t)G + 1, 0), eoff((size_t)G + 1, 0);
+    uint64_t nv = 0, ne = 0;
+    for (uint32_t i = 0; i < G; i++) {
+        if (!dVs[i] || (m[i] && !dEs[i]))
+            return gc_fail(ctx, GC_ERR_INVALID, "graph " + std::to_string(i) + ": null device CSR");
+        nv += n[i];
+        ne += m[i];
+        if (nv >= 0xffffffffULL || ne > 0xffffffffULL)
+            return gc_fail(ctx, GC_ERR_INVALID, "batch exceeds 2^32 vertices or edges");
+        voff[i + 1] = (uint32_t)nv;
+        eoff[i + 1] = (uint32_t)ne;
+    }
+    const uint32_t N = voff[G], M = eoff[G];
+    if (N > g->cap_N || M > g->cap_M || G > b->cap_G)
+        return gc_fail(ctx, GC_ERR_INVALID, "batch exceeds the allocated capacity");
+    gc_status s;
+    const size_t vloc_words = (size_t)N + G;
+    if (vloc_words > b->vloc_cap) {
+        gc_dev_free(ctx, b->d_vloc);
+        b->d_vloc = nullptr;
+        if ((s = gc_alloc(ctx, &b->d_vloc, std::max(vloc_words, (size_t)g->cap_N + b->cap_G), "staged row offsets")) !=
+            GC_OK)
+            return s;
+        b->vloc_cap = std::max(vloc_words, (size_t)g->cap_N + b->cap_G);
+    }
+    if ((s = gc_alloc(ctx, &b->d_src, (size_t)b->cap_G, "gather descriptors")) != GC_OK) return s;
+    if (!b->h_src && (s = gc_check_cuda(ctx, cudaMallocHost((void **)&b->h_src, sizeof(gc_seg_src) * b->cap_G),
+                                        "pinned descriptors")) != GC_OK)
+        return s;
+    // the previous refill's descriptor copy must be done before the pinned staging is rewritten
+    if ((s = gc_check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "batch refill")) != GC_OK) return s;
+    for (uint32_t i = 0; i < G; i++) b->h_src[i] = gc_seg_src{dVs[i], dEs[i], n[i], m[i], voff[i] + i, eoff[i]};
+    g->N = N;
+    g->M = M;
+    if (G && (s = gc_check_cuda(ctx, cudaMemcpyAsync(b->d_src, b->h_src, sizeof(gc_seg_src) * G, cudaMemcpyHostToDevice,
+                                                     ctx->stream), "upload descriptors")) != GC_OK)
+        return s;
+    if ((s = gc_check_cuda(ctx, cudaMemcpyAsync(g->seg_voff, voff.data(), sizeof(uint32_t) * ((size_t)G + 1),
+                                                cudaMemcpyHostToDevice, ctx->stream), "upload offsets")) != GC_OK)
+        return s;
+    if ((s = gc_check_cuda(ctx, cudaMemcpyAsync(b->d_eoff, eoff.data(), sizeof(uint32_t) * ((size_t)G + 1),
+                                                cudaMemcpyHostToDevice, ctx->stream), "upload offsets")) != GC_OK)
+        return s;
+    if (G) {
+        k_seg_gather<<<std::min<uint32_t>(G, 65535u), 256, 0, ctx->stream>>>(b->d_src, G, b->d_vloc, g->E);
+        ctx->launches++;
+        if ((s = gc_check_launch(ctx, "gather graphs")) != GC_OK) return s;
+    }
+    k_seg_rows<<<ctx->num_sms * 4, 256, 0, ctx->stream>>>(b->d_vloc, g->seg_voff, b->d_eoff, G, N, M, g->V);
+    ctx->launches++;
+    if ((s = gc_check_launch(ctx, "segment rows")) != GC_OK) return s;
+    // the host vectors must outlive the copies above
+    if ((s = gc_check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "batch refill")) != GC_OK) return s;
+    return finish_batch_upload(b, G, voff.data());
+}
+
 void gc_batch_free(gc_batch *b) {
     if (!b) return;
     {
@@ -483,8 +567,10 @@ void gc_batch_free(gc_batch *b) {
         if (b->g) {
             gc_dev_free(b->ctx, b->d_vloc);
             gc_dev_free(b->ctx, b->d_eoff);
+            gc_dev_free(b->ctx, b->d_src);
         }
         if (b->h_stat) cudaFreeHost(b->h_stat);
+        if (b->h_src) cudaFreeHost(b->h_src);
     }
     if (b->g) gc_graph_free(b->g);
     delete b;

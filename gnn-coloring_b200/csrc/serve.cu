@@ -22,6 +22,12 @@
 //             that arrive while the lanes are busy accumulate and join the next free lane's batch.
 //   isolation a batch that fails (a malformed CSR of one job) is re-run job by job on the plain
 //             path, so one bad job cannot fail its batch-mates.
+//   resident  graphs registered once (gc_serve_register) stay in device memory, charged to the
+//             budget until released; jobs on them skip the host-to-device copy: batched ones are
+//             gathered into the slot by one kernel, the others wrap the resident CSR.
+//   copies    a job's CSR from host memory goes up through two pinned chunks per lane, filled by
+//             several host threads while the previous chunk's DMA runs (pageable copies through the
+//             driver reach a fraction of the link's bandwidth); colors come back the same way.
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -44,8 +50,18 @@ double seconds_since(Clock::time_point t0, Clock::time_point t) {
     return std::chrono::duration<double>(t - t0).count();
 }
 
+// A CSR registered with the server: device-resident until released.
+struct Reg {
+    uint64_t id = 0;
+    uint32_t N = 0, M = 0;
+    uint32_t *dV = nullptr, *dE = nullptr;
+    uint64_t bytes = 0;
+    uint32_t refs = 0;  // jobs pending or running on it
+};
+
 struct Job {
     uint64_t id = 0;
+    Reg *reg = nullptr;        // set for jobs on a registered graph (V, E are then unused)
     uint32_t N = 0, M = 0;
     const uint32_t *V = nullptr, *E = nullptr;
     int32_t *color_out = nullptr;
@@ -69,8 +85,13 @@ struct Lane {
     gc_model *models[8] = {};    // by layer count
     uint32_t *h_voff = nullptr, *h_V = nullptr, *h_E = nullptr;
     int32_t *h_color = nullptr, *h_counts = nullptr;
+    char *stage[2] = {nullptr, nullptr};  // pinned chunks of the copies of jobs run alone
+    cudaEvent_t stage_ev[2] = {nullptr, nullptr};
     std::thread thread;
 };
+
+constexpr size_t STAGE_BYTES = 32u << 20;  // bytes per pinned chunk
+constexpr int COPY_THREADS = 4;            // host threads filling / draining one chunk
 
 }  // namespace
 
@@ -87,6 +108,9 @@ struct gc_server {
     std::condition_variable cv_done;  // callers wait for jobs
     std::deque<Job *> pending;
     std::unordered_map<uint64_t, Job *> jobs;  // every job not yet released by gc_serve_wait
+    std::unordered_map<uint64_t, Reg *> regs;  // registered graphs
+    uint64_t next_reg = 1;
+    cudaStream_t reg_stream = nullptr;         // uploads and releases of registered graphs
     uint64_t next_id = 1;
     uint64_t reserved = 0, peak_reserved = 0;
     bool large_blocked = false;  // set during a pick when the oldest large job did not fit
@@ -113,7 +137,7 @@ struct Work {
 };
 
 bool same_class(const Job *a, const Job *b) {
-    return a->h == b->h && a->layers == b->layers && a->recolor == b->recolor;
+    return a->h == b->h && a->layers == b->layers && a->recolor == b->recolor && (a->reg != nullptr) == (b->reg != nullptr);
 }
 
 Work pick_work(gc_server *s) {
@@ -175,6 +199,7 @@ void complete(gc_server *s, Job *j, gc_status st, int colors, uint32_t batch_job
     j->error = err;
     j->t_done = Clock::now();
     j->done = true;
+    if (j->reg) j->reg->refs--;
     if (st == GC_OK) {
         s->st_completed++;
         s->st_edges += j->M;
@@ -191,36 +216,121 @@ void complete(gc_server *s, Job *j, gc_status st, int colors, uint32_t batch_job
 
 gc_model *lane_model(Lane *L, const Job *j) { return j->h == GC_GNN ? L->models[j->layers] : nullptr; }
 
-// One job alone on the plain path: upload, priority, coloring, colors back.
+// memcpy split over COPY_THREADS host threads (large copies only).
+void copy_host(void *dst, const void *src, size_t bytes) {
+    if (bytes < (4u << 20)) {
+        memcpy(dst, src, bytes);
+        return;
+    }
+    const size_t piece = (bytes + COPY_THREADS - 1) / COPY_THREADS;
+#pragma omp parallel for num_threads(COPY_THREADS) schedule(static)
+    for (int t = 0; t < COPY_THREADS; t++) {
+        const size_t a = (size_t)t * piece;
+        if (a < bytes) memcpy((char *)dst + a, (const char *)src + a, std::min(piece, bytes - a));
+    }
+}
+
+// Host memory to device memory through the lane's two pinned chunks: chunk k is filled while the
+// DMA of chunk k - 1 runs.
+gc_status h2d_staged(Lane *L, void *dst, const void *src, size_t bytes) {
+    gc_ctx *ctx = L->ctx;
+    gc_status st = GC_OK;
+    for (size_t off = 0, k = 0; off < bytes && st == GC_OK; off += STAGE_BYTES, k++) {
+        const size_t n = std::min(STAGE_BYTES, bytes - off);
+        const int b = (int)(k & 1);
+        st = gc_check_cuda(ctx, cudaEventSynchronize(L->stage_ev[b]), "staging");
+        if (st != GC_OK) break;
+        copy_host(L->stage[b], (const char *)src + off, n);
+        st = gc_check_cuda(ctx, cudaMemcpyAsync((char *)dst + off, L->stage[b], n, cudaMemcpyHostToDevice, ctx->stream),
+                           "upload");
+        if (st == GC_OK) st = gc_check_cuda(ctx, cudaEventRecord(L->stage_ev[b], ctx->stream), "staging");
+    }
+    return st;
+}
+
+// Device memory to host memory the same way: the DMA of chunk k + 1 runs while chunk k is copied out.
+gc_status d2h_staged(Lane *L, void *dst, const void *src, size_t bytes) {
+    gc_ctx *ctx = L->ctx;
+    const size_t chunks = (bytes + STAGE_BYTES - 1) / STAGE_BYTES;
+    auto issue = [&](size_t k) -> gc_status {
+        const size_t off = k * STAGE_BYTES, n = std::min(STAGE_BYTES, bytes - off);
+        const int b = (int)(k & 1);
+        gc_status st = gc_check_cuda(ctx, cudaMemcpyAsync(L->stage[b], (const char *)src + off, n,
+                                                          cudaMemcpyDeviceToHost, ctx->stream), "download");
+        if (st == GC_OK) st = gc_check_cuda(ctx, cudaEventRecord(L->stage_ev[b], ctx->stream), "staging");
+        return st;
+    };
+    gc_status st = chunks ? issue(0) : GC_OK;
+    for (size_t k = 0; k < chunks && st == GC_OK; k++) {
+        const int b = (int)(k & 1);
+        if ((st = gc_check_cuda(ctx, cudaEventSynchronize(L->stage_ev[b]), "staging")) != GC_OK) break;
+        if (k + 1 < chunks && (st = issue(k + 1)) != GC_OK) break;
+        const size_t off = k * STAGE_BYTES;
+        copy_host((char *)dst + off, L->stage[b], std::min(STAGE_BYTES, bytes - off));
+    }
+    return st;
+}
+
+// One job alone on the plain path: its CSR up (or the registered one wrapped), priority,
+// coloring, colors back.
 gc_status run_alone(Lane *L, Job *j, int *colors, std::string *err) {
     gc_ctx *ctx = L->ctx;
     gc_graph *g = nullptr;
-    gc_status st = gc_graph_upload(ctx, j->N, j->V, j->E, &g);
+    gc_status st;
+    if (j->reg) {
+        st = gc_graph_wrap_device(ctx, j->N, j->M, j->reg->dV, j->reg->dE, &g);
+    } else {
+        st = gc_graph_create(ctx, j->N, j->M, &g);
+        if (st == GC_OK) st = h2d_staged(L, g->V, j->V, sizeof(uint32_t) * ((size_t)j->N + 1));
+        if (st == GC_OK && j->M) st = h2d_staged(L, g->E, j->E, sizeof(uint32_t) * (size_t)j->M);
+        if (st == GC_OK) {
+            g->N = j->N;
+            g->M = j->M;
+            st = gc_graph_finish_upload(g);
+        }
+    }
     if (st == GC_OK) st = gc_priority(ctx, g, j->h, lane_model(L, j));
     if (st == GC_OK) st = gc_color(ctx, g, j->recolor, colors);
-    if (st == GC_OK && j->color_out) st = gc_download_colors(ctx, g, j->color_out);
+    if (st == GC_OK && j->color_out && j->N) st = d2h_staged(L, j->color_out, g->color, sizeof(int32_t) * (size_t)j->N);
     if (st != GC_OK) *err = gc_last_error(ctx);
     if (g) gc_graph_free(g);
     return st;
 }
 
-// Small jobs of one class as one batch: stage the segmented CSR in pinned memory, refill the
-// lane's slot, color, and scatter the colors back to each job's buffer.
+// Small jobs of one class as one batch: their CSRs into the lane's slot (staged through pinned
+// memory, or gathered on the device for registered graphs), color, and scatter the colors back to
+// each job's buffer.
 gc_status run_batch(Lane *L, const std::vector<Job *> &jobs, std::string *err) {
     gc_ctx *ctx = L->ctx;
     const uint32_t G = (uint32_t)jobs.size();
     uint32_t nv = 0, ne = 0;
     L->h_voff[0] = 0;
-    L->h_V[0] = 0;
-    for (uint32_t i = 0; i < G; i++) {
-        const Job *j = jobs[i];
-        for (uint32_t u = 0; u < j->N; u++) L->h_V[nv + u + 1] = ne + j->V[u + 1];
-        if (j->M) memcpy(L->h_E + ne, j->E, sizeof(uint32_t) * j->M);
-        nv += j->N;
-        ne += j->M;
-        L->h_voff[i + 1] = nv;
+    gc_status st;
+    if (jobs[0]->reg) {
+        std::vector<uint32_t> n(G), m(G);
+        std::vector<const uint32_t *> dV(G), dE(G);
+        for (uint32_t i = 0; i < G; i++) {
+            const Reg *r = jobs[i]->reg;
+            n[i] = r->N;
+            m[i] = r->M;
+            dV[i] = r->dV;
+            dE[i] = r->dE;
+            nv += r->N;
+            L->h_voff[i + 1] = nv;
+        }
+        st = gc_batch_reupload_device_graphs(ctx, L->slot, G, n.data(), m.data(), dV.data(), dE.data());
+    } else {
+        L->h_V[0] = 0;
+        for (uint32_t i = 0; i < G; i++) {
+            const Job *j = jobs[i];
+            for (uint32_t u = 0; u < j->N; u++) L->h_V[nv + u + 1] = ne + j->V[u + 1];
+            if (j->M) memcpy(L->h_E + ne, j->E, sizeof(uint32_t) * j->M);
+            nv += j->N;
+            ne += j->M;
+            L->h_voff[i + 1] = nv;
+        }
+        st = gc_batch_reupload(ctx, L->slot, G, L->h_voff, L->h_V, L->h_E);
     }
-    gc_status st = gc_batch_reupload(ctx, L->slot, G, L->h_voff, L->h_V, L->h_E);
     const Job *j0 = jobs[0];
     if (st == GC_OK) st = gc_batch_color_once(ctx, L->slot, j0->h, lane_model(L, j0), j0->recolor, L->h_counts);
     bool any_out = false;
@@ -305,18 +415,24 @@ void destroy_lane(Lane *L) {
     if (L->h_E) cudaFreeHost(L->h_E);
     if (L->h_color) cudaFreeHost(L->h_color);
     if (L->h_counts) cudaFreeHost(L->h_counts);
+    for (int b = 0; b < 2; b++) {
+        if (L->stage[b]) cudaFreeHost(L->stage[b]);
+        if (L->stage_ev[b]) cudaEventDestroy(L->stage_ev[b]);
+    }
     if (L->ctx) gc_ctx_destroy(L->ctx);
     delete L;
 }
 
-gc_status submit_locked(gc_server *s, uint32_t N, const uint32_t *V, const uint32_t *E, gc_heuristic h, int layers,
-                        int recolor, int32_t *color_out, Clock::time_point now, uint64_t *job_id) {
+gc_status submit_locked(gc_server *s, Reg *reg, uint32_t N, const uint32_t *V, const uint32_t *E, gc_heuristic h,
+                        int layers, int recolor, int32_t *color_out, Clock::time_point now, uint64_t *job_id) {
     // argument checks that need no lock are done by the caller
     const gc_serve_config &c = s->cfg;
     Job *j = new Job();
     j->id = s->next_id++;
-    j->N = N;
-    j->M = V[N];
+    j->reg = reg;
+    j->N = reg ? reg->N : N;
+    j->M = reg ? reg->M : V[N];
+    N = j->N;
     j->V = V;
     j->E = E;
     j->color_out = color_out;
@@ -342,7 +458,16 @@ gc_status submit_locked(gc_server *s, uint32_t N, const uint32_t *V, const uint3
     s->st_submitted++;
     s->jobs[j->id] = j;
     s->pending.push_back(j);
+    if (reg) reg->refs++;
     *job_id = j->id;
+    return GC_OK;
+}
+
+gc_status check_kind(gc_server *s, gc_heuristic h, int layers, int recolor) {
+    if (recolor < 0) return fail(s, GC_ERR_INVALID, "recolor must be >= 0");
+    if ((int)h < GC_FF || (int)h > GC_GNN) return fail(s, GC_ERR_INVALID, "unknown heuristic");
+    if (h == GC_GNN && (layers < 2 || layers > 7 || !s->have_model[layers]))
+        return fail(s, GC_ERR_INVALID, "no GNN model with " + std::to_string(layers) + " layers was added");
     return GC_OK;
 }
 
@@ -352,11 +477,27 @@ gc_status check_job(gc_server *s, uint32_t N, const uint32_t *V, const uint32_t 
     if (V[0] != 0) return fail(s, GC_ERR_INVALID, "V[0] must be 0");
     if (V[N] && !E) return fail(s, GC_ERR_INVALID, "E is NULL");
     if (N >= 0xffffffffu) return fail(s, GC_ERR_INVALID, "too many vertices");
-    if (recolor < 0) return fail(s, GC_ERR_INVALID, "recolor must be >= 0");
-    if ((int)h < GC_FF || (int)h > GC_GNN) return fail(s, GC_ERR_INVALID, "unknown heuristic");
-    if (h == GC_GNN && (layers < 2 || layers > 7 || !s->have_model[layers]))
-        return fail(s, GC_ERR_INVALID, "no GNN model with " + std::to_string(layers) + " layers was added");
-    return GC_OK;
+    return check_kind(s, h, layers, recolor);
+}
+
+// Host-side check of a CSR to register: rows monotone and ending at M, ids below N.
+bool csr_valid(uint32_t N, const uint32_t *V, const uint32_t *E) {
+    if (V[0] != 0) return false;
+    bool ok = true;
+#pragma omp parallel for reduction(&& : ok) schedule(static)
+    for (int64_t u = 0; u < (int64_t)N; u++) ok = ok && V[u] <= V[u + 1];
+    if (!ok) return false;
+    const int64_t M = V[N];
+#pragma omp parallel for reduction(&& : ok) schedule(static)
+    for (int64_t i = 0; i < M; i++) ok = ok && E[i] < N;
+    return ok;
+}
+
+void free_reg(gc_server *s, Reg *r) {
+    if (r->dV) cudaFreeAsync(r->dV, s->reg_stream);
+    if (r->dE) cudaFreeAsync(r->dE, s->reg_stream);
+    cudaStreamSynchronize(s->reg_stream);
+    delete r;
 }
 
 void fill_info(const Job *j, gc_job_info *info) {
@@ -458,10 +599,22 @@ gc_status gc_serve_create(const gc_serve_config *cfg_in, gc_server **out) {
                 cudaGetLastError();
                 st = GC_ERR_NOMEM;
             }
+        for (int b = 0; b < 2 && st == GC_OK; b++) {
+            if (cudaMallocHost((void **)&L->stage[b], STAGE_BYTES) != cudaSuccess ||
+                cudaEventCreateWithFlags(&L->stage_ev[b], cudaEventDisableTiming) != cudaSuccess) {
+                cudaGetLastError();
+                st = GC_ERR_NOMEM;
+            }
+        }
         if (st == GC_OK && cudaStreamSynchronize(L->ctx->stream) != cudaSuccess) st = GC_ERR_CUDA;
+    }
+    if (st == GC_OK && cudaStreamCreateWithFlags(&s->reg_stream, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaGetLastError();
+        st = GC_ERR_CUDA;
     }
     if (st != GC_OK) {
         for (Lane *L : s->lanes) destroy_lane(L);
+        if (s->reg_stream) cudaStreamDestroy(s->reg_stream);
         cudaMemPoolDestroy(s->pool);
         delete s;
         return st;
@@ -504,9 +657,143 @@ gc_status gc_serve_submit(gc_server *s, uint32_t N, const uint32_t *V, const uin
     if (st != GC_OK) return st;
     std::lock_guard<std::mutex> lk(s->mu);
     if (s->stop) return GC_ERR_STATE;
-    st = submit_locked(s, N, V, E, h, layers, recolor, color_out, Clock::now(), job);
+    st = submit_locked(s, nullptr, N, V, E, h, layers, recolor, color_out, Clock::now(), job);
     if (st == GC_OK) s->cv_work.notify_one();
     return st;
+}
+
+gc_status gc_serve_register(gc_server *s, uint32_t N, const uint32_t *V, const uint32_t *E, uint64_t *graph) {
+    if (!s || !graph || !V) return GC_ERR_INVALID;
+    *graph = 0;
+    if (N >= 0xffffffffu) return fail(s, GC_ERR_INVALID, "too many vertices");
+    const uint32_t M = V[N];
+    if (M && !E) return fail(s, GC_ERR_INVALID, "E is NULL");
+    if (!csr_valid(N, V, E)) return fail(s, GC_ERR_INVALID, "malformed CSR: rows not monotone or an id out of range");
+    const uint64_t bytes = 4ull * ((uint64_t)N + 1) + 4ull * M;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        if (s->reserved + bytes > s->cfg.hbm_budget) {
+            s->st_rejected++;
+            s->last_error = "registering needs " + std::to_string(bytes) + " device bytes beyond the budget";
+            return GC_ERR_BUDGET;
+        }
+        s->reserved += bytes;  // held while the copy runs
+        s->peak_reserved = std::max(s->peak_reserved, s->reserved);
+    }
+    cudaSetDevice(s->device);
+    Reg *r = new Reg();
+    r->N = N;
+    r->M = M;
+    r->bytes = bytes;
+    cudaError_t e = cudaMallocFromPoolAsync((void **)&r->dV, 4ull * ((size_t)N + 1), s->pool, s->reg_stream);
+    if (e == cudaSuccess) e = cudaMallocFromPoolAsync((void **)&r->dE, 4ull * (M ? M : 1), s->pool, s->reg_stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(r->dV, V, 4ull * ((size_t)N + 1), cudaMemcpyHostToDevice, s->reg_stream);
+    if (e == cudaSuccess && M) e = cudaMemcpyAsync(r->dE, E, 4ull * M, cudaMemcpyHostToDevice, s->reg_stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->reg_stream);
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        s->reserved -= bytes;
+        s->last_error = std::string("register: ") + cudaGetErrorString(e);
+        free_reg(s, r);
+        return e == cudaErrorMemoryAllocation ? GC_ERR_NOMEM : GC_ERR_CUDA;
+    }
+    r->id = s->next_reg++;
+    s->regs[r->id] = r;
+    *graph = r->id;
+    return GC_OK;
+}
+
+gc_status gc_serve_unregister(gc_server *s, uint64_t graph) {
+    if (!s) return GC_ERR_INVALID;
+    Reg *r = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        auto it = s->regs.find(graph);
+        if (it == s->regs.end()) return GC_ERR_INVALID;
+        if (it->second->refs) {
+            s->last_error = "graph still has jobs pending or running";
+            return GC_ERR_STATE;
+        }
+        r = it->second;
+        s->regs.erase(it);
+        s->reserved -= r->bytes;
+    }
+    cudaSetDevice(s->device);
+    free_reg(s, r);
+    return GC_OK;
+}
+
+gc_status gc_serve_submit_registered(gc_server *s, uint64_t graph, gc_heuristic h, int layers, int recolor,
+                                     int32_t *color_out, uint64_t *job) {
+    if (!s || !job) return GC_ERR_INVALID;
+    *job = 0;
+    gc_status st = check_kind(s, h, layers, recolor);
+    if (st != GC_OK) return st;
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->stop) return GC_ERR_STATE;
+    auto it = s->regs.find(graph);
+    if (it == s->regs.end()) {
+        s->last_error = "unknown registered graph";
+        return GC_ERR_INVALID;
+    }
+    st = submit_locked(s, it->second, 0, nullptr, nullptr, h, layers, recolor, color_out, Clock::now(), job);
+    if (st == GC_OK) s->cv_work.notify_one();
+    return st;
+}
+
+gc_status gc_serve_replay_registered(gc_server *s, uint32_t J, const double *arrive_s, const uint64_t *graph,
+                                     const int *h, const int *layers, const int *recolor, int32_t *const *color_out,
+                                     gc_job_info *info) {
+    if (!s || (J && (!arrive_s || !graph || !h))) return GC_ERR_INVALID;
+    std::vector<Reg *> regs(J, nullptr);
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        for (uint32_t i = 0; i < J; i++) {
+            auto it = s->regs.find(graph[i]);
+            if (it == s->regs.end()) {
+                s->last_error = "unknown registered graph";
+                return GC_ERR_INVALID;
+            }
+            regs[i] = it->second;
+        }
+    }
+    for (uint32_t i = 0; i < J; i++) {
+        gc_status st = check_kind(s, (gc_heuristic)h[i], layers ? layers[i] : 0, recolor ? recolor[i] : 0);
+        if (st != GC_OK) return st;
+        if (i && arrive_s[i] < arrive_s[i - 1]) return fail(s, GC_ERR_INVALID, "arrival times must not decrease");
+    }
+    std::vector<uint64_t> ids(J, 0);
+    std::vector<gc_status> sub(J, GC_OK);
+    const auto t0 = Clock::now();
+    for (uint32_t i = 0; i < J; i++) {
+        const auto due = t0 + std::chrono::duration_cast<Clock::duration>(std::chrono::duration<double>(arrive_s[i]));
+        for (;;) {
+            const auto now = Clock::now();
+            if (now >= due) break;
+            const auto left = due - now;
+            if (left > std::chrono::microseconds(200)) std::this_thread::sleep_for(left - std::chrono::microseconds(150));
+        }
+        std::lock_guard<std::mutex> lk(s->mu);
+        if (!s->regs.count(graph[i])) {
+            sub[i] = GC_ERR_INVALID;  // released meanwhile by another thread
+            continue;
+        }
+        sub[i] = submit_locked(s, regs[i], 0, nullptr, nullptr, (gc_heuristic)h[i], layers ? layers[i] : 0,
+                               recolor ? recolor[i] : 0, color_out ? color_out[i] : nullptr, due, &ids[i]);
+        if (sub[i] == GC_OK) s->cv_work.notify_one();
+    }
+    gc_status worst = GC_OK;
+    for (uint32_t i = 0; i < J; i++) {
+        gc_status st = sub[i];
+        if (st == GC_OK) st = gc_serve_wait(s, ids[i], info ? info + i : nullptr);
+        else if (info) {
+            memset(info + i, 0, sizeof(gc_job_info));
+            info[i].status = st;
+        }
+        if (st != GC_OK && worst == GC_OK) worst = st;
+    }
+    return worst;
 }
 
 gc_status gc_serve_test(gc_server *s, uint64_t job, int *done) {
@@ -563,7 +850,7 @@ gc_status gc_serve_replay(gc_server *s, uint32_t J, const double *arrive_s, cons
             if (left > std::chrono::microseconds(200)) std::this_thread::sleep_for(left - std::chrono::microseconds(150));
         }
         std::lock_guard<std::mutex> lk(s->mu);
-        sub[i] = submit_locked(s, N[i], V[i], E[i], (gc_heuristic)h[i], layers ? layers[i] : 0,
+        sub[i] = submit_locked(s, nullptr, N[i], V[i], E[i], (gc_heuristic)h[i], layers ? layers[i] : 0,
                                recolor ? recolor[i] : 0, color_out ? color_out[i] : nullptr, due, &ids[i]);
         if (sub[i] == GC_OK) s->cv_work.notify_one();
     }
@@ -647,6 +934,8 @@ void gc_serve_destroy(gc_server *s) {
     cudaSetDevice(s->device);
     for (Lane *L : s->lanes) destroy_lane(L);
     for (auto &kv : s->jobs) delete kv.second;
+    for (auto &kv : s->regs) free_reg(s, kv.second);
+    if (s->reg_stream) cudaStreamDestroy(s->reg_stream);
     if (s->pool) cudaMemPoolDestroy(s->pool);
     delete s;
 }

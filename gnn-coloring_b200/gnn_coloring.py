@@ -177,6 +177,12 @@ _sig("gc_serve_wait", C.c_int, vp, C.c_uint64, C.POINTER(JobInfo))
 _sig("gc_serve_drain", C.c_int, vp)
 _sig("gc_serve_replay", C.c_int, vp, C.c_uint32, f64p, u32p, C.POINTER(u32p), C.POINTER(u32p), C.POINTER(C.c_int),
      C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(i32p), C.POINTER(JobInfo))
+_sig("gc_serve_register", C.c_int, vp, C.c_uint32, u32p, u32p, C.POINTER(C.c_uint64))
+_sig("gc_serve_unregister", C.c_int, vp, C.c_uint64)
+_sig("gc_serve_submit_registered", C.c_int, vp, C.c_uint64, C.c_int, C.c_int, C.c_int, i32p, C.POINTER(C.c_uint64))
+_sig("gc_serve_replay_registered", C.c_int, vp, C.c_uint32, f64p, C.POINTER(C.c_uint64), C.POINTER(C.c_int),
+     C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(i32p), C.POINTER(JobInfo))
+_sig("gc_batch_reupload_device_graphs", C.c_int, vp, vp, C.c_uint32, u32p, u32p, C.POINTER(u32p), C.POINTER(u32p))
 _sig("gc_serve_read_stats", C.c_int, vp, C.POINTER(ServeStats))
 _sig("gc_serve_reset_stats", None, vp)
 _sig("gc_serve_last_error", C.c_char_p, vp)
@@ -251,15 +257,27 @@ def gen_mixed(seed: int, n_min: int = 1000, n_max: int = 200000):
     return N, V, E, kind.value, param.value
 
 
+def _owned(p, count: int) -> np.ndarray:
+    """A uint32 array over a buffer the library malloc'd, freed when the array is collected (no copy:
+    batches reach several GB)."""
+    if count == 0:
+        lib.gc_host_free(C.cast(p, vp))
+        return np.zeros(0, np.uint32)
+    a = np.ctypeslib.as_array(p, shape=(count,))
+    weakref.finalize(a, lib.gc_host_free, C.cast(p, vp))
+    return a
+
+
 def gen_mixed_batch(G: int, seed0: int, n_min: int = 1000, n_max: int = 200000):
     """G mixed graphs as one segmented CSR: (voff, V with global row offsets, E with local ids)."""
     Op, Vp, Ep = u32p(), u32p(), u32p()
     _check(lib.gc_gen_mixed_batch(G, seed0, n_min, n_max, C.byref(Op), C.byref(Vp), C.byref(Ep)),
            what="gen_mixed_batch")
     voff = np.ctypeslib.as_array(Op, shape=(G + 1,)).copy()
-    N = int(voff[G])
-    _, V, E = _take_csr(N, Vp, Ep)
     lib.gc_host_free(C.cast(Op, vp))
+    N = int(voff[G])
+    V = _owned(Vp, N + 1)
+    E = _owned(Ep, int(V[N]))
     return voff, V, E
 
 
@@ -590,6 +608,7 @@ class Server:
             raise GCError(st, "gc_serve_create")
         self.h = h
         self._held = {}
+        self._reg_n = {}
         _live_objects.add(self)
         for params, md in models:
             self.add_model(params, md)
@@ -619,6 +638,48 @@ class Server:
                                         _ptr(out, i32p) if out is not None else None, C.byref(jid)), "submit")
         self._held[jid.value] = (Vc, Ec, out, int(N))
         return jid.value
+
+    def register(self, N: int, V: np.ndarray, E: np.ndarray) -> int:
+        """Uploads a CSR once; returns its id for submit_registered / replay_registered."""
+        Vc, Ec = self._job_arrays(N, V, E)
+        gid = C.c_uint64(0)
+        self._check(lib.gc_serve_register(self.h, int(N), _ptr(Vc, u32p), _ptr(Ec, u32p), C.byref(gid)), "register")
+        self._reg_n[gid.value] = int(N)
+        return gid.value
+
+    def unregister(self, graph: int):
+        self._check(lib.gc_serve_unregister(self.h, graph), "unregister")
+        self._reg_n.pop(graph, None)
+
+    def submit_registered(self, graph: int, heuristic="FF", layers: int = 0, recolor: int = 0,
+                          want_colors: bool = True) -> int:
+        h = HEURISTICS[heuristic] if isinstance(heuristic, str) else int(heuristic)
+        N = self._reg_n[graph]
+        out = np.zeros(max(N, 1), np.int32) if want_colors else None
+        jid = C.c_uint64(0)
+        self._check(lib.gc_serve_submit_registered(self.h, graph, h, layers, recolor,
+                                                   _ptr(out, i32p) if out is not None else None, C.byref(jid)),
+                    "submit registered")
+        self._held[jid.value] = (None, None, out, N)
+        return jid.value
+
+    def replay_registered(self, arrive_s, graphs, heuristics, layers=None, recolor=None, want_colors: bool = False):
+        """Open-loop load on registered graphs: job i runs on graphs[i] (an id) at arrive_s[i] seconds."""
+        J = len(graphs)
+        arr = np.ascontiguousarray(arrive_s, np.float64)
+        ids = (C.c_uint64 * max(J, 1))(*[int(g) for g in graphs])
+        hs = np.array([HEURISTICS[x] if isinstance(x, str) else int(x) for x in heuristics], np.int32)
+        ls = np.array(layers if layers is not None else [0] * J, np.int32)
+        rs = np.array(recolor if recolor is not None else [0] * J, np.int32)
+        outs = [np.zeros(max(self._reg_n[int(g)], 1), np.int32) for g in graphs] if want_colors else None
+        op = (i32p * max(J, 1))(*[_ptr(o, i32p) for o in outs]) if want_colors else None
+        infos = (JobInfo * max(J, 1))()
+        i32 = C.POINTER(C.c_int)
+        st = lib.gc_serve_replay_registered(self.h, J, _ptr(arr, f64p), ids, hs.ctypes.data_as(i32),
+                                            ls.ctypes.data_as(i32), rs.ctypes.data_as(i32), op, infos)
+        self._check(st, "replay registered")
+        cols = [o[: self._reg_n[int(g)]] for o, g in zip(outs, graphs)] if want_colors else None
+        return cols, [infos[i].as_dict() for i in range(J)]
 
     def done(self, job: int) -> bool:
         d = C.c_int(0)

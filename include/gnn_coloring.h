@@ -205,6 +205,11 @@ gc_status gc_batch_reupload_graphs(gc_ctx *ctx, gc_batch *b, uint32_t G, const u
  * without new device allocations; pinned host memory makes the copies asynchronous. */
 gc_status gc_batch_reupload(gc_ctx *ctx, gc_batch *b, uint32_t G, const uint32_t *voff, const uint32_t *V,
                             const uint32_t *E);
+/* Refills an existing batch from G CSRs that already live in device memory (graph g: n[g] vertices,
+ * m[g] directed edges, local row offsets dVs[g] and neighbour ids dEs[g]); one gather kernel copies
+ * them into the batch, no device allocation happens.  The sources are only read. */
+gc_status gc_batch_reupload_device_graphs(gc_ctx *ctx, gc_batch *b, uint32_t G, const uint32_t *n, const uint32_t *m,
+                                          const uint32_t *const *dVs, const uint32_t *const *dEs);
 void gc_batch_free(gc_batch *b);
 uint32_t gc_batch_num_graphs(const gc_batch *b);
 uint32_t gc_batch_num_vertices(const gc_batch *b);
@@ -262,6 +267,9 @@ void gc_tuning_default(gc_tuning *t);
  *              only when that fits what is left.  Such jobs start in arrival order.  A job that
  *              could never fit is refused at submission with GC_ERR_BUDGET.
  *   isolation  a batch that fails is re-run job by job, so a malformed job fails alone.
+ *   resident   graphs registered once stay in device memory; jobs on them skip the upload.
+ *   copies     CSRs of jobs that run alone go up through pinned chunks filled by several host
+ *              threads while the previous chunk's DMA runs; colors come back the same way.
  *
  * The caller's V, E and color_out buffers must stay valid and unchanged until the job is done. */
 typedef struct gc_server gc_server;
@@ -324,6 +332,19 @@ gc_status gc_serve_drain(gc_server *s);
 gc_status gc_serve_replay(gc_server *s, uint32_t J, const double *arrive_s, const uint32_t *N,
                           const uint32_t *const *V, const uint32_t *const *E, const int *h, const int *layers,
                           const int *recolor, int32_t *const *color_out, gc_job_info *info);
+/* Device-resident graphs: gc_serve_register checks a host CSR (rows monotone, ids below N), copies
+ * it to device memory once and returns its id; it stays there, charged 4 (N + 1) + 4 M bytes to the
+ * budget, until gc_serve_unregister (GC_ERR_STATE while jobs on it are pending or running).  Jobs on
+ * a registered graph skip the host-to-device copy; the host arrays may be freed after registering. */
+gc_status gc_serve_register(gc_server *s, uint32_t N, const uint32_t *V, const uint32_t *E, uint64_t *graph);
+gc_status gc_serve_unregister(gc_server *s, uint64_t graph);
+/* gc_serve_submit for a registered graph. */
+gc_status gc_serve_submit_registered(gc_server *s, uint64_t graph, gc_heuristic h, int layers, int recolor,
+                                     int32_t *color_out, uint64_t *job);
+/* gc_serve_replay for registered graphs: job i runs on graph[i]. */
+gc_status gc_serve_replay_registered(gc_server *s, uint32_t J, const double *arrive_s, const uint64_t *graph,
+                                     const int *h, const int *layers, const int *recolor, int32_t *const *color_out,
+                                     gc_job_info *info);
 gc_status gc_serve_read_stats(gc_server *s, gc_serve_stats *st);
 void gc_serve_reset_stats(gc_server *s);
 const char *gc_serve_last_error(gc_server *s);

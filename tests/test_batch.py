@@ -266,3 +266,40 @@ def test_batch_rejects_bad_input(gpu_ctx, models):
     ok = gcn.Batch(gpu_ctx, graphs=graphs)
     assert (ok.color("FF") > 0).all()
     ok.close()
+
+
+@pytest.mark.gpu
+def test_reupload_from_device_graphs(gpu_ctx, models):
+    """gc_batch_reupload_device_graphs: a batch gathered from device-resident CSRs colors exactly like
+    the same graphs uploaded from host memory."""
+    import ctypes as C
+    import torch
+    graphs = _small_mixed(9, 600) + _edge_cases()
+    dev = [(torch.from_numpy(V.astype(np.int32)).cuda(), torch.from_numpy(E.astype(np.int32) if len(E) else
+                                                                           np.zeros(1, np.int32)).cuda())
+           for _, V, E in graphs]
+    torch.cuda.synchronize()
+    G = len(graphs)
+    b = gcn.Batch(gpu_ctx, graphs=graphs)
+    ref_counts = b.color("GNN", models[3])
+    ref = b.colors()
+    bh = C.c_void_p()
+    gpu_ctx.check(gcn.lib.gc_batch_create(gpu_ctx.h, G + 3, b.N + 10, b.M + 10, C.byref(bh)), "create")
+    n = np.array([g[0] for g in graphs], np.uint32)
+    m = np.array([int(g[1][-1]) for g in graphs], np.uint32)
+    u32p = C.POINTER(C.c_uint32)
+    dVs = (u32p * G)(*[C.cast(v.data_ptr(), u32p) for v, _ in dev])
+    dEs = (u32p * G)(*[C.cast(e.data_ptr(), u32p) for _, e in dev])
+    for _ in range(2):  # twice: the second refill reuses the first one's buffers
+        gpu_ctx.check(gcn.lib.gc_batch_reupload_device_graphs(gpu_ctx.h, bh, G, n.ctypes.data_as(u32p),
+                                                              m.ctypes.data_as(u32p), dVs, dEs), "refill")
+        counts = np.zeros(G, np.int32)
+        gpu_ctx.check(gcn.lib.gc_batch_color_once(gpu_ctx.h, bh, gcn.GC_GNN, models[3].h, 0,
+                                                  counts.ctypes.data_as(C.POINTER(C.c_int32))), "color")
+        got = np.zeros(max(b.N, 1), np.int32)
+        gpu_ctx.check(gcn.lib.gc_batch_download_colors(gpu_ctx.h, bh, got.ctypes.data_as(C.POINTER(C.c_int32))),
+                      "colors")
+        assert np.array_equal(counts, ref_counts)
+        assert np.array_equal(got[: b.N], ref)
+    gcn.lib.gc_batch_free(bh)
+    b.close()

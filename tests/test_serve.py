@@ -228,3 +228,72 @@ def test_open_loop_replay(gpu_ctx, models, model_params):
             cache[key] = _alone(gpu_ctx, models, pool[which[i]], names[i])
         assert np.array_equal(cols[i], cache[key][0]), (i, key)
         assert infos[i]["colors"] == cache[key][1]
+
+
+@pytest.mark.gpu
+def test_registered_graphs(gpu_ctx, models, model_params):
+    """Device-resident graphs: jobs on them (batched or alone, concurrently with host-CSR jobs) equal
+    their graphs colored alone; a graph with jobs outstanding cannot be released; releasing returns
+    its budget charge."""
+    srv = _server(model_params, lanes=3, batch_max_job_vertices=4000)
+    base = srv.stats()["reserved_bytes"]
+    graphs = _small_graphs(10, seed0=8000) + [gcn.gen_rmat(1 << 14, 16, 81)]
+    ids = [srv.register(*g) for g in graphs]
+    charged = sum(4 * (g[0] + 1) + 4 * int(g[1][-1]) for g in graphs)
+    assert srv.stats()["reserved_bytes"] == base + charged
+    names = ["FF", "LLF", "GNN3", "LF", "GNN2", "SLL"]
+    jobs = []
+    for rep in range(3):
+        for k, gid in enumerate(ids):
+            name = names[(k + rep) % len(names)]
+            heur, layers = _heur_args(name)
+            jobs.append((k, name, srv.submit_registered(gid, heur, layers)))
+    host = [srv.submit(*graphs[k], heuristic="FF") for k in range(3)]
+    with pytest.raises(gcn.GCError) as e:
+        srv.unregister(ids[-1])
+    assert e.value.name == "GC_ERR_STATE"
+    for k, name, jid in jobs:
+        col, info = srv.wait(jid)
+        ref_col, ref_count = _alone(gpu_ctx, models, graphs[k], name)
+        assert np.array_equal(col, ref_col), (k, name)
+        assert info.colors == ref_count
+    for k, jid in enumerate(host):
+        col, _ = srv.wait(jid)
+        assert np.array_equal(col, _alone(gpu_ctx, models, graphs[k], "FF")[0])
+    st = srv.stats()
+    assert st["batched_jobs"] > 0 and st["failed"] == 0
+    for gid in ids:
+        srv.unregister(gid)
+    assert srv.stats()["reserved_bytes"] == base
+    # a malformed CSR is refused at registration
+    N, V, E = graphs[0]
+    E_bad = E.copy()
+    E_bad[0] = N
+    with pytest.raises(gcn.GCError) as e:
+        srv.register(N, V, E_bad)
+    assert e.value.name == "GC_ERR_INVALID"
+    srv.close()
+
+
+@pytest.mark.gpu
+def test_registered_replay(gpu_ctx, models, model_params):
+    rng = np.random.default_rng(3)
+    graphs = _small_graphs(8, seed0=9000, n_max=20000) + [gcn.gen_rmat(1 << 15, 16, 91)]
+    srv = _server(model_params, lanes=4, batch_max_job_vertices=20000)
+    ids = [srv.register(*g) for g in graphs]
+    J = 120
+    which = [int(rng.integers(len(graphs))) for _ in range(J)]
+    names = [["FF", "LLF", "GNN3"][int(rng.integers(3))] for _ in range(J)]
+    arrive = np.cumsum(rng.exponential(1.0 / 3000.0, J))
+    heur = [_heur_args(n) for n in names]
+    cols, infos = srv.replay_registered(arrive, [ids[w] for w in which], [h for h, _ in heur],
+                                        layers=[l for _, l in heur], want_colors=True)
+    st = srv.stats()
+    srv.close()
+    assert st["completed"] == J and st["failed"] == 0 and st["p99_ms"] >= st["p50_ms"] > 0
+    cache = {}
+    for i in range(J):
+        key = (which[i], names[i])
+        if key not in cache:
+            cache[key] = _alone(gpu_ctx, models, graphs[which[i]], names[i])
+        assert np.array_equal(cols[i], cache[key][0]) and infos[i]["colors"] == cache[key][1], (i, key)
