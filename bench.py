@@ -487,12 +487,14 @@ def serving_jobs(pool, J: int, seed: int):
 
 
 def _sweep(srv, pool, J, replay, alone_counts):
-    """Poisson arrivals at each rate of SERVE_RATES (J jobs each) through `replay`; per-rate latency
-    percentiles and throughput from the server's own statistics."""
+    """Poisson arrivals at each rate of SERVE_RATES (J jobs, more at high rates: up to 2 s of arrivals,
+    at most 1,500) through `replay`; per-rate latency percentiles and throughput from the server's
+    own statistics."""
     sweep, same = [], True
     for i, rate in enumerate(SERVE_RATES):
-        jobs = serving_jobs(pool, J, 1000 + i)
-        arrive = np.cumsum(np.random.default_rng(2000 + i).exponential(1.0 / rate, J))
+        Jr = max(J, min(1500, 2 * rate))  # enough large jobs at the high rates for a stable edges/s
+        jobs = serving_jobs(pool, Jr, 1000 + i)
+        arrive = np.cumsum(np.random.default_rng(2000 + i).exponential(1.0 / rate, Jr))
         srv.reset_stats()
         infos = replay(arrive, jobs)
         st = srv.stats()
@@ -500,7 +502,7 @@ def _sweep(srv, pool, J, replay, alone_counts):
             c = alone_counts.get((id(gr), h))
             if c is not None and c != inf["colors"]:
                 same = False
-        sweep.append({"offered_jobs_per_s": rate, "jobs": J, "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
+        sweep.append({"offered_jobs_per_s": rate, "jobs": Jr, "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
                       "max_ms": st["max_ms"], "edges_per_s": st["edges_per_s"],
                       "jobs_per_s": st["completed"] / st["span_s"] if st["span_s"] else None,
                       "passes": st["launches"], "batched_jobs": st["batched_jobs"],
