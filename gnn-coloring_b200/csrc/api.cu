@@ -107,7 +107,7 @@ void gc_graph_free_buffers(gc_graph *g) {
     void *bufs[] = {g->key,       g->color,  g->P,        g->pc,       g->order,    g->sort_buf, g->sort_hist,
                     g->big,       g->hubs,   g->x,        g->y,        g->t01,      g->deg_rem,  g->frontier,
                     g->frontier2, g->removed, g->leaf_list, g->vorder, g->rank,     g->p64,      g->seg_voff,
-                    g->seg_stat};
+                    g->seg_stat,  g->fmask,    g->giant,    g->hub_stage};
     for (void *p : bufs) gc_dev_free(ctx, p);
 }
 
@@ -190,8 +190,9 @@ gc_status gc_ctx_create(int device, gc_ctx **out) {
     // tuning of the coloring kernel's polling (defaults measured on B200)
     if (const char *e = getenv("GC_JP_CTAS_PER_SM")) ctx->jp_ctas_per_sm = atoi(e);
     if (const char *e = getenv("GC_JP_TIGHT")) ctx->jp_tight = (unsigned int)strtoul(e, nullptr, 10);
+    if (const char *e = getenv("GC_JP_DECIDE")) ctx->jp_decide = atoi(e) != 0;
     if (const char *e = getenv("GC_JP_NAP")) ctx->jp_nap = (unsigned int)strtoul(e, nullptr, 10);
-    if (const char *e = getenv("GC_GNN_SERIAL")) ctx->gnn_serial = atoi(e) != 0;  // 0: overlap hubs and bulk
+    if (const char *e = getenv("GC_GNN_SERIAL")) ctx->gnn_serial = atoi(e) != 0;  // 1: hubs first, then the bulk
     if (s != GC_OK) {
         gc_ctx_destroy(ctx);
         return s;

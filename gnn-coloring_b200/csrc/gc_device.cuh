@@ -46,6 +46,14 @@ __device__ __forceinline__ unsigned int ld_relaxed_u32(const unsigned int *p) {
 __device__ __forceinline__ void st_relaxed(int *p, int v) {
     asm volatile("st.relaxed.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
+__device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long *p) {
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_relaxed_u64(unsigned long long *p, unsigned long long v) {
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
 
 // Streaming load (evict-first): CSR edge arrays are read once per pass.
 __device__ __forceinline__ uint32_t ld_stream(const uint32_t *p) { return __ldcs(p); }

@@ -27,8 +27,9 @@ struct gc_ctx {
     int jp_ctas_per_sm = 2;              // CTAs per SM of the coloring kernel: fewer pollers beat more lookahead (measured)
     unsigned int jp_tight = 32;          // coloring: unproductive polling rounds before sleeping
     unsigned int jp_nap = 32;            // coloring: first sleep between polling rounds (ns)
+    bool jp_decide = true;               // coloring: early decisions from published forbidden colors
     int gnn_blocks_per_sm[3] = {0, 0, 0};  // resident CTAs of each GNN layer kernel
-    bool gnn_serial = true;              // hub CTAs before the bulk (measured faster than beside it)
+    bool gnn_serial = false;             // hub CTAs beside the bulk on a high-priority stream (GC_GNN_SERIAL=1: before it)
     bool hub_smem_set[3] = {false, false, false};  // hub kernels' shared-memory limit raised
     cudaMemPool_t pool = nullptr;        // when set, graph buffers are stream-ordered allocations from this pool
     gc::DevState *dstate = nullptr;      // device status block
@@ -60,6 +61,13 @@ constexpr uint32_t GC_GNN_WARP_DEGREE = 256;
 // Hubs (more than GC_GNN_HUB_DEGREE neighbours) are split across several warps in the JP split
 // pass, this many edges per warp task.
 constexpr uint32_t GC_SPLIT_CHUNK = 1024;  // edges per warp task (shared-memory buffer per warp)
+constexpr int GC_JP_MASK_WORDS = 8;        // published forbidden colors: 8 x 32 = colors 1..256
+// Giant hubs: hubs with at least max(2 * hub degree, largest hub degree / 3) neighbours.  One SM
+// gathers scattered 64-byte rows at only about 11 GB/s, so before each GNN layer all SMs copy these
+// hubs' neighbour rows, in CSR order, into a contiguous staging buffer that the hub's chain then
+// streams with bulk copies.  GC_GIANT_TASK rows per gather task; at most GC_GIANT_MAX_ROWS rows.
+constexpr uint32_t GC_GIANT_TASK = 2048;
+constexpr uint64_t GC_GIANT_MAX_ROWS = 1ull << 25;
 
 struct gc_graph {
     gc_ctx *ctx = nullptr;
@@ -79,6 +87,10 @@ struct gc_graph {
     uint32_t *order = nullptr;  // vertices by descending key, ascending id on ties: the ticket order
     uint32_t *leaf_list = nullptr;  // leaves too large for one thread
     uint32_t *rank = nullptr;       // ticket of each ordered vertex (all ones elsewhere)
+    // forbidden colors 1..256 published by waiting vertices of the ordered coloring kernel:
+    // GC_JP_MASK_WORDS words per vertex, each (epoch << 32 | 32 color bits); the word after the
+    // last vertex's holds the epoch counter, advanced once per coloring run
+    unsigned long long *fmask = nullptr;
     uint32_t *sort_buf = nullptr;  // radix sort ping-pong (keys and values), 4 * cap_N words
     uint32_t *sort_hist = nullptr;
     uint32_t sort_hist_cap = 0;
@@ -86,8 +98,16 @@ struct gc_graph {
     uint32_t *big = nullptr;         // split tasks of the hubs: (vertex, first edge) pairs
     uint32_t n_big_tasks = 0;
     size_t big_cap = 0;              // words allocated for `big`
-    uint32_t *hubs = nullptr;        // vertices with deg > GC_GNN_HUB_DEGREE
+    uint32_t *hubs = nullptr;        // vertices with deg > GC_GNN_HUB_DEGREE, by descending degree
     uint32_t n_hubs = 0;
+    // the leading n_giant hubs are giant: giant[0..n_giant] their staging row offsets (even, so
+    // 8-byte rows start 16-byte aligned), then n_giant_tasks (hub slot, first row) gather tasks
+    uint32_t n_giant = 0, n_giant_tasks = 0;
+    uint32_t *giant = nullptr;
+    size_t giant_cap = 0;            // words allocated for `giant`
+    uint64_t giant_rows = 0;         // staging rows
+    float *hub_stage = nullptr;      // GNN: giant_rows + 2 rows of 16 floats (allocated on first use)
+    uint64_t hub_stage_rows = 0;
     uint32_t *vorder = nullptr;      // the other vertices by descending degree (GNN schedule)
     uint32_t n_vorder = 0;
     uint32_t n_wide = 0;             // leading vorder entries with more than GC_GNN_WARP_DEGREE neighbours

@@ -283,8 +283,15 @@ __global__ void __launch_bounds__(GNN_THREADS, 4) k_gnn_layer(const uint32_t *__
 // on expiry the kernel raises ERR_WAIT_EXPIRED and returns.
 constexpr int HUB_THREADS = 64;    // warp 0 adds, warp 1 loads
 constexpr int HUB_ROWS = 128;      // rows per stage: 4 per producer lane
-constexpr int HUB_STAGES = 12;
-constexpr int HUB_ID_AHEAD = 4;    // the producer reads neighbour ids this many stages early
+#ifndef GC_HUB_STAGES
+#define GC_HUB_STAGES 12
+#endif
+constexpr int HUB_STAGES = GC_HUB_STAGES;
+#ifndef GC_HUB_ID_AHEAD
+#define GC_HUB_ID_AHEAD 4
+#endif
+constexpr int HUB_ID_AHEAD = GC_HUB_ID_AHEAD;  // the producer reads neighbour ids this many stages early
+constexpr int HUB_BATCH = 16;      // staged values the consumer loads ahead of its add chain
 constexpr unsigned int HUB_WAIT_LIMIT = 1u << 20;  // each try_wait may also suspend briefly
 
 __device__ __forceinline__ unsigned int smem_u32(const void *p) { return (unsigned int)__cvta_generic_to_shared(p); }
@@ -315,19 +322,75 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned int parity, De
     raise_error(st, ERR_WAIT_EXPIRED, 0xffffffffu);
     return false;
 }
-__device__ __forceinline__ void cp_async_16(void *smem, const void *gmem) {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(smem)), "l"(gmem) : "memory");
-}
 __device__ __forceinline__ void cp_async_8(void *smem, const void *gmem) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(smem)), "l"(gmem) : "memory");
 }
+// A contiguous block by the TMA engine: `bytes` (a multiple of 16; both addresses 16-byte aligned)
+// from global to this CTA's shared memory, completing `bytes` of the mbarrier's transaction count.
+__device__ __forceinline__ void bulk_g2s(void *smem, const void *gmem, unsigned int bytes, uint64_t *bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(smem)),
+                 "l"(gmem), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, unsigned int bytes) {
+    asm volatile("{\n .reg .b64 st;\n mbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n}" ::"r"(smem_u32(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_16(void *smem, const void *gmem) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(smem)), "l"(gmem) : "memory");
+}
 
+// Giant hubs' neighbour rows, in CSR order, into the staging buffer: all SMs, one warp per task of
+// GC_GIANT_TASK rows; four lanes per 64-byte row (one lane per 8-byte input-layer row).
+template <int MODE>
+__global__ void __launch_bounds__(256) k_gnn_hub_gather(const uint32_t *__restrict__ V, const uint32_t *__restrict__ E,
+                                                        const uint32_t *__restrict__ hubs,
+                                                        const uint32_t *__restrict__ giant, uint32_t n_giant,
+                                                        uint32_t n_tasks, const float2 *__restrict__ t01,
+                                                        const float *__restrict__ x, float *__restrict__ stage) {
+    const uint32_t *tasks = giant + n_giant + 1;
+    const int lane = threadIdx.x & 31, q = lane & 3;
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t t = warp; t < n_tasks; t += nwarps) {
+        const uint32_t slot = tasks[2 * t], r0 = tasks[2 * t + 1];
+        const uint32_t u = hubs[slot], base = V[u], d = V[u + 1] - base;
+        const uint32_t rend = min(d, r0 + GC_GIANT_TASK);
+        const size_t off = giant[slot];
+        if (MODE == MODE_INPUT) {
+            float2 *dst = reinterpret_cast<float2 *>(stage) + off;
+            for (uint32_t r = r0 + lane; r < rend; r += 32) dst[r] = t01[ld_stream(E + base + r)];
+        } else {
+            const float4 *X4 = reinterpret_cast<const float4 *>(x);
+            float4 *dst = reinterpret_cast<float4 *>(stage) + off * 4;
+            for (uint32_t r = r0 + (lane >> 2); r < rend; r += 32) {
+                uint32_t v[4];
+                float4 val[4];
+#pragma unroll
+                for (int k = 0; k < 4; k++) v[k] = r + 8 * k < rend ? E[base + r + 8 * k] : 0u;
+#pragma unroll
+                for (int k = 0; k < 4; k++)
+                    if (r + 8 * k < rend) val[k] = X4[(size_t)v[k] * 4 + q];
+#pragma unroll
+                for (int k = 0; k < 4; k++)
+                    if (r + 8 * k < rend) dst[(size_t)(r + 8 * k) * 4 + q] = val[k];
+            }
+        }
+    }
+}
+
+// Giant hubs (blockIdx.x < n_giant: the leading, largest hubs) read their rows from the staging
+// buffer: one bulk copy per stage by the producer's lane 0.  The others gather rows with cp.async.
 template <int MODE>
 __global__ void __launch_bounds__(HUB_THREADS) k_gnn_hub(const uint32_t *__restrict__ V, const uint32_t *__restrict__ E,
                                                          const uint32_t *__restrict__ hubs,
                                                          const float2 *__restrict__ t01, const float *__restrict__ x,
                                                          float *__restrict__ y, uint32_t *__restrict__ key,
-                                                         const float *__restrict__ Wb, DevState *st) {
+                                                         const float *__restrict__ Wb, DevState *st,
+                                                         const float *__restrict__ staged_rows,
+                                                         const uint32_t *__restrict__ giant, uint32_t n_giant) {
     constexpr int ROW = (MODE == MODE_INPUT) ? 2 : FEAT;  // floats per staged row
     extern __shared__ __align__(16) float stage[];         // HUB_STAGES * HUB_ROWS * ROW floats
     __shared__ __align__(16) float sW[LAYER_PARAMS];
@@ -335,7 +398,9 @@ __global__ void __launch_bounds__(HUB_THREADS) k_gnn_hub(const uint32_t *__restr
     for (int i = threadIdx.x; i < LAYER_PARAMS; i += blockDim.x) sW[i] = Wb[i];
     if (threadIdx.x == 0) {
         for (int i = 0; i < HUB_STAGES; i++) {
-            mbar_init(&full[i], 32);  // one copy-completion arrival per producer lane
+            // staged: the producer's expect-tx arrival, completed by the bulk copy's bytes;
+            // otherwise one copy-completion arrival per producer lane
+            mbar_init(&full[i], blockIdx.x < n_giant ? 1 : 32);
             mbar_init(&empty[i], 1);  // the consumer's release
         }
     }
@@ -345,6 +410,22 @@ __global__ void __launch_bounds__(HUB_THREADS) k_gnn_hub(const uint32_t *__restr
     const uint32_t nchunks = (d + HUB_ROWS - 1) / HUB_ROWS;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
+    const bool staged = blockIdx.x < n_giant;
+    if (warp == 1 && staged) {
+        if (lane == 0) {
+            constexpr uint32_t ROWB = ROW * sizeof(float);  // 64 bytes (8 in the input layer)
+            const char *src = reinterpret_cast<const char *>(staged_rows) + (size_t)giant[blockIdx.x] * ROWB;
+            for (uint32_t c = 0; c < nchunks; c++) {
+                const uint32_t s = c % HUB_STAGES;
+                if (c >= HUB_STAGES && !mbar_wait(&empty[s], ((c / HUB_STAGES) - 1) & 1u, st)) return;
+                const uint32_t rows = min((uint32_t)HUB_ROWS, d - c * HUB_ROWS);
+                const uint32_t bytes = (rows * ROWB + 15u) & ~15u;  // an odd 8-byte row count reads one pad row
+                mbar_arrive_expect_tx(&full[s], bytes);
+                bulk_g2s(stage + (size_t)s * HUB_ROWS * ROW, src + (size_t)c * HUB_ROWS * ROWB, bytes, &full[s]);
+            }
+        }
+        return;
+    }
     if (warp == 1) {
         // producer: ids HUB_ID_AHEAD stages ahead in registers, rows via cp.async
         uint32_t ids[HUB_ID_AHEAD][4];
@@ -364,17 +445,24 @@ __global__ void __launch_bounds__(HUB_THREADS) k_gnn_hub(const uint32_t *__restr
                 return;
             }
             float *buf = stage + (size_t)s * HUB_ROWS * ROW;
+            if (MODE == MODE_INPUT) {
 #pragma unroll
-            for (int k = 0; k < 4; k++) {
-                const uint32_t v = ids[0][k];
-                if (v != 0xffffffffu) {
-                    float *dst = buf + (size_t)(k * 32 + lane) * ROW;
-                    if (MODE == MODE_INPUT) {
-                        cp_async_8(dst, t01 + v);
-                    } else {
-                        const float *src = x + (size_t)v * FEAT;
+                for (int k = 0; k < 4; k++) {
+                    const uint32_t v = ids[0][k];
+                    if (v != 0xffffffffu) cp_async_8(buf + (size_t)(k * 32 + lane) * ROW, t01 + v);
+                }
+            } else {
+                // four adjacent lanes copy the four 16-byte pieces of one row: each instruction
+                // moves eight whole 64-byte rows (two sectors each) rather than 32 scattered pieces
+                const int piece = lane & 3;
 #pragma unroll
-                        for (int w = 0; w < 4; w++) cp_async_16(dst + 4 * w, src + 4 * w);
+                for (int k = 0; k < 4; k++) {
+#pragma unroll
+                    for (int j = 0; j < 4; j++) {
+                        const int r = j * 8 + (lane >> 2);  // row k * 32 + r of the stage
+                        const uint32_t v = __shfl_sync(0xffffffffu, ids[0][k], r);
+                        if (v != 0xffffffffu)
+                            cp_async_16(buf + (size_t)(k * 32 + r) * ROW + 4 * piece, x + (size_t)v * FEAT + 4 * piece);
                     }
                 }
             }
@@ -394,13 +482,34 @@ __global__ void __launch_bounds__(HUB_THREADS) k_gnn_hub(const uint32_t *__restr
     float acc = 0.0f;
     for (uint32_t c = 0; c < nchunks; c++) {
         const uint32_t s = c % HUB_STAGES;
-        if (!mbar_wait(&full[s], (c / HUB_STAGES) & 1u, st)) return;
+        if (!mbar_wait(&full[s], (c / HUB_STAGES) & 1u, st)) {
+            // staged: the bulk copies already issued into this CTA's shared memory must land
+            // before it exits (each wait again bounded); the producer stops at its next wait
+            if (staged)
+                for (uint32_t k = c + 1; k < nchunks && k < c + HUB_STAGES; k++)
+                    mbar_wait(&full[k % HUB_STAGES], (k / HUB_STAGES) & 1u, st);
+            return;
+        }
         const float *buf = stage + (size_t)s * HUB_ROWS * ROW;
         const uint32_t cnt = min((uint32_t)HUB_ROWS, end - (beg + c * HUB_ROWS));
         if (lane < ROW) {
             if (cnt == HUB_ROWS) {
-#pragma unroll 32
-                for (uint32_t r = 0; r < HUB_ROWS; r++) acc = __fadd_rn(acc, buf[r * ROW + lane]);
+                // software pipeline: the next HUB_BATCH staged values are loaded while the current
+                // ones are added, so the chain runs at the add latency, not the shared-load latency
+                float cur[HUB_BATCH], nxt[HUB_BATCH];
+#pragma unroll
+                for (int k = 0; k < HUB_BATCH; k++) cur[k] = buf[k * ROW + lane];
+#pragma unroll
+                for (int r = 0; r < HUB_ROWS; r += HUB_BATCH) {
+                    if (r + HUB_BATCH < HUB_ROWS) {
+#pragma unroll
+                        for (int k = 0; k < HUB_BATCH; k++) nxt[k] = buf[(r + HUB_BATCH + k) * ROW + lane];
+                    }
+#pragma unroll
+                    for (int k = 0; k < HUB_BATCH; k++) acc = __fadd_rn(acc, cur[k]);
+#pragma unroll
+                    for (int k = 0; k < HUB_BATCH; k++) cur[k] = nxt[k];
+                }
             } else {
                 for (uint32_t r = 0; r < cnt; r++) acc = __fadd_rn(acc, buf[r * ROW + lane]);
             }
@@ -464,8 +573,14 @@ gc_status launch_layer(gc_graph *g, const float *Wb, const float *x, float *y, c
         if ((s = gc_check_cuda(ctx, cudaStreamWaitEvent(side, fork, 0), "fork")) != GC_OK) return s;
         ProfScope ps(ctx, MODE == MODE_INPUT ? "gnn_hub_input" : (MODE == MODE_HIDDEN ? "gnn_hub_hidden" : "gnn_hub_output"),
                      side);
+        if (g->n_giant) {
+            ProfScope pg(ctx, "gnn_hub_gather", side);
+            k_gnn_hub_gather<MODE><<<ctx->num_sms * 4, 256, 0, side>>>(g->V, g->E, g->hubs, g->giant, g->n_giant,
+                                                                        g->n_giant_tasks, g->t01, x, g->hub_stage);
+            ctx->launches++;
+        }
         k_gnn_hub<MODE><<<g->n_hubs, HUB_THREADS, smem, side>>>(g->V, g->E, g->hubs, g->t01, x, y, g->key, Wb,
-                                                                ctx->dstate);
+                                                                ctx->dstate, g->hub_stage, g->giant, g->n_giant);
         ctx->launches++;
         if ((s = gc_check_launch(ctx, "gnn hub layer")) != GC_OK) return s;
     }
@@ -503,6 +618,12 @@ gc_status gc_priority_gnn(gc_graph *g, const gc_model *m) {
     if ((s = gc_alloc(ctx, &g->x, rows * FEAT, "gnn features")) != GC_OK) return s;
     if ((s = gc_alloc(ctx, &g->y, rows * FEAT, "gnn features")) != GC_OK) return s;
     if ((s = gc_alloc(ctx, &g->t01, rows, "gnn input table")) != GC_OK) return s;
+    if (g->n_giant && g->hub_stage_rows < g->giant_rows + 2) {
+        gc_dev_free(ctx, g->hub_stage);
+        g->hub_stage = nullptr;
+        if ((s = gc_alloc(ctx, &g->hub_stage, (size_t)(g->giant_rows + 2) * FEAT, "giant hub rows")) != GC_OK) return s;
+        g->hub_stage_rows = g->giant_rows + 2;
+    }
     if (ctx->side_stream == nullptr) {
         int lo = 0, hi = 0;
         cudaDeviceGetStreamPriorityRange(&lo, &hi);

@@ -15,6 +15,14 @@
 //                0, builds a forbidden-color bitmap in shared memory and stores the mex.  A warp
 //                only ever waits on vertices with smaller tickets, which are held by running warps
 //                or done, so the oldest unfinished ticket always progresses.
+//                Early decisions shorten the waits (the critical path is the DAG's depth): a warp
+//                with few predecessors left takes the candidate c = mex(colors seen so far) at once
+//                when every pending predecessor v provably cannot end up with color c, because
+//                pc[v] + 1 < c (v's color is at most its predecessor count + 1) or because one of
+//                v's own predecessors already has color c (v's color is the mex of those).  The
+//                second fact comes from v's warp, which publishes the colors it has seen
+//                (colors 1..256) while it waits.  Every published bit is a final color, so the
+//                decision is exact: the final mex is c whatever the pending colors turn out to be.
 //
 // Colors are published with relaxed GPU-scope stores and read with relaxed GPU-scope loads: the
 // color value is itself the whole message, so no fences are needed.
@@ -229,6 +237,14 @@ __device__ int color_one(const uint32_t *__restrict__ list, uint32_t cnt, const 
 
 constexpr int COLOR_WARPS_PER_CTA = 8;
 constexpr int PENDING = 128;  // per warp: uncolored predecessors remembered for polling
+constexpr uint32_t DECIDE_MAX = 32;  // early decisions are tried with at most this many predecessors pending
+
+// Publishes the warp's forbidden colors 1..256 (window 0 of its bitmap) for vertex `self`, tagged
+// with the run's epoch.  Lanes 0..7, one 64-bit word each.
+__device__ __forceinline__ void publish_mask(unsigned long long *fmask, uint32_t self, unsigned long long tag,
+                                             const uint32_t *fb, int lane) {
+    if (lane < GC_JP_MASK_WORDS) st_relaxed_u64(fmask + (size_t)self * GC_JP_MASK_WORDS + lane, tag | fb[lane]);
+}
 
 // Colors one ordered vertex whose predecessors are list[0..cnt): the smallest color >= 1 none of
 // them has.  Every predecessor color is read first without waiting (LOADS per lane in flight);
@@ -236,9 +252,13 @@ constexpr int PENDING = 128;  // per warp: uncolored predecessors remembered for
 // re-read (one global load each) until colored: back to back at first, then with growing sleeps.
 // Pending-list overflow (more than PENDING uncolored predecessors) waits in place.  Returns -1
 // when a wait exceeded spin_limit rounds or another warp raised the error flag.
+// With `fmask` set, the warp also publishes the colors it has seen (for vertex `self`) while it
+// waits, and tries early decisions once at most DECIDE_MAX predecessors are pending.
 __device__ int color_one_v(const uint32_t *__restrict__ list, uint32_t cnt, const int *color, uint32_t *fb,
                            uint32_t *pend, int lane, DevState *st, unsigned int spin_limit, unsigned int tight,
-                           unsigned int nap) {
+                           unsigned int nap, const uint32_t *__restrict__ pc, unsigned long long *fmask,
+                           uint32_t epoch, uint32_t self) {
+    const unsigned long long tag = (unsigned long long)epoch << 32;
     for (uint32_t window = 0;; window++) {
         fb[lane] = 0;
         __syncwarp();
@@ -281,24 +301,55 @@ __device__ int color_one_v(const uint32_t *__restrict__ list, uint32_t cnt, cons
             }
         }
         __syncwarp();
+        const bool publish = fmask && window == 0 && npend > 0;
+        if (publish) publish_mask(fmask, self, tag, fb, lane);
         // poll the pending list: lane l re-reads entries l, l + 32, ...
+        uint32_t nleft = npend;  // pending entries after the last round (warp-uniform)
         unsigned int spins = 0;
         for (;;) {
-            bool left = false, progress = false;
+            // the candidate of an early decision: the mex of the colors seen so far
+            int cand = 0;
+            if (fmask && nleft <= DECIDE_MAX) {
+                __syncwarp();
+                cand = window_mex(fb, lane, window);
+            }
+            bool progress = false, undecided = false;
+            uint32_t mine = 0;
             for (uint32_t i = lane; i < npend && !gave_up; i += 32) {
                 const uint32_t v = pend[i];
                 if (v == 0xffffffffu) continue;
                 const int cc = ld_relaxed(color + v);
+                bool excluded = false;  // v cannot end up with color cand
+                if (cand > 0 && cc == 0) {
+                    excluded = __ldg(pc + v) + 1u < (uint32_t)cand;
+                    if (!excluded && cand <= 32 * GC_JP_MASK_WORDS) {
+                        const unsigned long long w =
+                            ld_relaxed_u64(fmask + (size_t)v * GC_JP_MASK_WORDS + ((uint32_t)(cand - 1) >> 5));
+                        excluded = (uint32_t)(w >> 32) == epoch && ((w >> ((uint32_t)(cand - 1) & 31u)) & 1ull);
+                    }
+                }
                 if (cc) {
                     mark(fb, cc, window);
                     pend[i] = 0xffffffffu;
                     progress = true;
+                    if (cc == cand) undecided = true;  // the candidate is taken
                 } else {
-                    left = true;
+                    mine++;
+                    if (!excluded) undecided = true;
                 }
             }
-            if (!__any_sync(0xffffffffu, left && !gave_up)) break;
-            if (!__any_sync(0xffffffffu, progress)) {
+            if (cand > 0 && !__any_sync(0xffffffffu, undecided || gave_up)) {
+                __syncwarp();
+                return cand;  // every pending predecessor is excluded from cand: the mex is cand
+            }
+            nleft = __reduce_add_sync(0xffffffffu, mine);
+            if (nleft == 0 || __any_sync(0xffffffffu, gave_up)) break;
+            if (__any_sync(0xffffffffu, progress)) {
+                if (publish) {
+                    __syncwarp();
+                    publish_mask(fmask, self, tag, fb, lane);
+                }
+            } else {
                 if (++spins > spin_limit || ((spins & 255u) == 0 && ld_relaxed_u32(&st->err))) gave_up = true;
                 else if (spins > tight) __nanosleep(spins > 16 * tight + 64 ? 4 * nap : nap);
             }
@@ -319,11 +370,14 @@ __global__ void __launch_bounds__(COLOR_WARPS_PER_CTA * 32) k_jp_color(const uin
                                                                        const uint32_t *__restrict__ pc,
                                                                        const uint32_t *__restrict__ order, int *color,
                                                                        DevState *st, unsigned int spin_limit,
-                                                                       unsigned int tight, unsigned int nap) {
+                                                                       unsigned int tight, unsigned int nap,
+                                                                       unsigned long long *fmask,
+                                                                       const unsigned long long *epoch_word) {
     __shared__ uint32_t forbid[COLOR_WARPS_PER_CTA][32];
     __shared__ uint32_t pending[COLOR_WARPS_PER_CTA][PENDING];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t n = ld_relaxed_u32(&st->ordered);
+    const uint32_t epoch = fmask ? (uint32_t)*epoch_word : 0u;
     for (;;) {
         uint32_t t = 0;
         if (lane == 0) t = atomicAdd(&st->ticket, 1u);
@@ -331,7 +385,7 @@ __global__ void __launch_bounds__(COLOR_WARPS_PER_CTA * 32) k_jp_color(const uin
         if (t >= n) break;
         const uint32_t u = order[t];
         const int c = color_one_v(P + V[u], pc[u], color, forbid[warp], pending[warp], lane, st, spin_limit, tight,
-                                  nap);
+                                  nap, pc, fmask, epoch, u);
         if (lane == 0) {
             if (c < 0) raise_error(st, ERR_WAIT_EXPIRED, u);
             // -1 on error is non-zero, so successors stop waiting; the host reports the error
@@ -470,9 +524,14 @@ __global__ void k_keys_from_colors(const int *__restrict__ color, uint32_t N, ui
         key[u] = (uint32_t)color[u];
 }
 
-__global__ void k_reset_ticket(DevState *st) {
+// Also advances the epoch of the published forbidden colors (never 0: the buffer starts zeroed).
+__global__ void k_reset_ticket(DevState *st, unsigned long long *epoch_word) {
     st->ticket = 0;
     st->big_leaves = 0;
+    if (epoch_word) {
+        const unsigned long long e = (*epoch_word + 1) & 0xffffffffull;
+        *epoch_word = e ? e : 1;
+    }
 }
 
 int bit_length(uint64_t x) {
@@ -498,6 +557,16 @@ gc_status gc_jp_color(gc_graph *g) {
     if ((s = gc_alloc(ctx, &g->pc, g->cap_N, "predecessor counts")) != GC_OK) return s;
     if ((s = gc_alloc(ctx, &g->order, g->cap_N, "ticket order")) != GC_OK) return s;
     if ((s = gc_alloc(ctx, &g->leaf_list, g->cap_N, "leaf list")) != GC_OK) return s;
+    const bool decide = ctx->jp_decide;
+    if (decide && !g->fmask) {
+        const size_t words = (size_t)g->cap_N * GC_JP_MASK_WORDS + 1;
+        if ((s = gc_alloc(ctx, &g->fmask, words, "published forbidden colors")) != GC_OK) return s;
+        if ((s = gc_check_cuda(ctx, cudaMemsetAsync(g->fmask, 0, sizeof(unsigned long long) * words, ctx->stream),
+                               "published forbidden colors")) != GC_OK)
+            return s;
+    }
+    unsigned long long *fmask = decide ? g->fmask : nullptr;
+    unsigned long long *epoch_word = decide ? g->fmask + (size_t)g->cap_N * GC_JP_MASK_WORDS : nullptr;
     const int grid = ctx->num_sms * 8;
 
     // 1. split, and color the sources
@@ -539,12 +608,12 @@ gc_status gc_jp_color(gc_graph *g) {
     const int blocks = (want > 0 && want < occupancy) ? want : occupancy;
     const unsigned int tight = g->jp_ctas > 0 ? g->jp_tight : ctx->jp_tight;
     const unsigned int nap = g->jp_ctas > 0 ? g->jp_nap : ctx->jp_nap;
-    k_reset_ticket<<<1, 1, 0, ctx->stream>>>(ctx->dstate);
+    k_reset_ticket<<<1, 1, 0, ctx->stream>>>(ctx->dstate, epoch_word);
     ctx->launches++;
     {
         ProfScope ps(ctx, "jp_color", ctx->stream);
         k_jp_color<<<ctx->num_sms * blocks, COLOR_WARPS_PER_CTA * 32, 0, ctx->stream>>>(
-            g->V, g->P, g->pc, g->order, g->color, ctx->dstate, ctx->spin_limit, tight, nap);
+            g->V, g->P, g->pc, g->order, g->color, ctx->dstate, ctx->spin_limit, tight, nap, fmask, epoch_word);
         ctx->launches++;
     }
     // 4. leaves
