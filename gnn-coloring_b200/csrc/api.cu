@@ -192,6 +192,8 @@ gc_status gc_ctx_create(int device, gc_ctx **out) {
     if (const char *e = getenv("GC_JP_TIGHT")) ctx->jp_tight = (unsigned int)strtoul(e, nullptr, 10);
     if (const char *e = getenv("GC_JP_DECIDE")) ctx->jp_decide = atoi(e) != 0;
     if (const char *e = getenv("GC_JP_NAP")) ctx->jp_nap = (unsigned int)strtoul(e, nullptr, 10);
+    if (const char *e = getenv("GC_GNN_WARP_DEGREE")) ctx->gnn_warp_deg = (uint32_t)strtoul(e, nullptr, 10);
+    if (const char *e = getenv("GC_GNN_THIN_DEGREE")) ctx->gnn_thin_deg = (uint32_t)strtoul(e, nullptr, 10);
     if (const char *e = getenv("GC_GNN_SERIAL")) ctx->gnn_serial = atoi(e) != 0;  // 1: hubs first, then the bulk
     if (s != GC_OK) {
         gc_ctx_destroy(ctx);
@@ -298,6 +300,7 @@ gc_status gc_graph_upload(gc_ctx *ctx, uint32_t N, const uint32_t *V, const uint
     if (s != GC_OK) return s;
     gc_graph *g = new gc_graph();
     g->ctx = ctx;
+    g->gnn_warp_deg = ctx->gnn_warp_deg;
     ctx_retain(ctx);
     if ((s = gc_graph_alloc(ctx, g, N, V[N], true)) != GC_OK) {
         gc_graph_free(g);
@@ -317,6 +320,7 @@ gc_status gc_graph_create(gc_ctx *ctx, uint32_t cap_N, uint32_t cap_M, gc_graph 
     *out = nullptr;
     gc_graph *g = new gc_graph();
     g->ctx = ctx;
+    g->gnn_warp_deg = ctx->gnn_warp_deg;
     ctx_retain(ctx);
     gc_status s = gc_graph_alloc(ctx, g, cap_N, cap_M, true);
     if (s != GC_OK) {
@@ -352,6 +356,7 @@ gc_status gc_graph_wrap_device(gc_ctx *ctx, uint32_t N, uint32_t M, const uint32
     *out = nullptr;
     gc_graph *g = new gc_graph();
     g->ctx = ctx;
+    g->gnn_warp_deg = ctx->gnn_warp_deg;
     ctx_retain(ctx);
     g->owns_csr = false;
     g->V = const_cast<uint32_t *>(dV);

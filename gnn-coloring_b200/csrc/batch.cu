@@ -117,7 +117,7 @@ void drop_captures(gc_batch *b) {
 }
 
 bool tuning_valid(const gc_tuning &t) {
-    return t.hub_degree >= 1 && t.warp_degree <= t.hub_degree &&
+    return t.hub_degree >= 1 && t.warp_degree <= t.hub_degree && t.gnn_warp_degree >= 1 &&
            (t.schedule == GC_SCHEDULE_DEGREE || t.schedule == GC_SCHEDULE_SEGMENT) && t.jp_ctas_per_sm >= 1 &&
            t.jp_ctas_per_sm <= 32;
 }
@@ -191,6 +191,7 @@ gc_status finish_batch_upload(gc_batch *b, uint32_t G, const uint32_t *voff_host
         }
     }
     g->warp_deg = b->tuning.warp_degree;
+    g->gnn_warp_deg = b->tuning.gnn_warp_degree;
     g->hub_deg = b->tuning.hub_degree;
     g->sched = b->tuning.schedule;
     g->jp_ctas = b->tuning.jp_ctas_per_sm;
@@ -356,10 +357,12 @@ gc_status capture(gc_batch *b, gc_heuristic h, const gc_model *m, int recolor, B
 
 gc_status apply_tuning(gc_batch *b, const gc_tuning &t) {
     gc_graph *g = b->g;
-    const bool reprepare = t.warp_degree != g->warp_deg || t.hub_degree != g->hub_deg || t.schedule != g->sched;
+    const bool reprepare = t.warp_degree != g->warp_deg || t.hub_degree != g->hub_deg || t.schedule != g->sched ||
+                           t.gnn_warp_degree != g->gnn_warp_deg;
     b->tuning = t;
     drop_captures(b);
     g->warp_deg = t.warp_degree;
+    g->gnn_warp_deg = t.gnn_warp_degree;
     g->hub_deg = t.hub_degree;
     g->sched = t.schedule;
     g->jp_ctas = t.jp_ctas_per_sm;
@@ -382,6 +385,7 @@ void gc_tuning_default(gc_tuning *t) {
     t->jp_ctas_per_sm = 2;
     t->jp_tight = 32;
     t->jp_nap = 32;
+    t->gnn_warp_degree = GC_GNN_WIDE_DEGREE;
 }
 
 uint64_t gc_batch_device_bytes(uint32_t G, uint32_t N, uint32_t M, gc_heuristic h) {
@@ -716,6 +720,15 @@ gc_status gc_batch_autotune(gc_ctx *ctx, gc_batch *b, gc_heuristic h, const gc_m
                     t.warp_degree = wd;
                     if ((s = consider(t)) != GC_OK) return s;
                 }
+    }
+    if (effort >= 1 && (h == GC_GNN) && best.schedule == GC_SCHEDULE_DEGREE) {
+        // stage 1b: the GNN layers' own warp tier
+        const gc_tuning base = best;
+        for (uint32_t gw : {256u, 1024u, 4096u}) {
+            gc_tuning t = base;
+            t.gnn_warp_degree = gw;
+            if ((s = consider(t)) != GC_OK) return s;
+        }
     }
     if (effort >= 1) {
         // stage 2: resident CTAs of the ordered coloring kernel

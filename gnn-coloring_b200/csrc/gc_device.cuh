@@ -22,7 +22,9 @@ struct DevState {
     unsigned int min_deg;     // SL peeling: smallest remaining degree
     unsigned int ordered;     // coloring: vertices that go through the ordered kernel
     unsigned int big_leaves;  // coloring: leaves with too many neighbours for one thread
-    unsigned int pad[6];
+    unsigned int thin;        // preparation: vertices with at most the GNN thin-tier degree
+    unsigned int gnn_wide;    // preparation: vertices in the GNN warp tier
+    unsigned int pad[4];
 };
 
 enum DevErr : unsigned int {

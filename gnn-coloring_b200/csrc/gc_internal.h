@@ -17,6 +17,15 @@ struct gc_prof_rec {
     cudaEvent_t a, b;
 };
 
+// GNN layer tiers by neighbour count: a whole CTA above GC_GNN_HUB_DEGREE, one warp above
+// GC_GNN_WARP_DEGREE, four lanes otherwise.
+constexpr uint32_t GC_GNN_HUB_DEGREE = 16384;
+constexpr uint32_t GC_GNN_WARP_DEGREE = 256;
+// The GNN layers' own warp tier (degree schedule): a warp stages 32 rows through shared memory, which
+// costs about 2.5 L1 wavefronts per row against 1 for the four-lane tier, so only vertices whose lists
+// are long enough to need a warp's latency hiding get one (the split kernel keeps GC_GNN_WARP_DEGREE).
+constexpr uint32_t GC_GNN_WIDE_DEGREE = 4096;
+
 struct gc_ctx {
     int device = 0;
     int num_sms = 0;
@@ -29,6 +38,8 @@ struct gc_ctx {
     unsigned int jp_nap = 32;            // coloring: first sleep between polling rounds (ns)
     bool jp_decide = true;               // coloring: early decisions from published forbidden colors
     int gnn_blocks_per_sm[3] = {0, 0, 0};  // resident CTAs of each GNN layer kernel
+    uint32_t gnn_warp_deg = GC_GNN_WIDE_DEGREE;  // GNN: above this many neighbours a vertex gets a warp
+    uint32_t gnn_thin_deg = 16;          // GNN: vertices with at most this many neighbours get one lane each
     bool gnn_serial = false;             // hub CTAs beside the bulk on a high-priority stream (GC_GNN_SERIAL=1: before it)
     bool hub_smem_set[3] = {false, false, false};  // hub kernels' shared-memory limit raised
     cudaMemPool_t pool = nullptr;        // when set, graph buffers are stream-ordered allocations from this pool
@@ -54,10 +65,6 @@ struct ProfScope {
     ~ProfScope();
 };
 
-// GNN layer tiers by neighbour count: a whole CTA above GC_GNN_HUB_DEGREE, one warp above
-// GC_GNN_WARP_DEGREE, four lanes otherwise.
-constexpr uint32_t GC_GNN_HUB_DEGREE = 16384;
-constexpr uint32_t GC_GNN_WARP_DEGREE = 256;
 // Hubs (more than GC_GNN_HUB_DEGREE neighbours) are split across several warps in the JP split
 // pass, this many edges per warp task.
 constexpr uint32_t GC_SPLIT_CHUNK = 1024;  // edges per warp task (shared-memory buffer per warp)
@@ -111,6 +118,10 @@ struct gc_graph {
     uint32_t *vorder = nullptr;      // the other vertices by descending degree (GNN schedule)
     uint32_t n_vorder = 0;
     uint32_t n_wide = 0;             // leading vorder entries with more than GC_GNN_WARP_DEGREE neighbours
+    uint32_t n_wide_gnn = 0;         // leading vorder entries the GNN gives a warp (more than gnn_warp_deg)
+    uint32_t gnn_warp_deg = GC_GNN_WIDE_DEGREE;
+    uint32_t n_thin = 0;             // trailing vorder entries with at most ctx->gnn_thin_deg neighbours
+                                     // (degree schedule only; 0 with the graph-major schedule)
     // GNN scratch (allocated on first use)
     float *x = nullptr, *y = nullptr;
     float2 *t01 = nullptr;

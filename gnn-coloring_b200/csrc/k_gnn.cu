@@ -21,6 +21,8 @@
 //
 // Compiled without fast-math; every add, divide and FMA is an explicit round-to-nearest
 // intrinsic so the compiler cannot contract or reassociate them.
+#include <algorithm>
+
 #include "gc_internal.h"
 
 namespace {
@@ -270,6 +272,143 @@ __global__ void __launch_bounds__(GNN_THREADS, 4) k_gnn_layer(const uint32_t *__
             if (valid && q == 0) key[u] = __float_as_uint(sum);
         } else if (valid) {
             Y4[(size_t)u * 4 + q] = out;
+        }
+    }
+}
+
+// ---- thin tier: one vertex per lane --------------------------------------------------------------
+
+// Vertices with at most ctx->gnn_thin_deg neighbours (the tail of the degree order, vorder[first,
+// n_vorder)): one per lane, 32 per warp, whose degrees are nearly equal because the order is sorted.
+// Each lane adds its vertex's neighbour rows in CSR order (the next row's loads in flight while the
+// current one is added; the 16 feature chains interleave) and runs the 32 x 16 dense part alone:
+// no lane sits idle on a short neighbour list, and no shuffles are needed.
+constexpr int THIN_THREADS = 256;
+
+template <int MODE>
+__global__ void __launch_bounds__(THIN_THREADS, 3) k_gnn_thin(const uint32_t *__restrict__ V, const uint32_t *__restrict__ E,
+                                                              const uint32_t *__restrict__ vorder, uint32_t first,
+                                                              uint32_t n_vorder, const float2 *__restrict__ t01,
+                                                              const float *__restrict__ x, float *__restrict__ y,
+                                                              uint32_t *__restrict__ key, const float *__restrict__ Wb) {
+    __shared__ __align__(16) float sW[LAYER_PARAMS];
+    for (int i = threadIdx.x; i < LAYER_PARAMS; i += blockDim.x) sW[i] = Wb[i];
+    __syncthreads();
+    const float4 *W4 = reinterpret_cast<const float4 *>(sW);
+    const float4 *X4 = reinterpret_cast<const float4 *>(x);
+    const int lane = threadIdx.x & 31;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t base = first + blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < n_vorder; base += stride) {
+        const uint32_t slot = base + lane;
+        const bool valid = slot < n_vorder;
+        const uint32_t u = valid ? vorder[slot] : 0u;
+        const uint32_t beg = valid ? V[u] : 0u, d = valid ? V[u + 1] - beg : 0u;
+        const uint32_t dmax = __reduce_max_sync(FULL, d);
+        const float fd = __uint2float_rn(d);
+        float c[FEAT];
+#pragma unroll
+        for (int j = 0; j < FEAT; j++) c[j] = sW[2 * FEAT * FEAT + j];
+        if (MODE == MODE_INPUT) {
+            float s0 = 0.0f, s1 = 0.0f;
+            float2 tn = d ? t01[__ldg(E + beg)] : make_float2(0.0f, 0.0f);
+            for (uint32_t k = 0; k < dmax; k++) {
+                const float2 t = tn;
+                if (k + 1 < d) tn = t01[__ldg(E + beg + k + 1)];
+                if (k < d) {
+                    s0 = __fadd_rn(s0, t.x);
+                    s1 = __fadd_rn(s1, t.y);
+                }
+            }
+            if (fd > 0.0f) {
+                s0 = __fdiv_rn(s0, fd);
+                s1 = __fdiv_rn(s1, fd);
+            }
+            const float2 self = valid ? t01[u] : make_float2(0.0f, 0.0f);
+#pragma unroll
+            for (int i = 0; i < 32; i++) {
+                const float a = i < 8 ? s0 : (i < 16 ? s1 : (i < 24 ? self.x : self.y));
+#pragma unroll
+                for (int jq = 0; jq < 4; jq++) {
+                    const float4 w = W4[i * 4 + jq];
+                    c[4 * jq + 0] = __fmaf_rn(w.x, a, c[4 * jq + 0]);
+                    c[4 * jq + 1] = __fmaf_rn(w.y, a, c[4 * jq + 1]);
+                    c[4 * jq + 2] = __fmaf_rn(w.z, a, c[4 * jq + 2]);
+                    c[4 * jq + 3] = __fmaf_rn(w.w, a, c[4 * jq + 3]);
+                }
+            }
+        } else {
+            float acc[FEAT];
+#pragma unroll
+            for (int f = 0; f < FEAT; f++) acc[f] = 0.0f;
+            // ids two ahead, rows one ahead
+            uint32_t vnext = d > 1 ? __ldg(E + beg + 1) : 0u;
+            float4 rn[4];
+            {
+                const uint32_t v0 = d ? __ldg(E + beg) : 0u;
+#pragma unroll
+                for (int p = 0; p < 4; p++) rn[p] = d ? X4[(size_t)v0 * 4 + p] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            }
+            for (uint32_t k = 0; k < dmax; k++) {
+                float4 r[4];
+#pragma unroll
+                for (int p = 0; p < 4; p++) r[p] = rn[p];
+                if (k + 1 < d) {
+                    const uint32_t v = vnext;
+                    vnext = k + 2 < d ? __ldg(E + beg + k + 2) : 0u;
+#pragma unroll
+                    for (int p = 0; p < 4; p++) rn[p] = X4[(size_t)v * 4 + p];
+                }
+                if (k < d) {
+#pragma unroll
+                    for (int p = 0; p < 4; p++) {
+                        acc[4 * p + 0] = __fadd_rn(acc[4 * p + 0], r[p].x);
+                        acc[4 * p + 1] = __fadd_rn(acc[4 * p + 1], r[p].y);
+                        acc[4 * p + 2] = __fadd_rn(acc[4 * p + 2], r[p].z);
+                        acc[4 * p + 3] = __fadd_rn(acc[4 * p + 3], r[p].w);
+                    }
+                }
+            }
+            if (fd > 0.0f) {
+#pragma unroll
+                for (int f = 0; f < FEAT; f++) acc[f] = __fdiv_rn(acc[f], fd);
+            }
+            float self[FEAT];
+#pragma unroll
+            for (int p = 0; p < 4; p++) {
+                const float4 s4 = valid ? X4[(size_t)u * 4 + p] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                self[4 * p + 0] = s4.x;
+                self[4 * p + 1] = s4.y;
+                self[4 * p + 2] = s4.z;
+                self[4 * p + 3] = s4.w;
+            }
+#pragma unroll
+            for (int i = 0; i < 32; i++) {
+                const float a = i < FEAT ? acc[i] : self[i - FEAT];
+#pragma unroll
+                for (int jq = 0; jq < 4; jq++) {
+                    const float4 w = W4[i * 4 + jq];
+                    c[4 * jq + 0] = __fmaf_rn(w.x, a, c[4 * jq + 0]);
+                    c[4 * jq + 1] = __fmaf_rn(w.y, a, c[4 * jq + 1]);
+                    c[4 * jq + 2] = __fmaf_rn(w.z, a, c[4 * jq + 2]);
+                    c[4 * jq + 3] = __fmaf_rn(w.w, a, c[4 * jq + 3]);
+                }
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < FEAT; j++) c[j] = relu(c[j]);
+        if (!valid) continue;
+        if (MODE == MODE_OUTPUT) {
+            // t_k = o_k + o_{k+8}, then ((t0+t1)+(t2+t3)) + ((t4+t5)+(t6+t7))  (dense_kernel_output)
+            float t[8];
+#pragma unroll
+            for (int k = 0; k < 8; k++) t[k] = __fadd_rn(c[k], c[k + 8]);
+            const float sum = __fadd_rn(__fadd_rn(__fadd_rn(t[0], t[1]), __fadd_rn(t[2], t[3])),
+                                        __fadd_rn(__fadd_rn(t[4], t[5]), __fadd_rn(t[6], t[7])));
+            key[u] = __float_as_uint(sum);
+        } else {
+            float4 *Y4 = reinterpret_cast<float4 *>(y) + (size_t)u * 4;
+#pragma unroll
+            for (int p = 0; p < 4; p++) Y4[p] = make_float4(c[4 * p], c[4 * p + 1], c[4 * p + 2], c[4 * p + 3]);
         }
     }
 }
@@ -595,10 +734,19 @@ gc_status launch_layer(gc_graph *g, const float *Wb, const float *x, float *y, c
     if (g->n_vorder) {
         ProfScope ps(ctx, MODE == MODE_INPUT ? "gnn_input" : (MODE == MODE_HIDDEN ? "gnn_hidden" : "gnn_output"),
                      ctx->stream);
-        k_gnn_layer<MODE><<<ctx->num_sms * blocks, GNN_THREADS, 0, ctx->stream>>>(
-            g->V, g->E, g->vorder, g->n_wide, g->n_vorder, g->t01, x, y, g->key, Wb);
+        const uint32_t first_thin = g->n_vorder - g->n_thin;
+        if (first_thin) {
+            k_gnn_layer<MODE><<<ctx->num_sms * blocks, GNN_THREADS, 0, ctx->stream>>>(
+                g->V, g->E, g->vorder, g->n_wide_gnn, first_thin, g->t01, x, y, g->key, Wb);
+            ctx->launches++;
+        }
+        if (g->n_thin) {
+            const uint32_t grid = std::min<uint32_t>((uint32_t)ctx->num_sms * 3, (g->n_thin + THIN_THREADS - 1) / THIN_THREADS);
+            k_gnn_thin<MODE><<<grid, THIN_THREADS, 0, ctx->stream>>>(g->V, g->E, g->vorder, first_thin, g->n_vorder,
+                                                                     g->t01, x, y, g->key, Wb);
+            ctx->launches++;
+        }
     }
-    ctx->launches++;
     if ((s = gc_check_launch(ctx, "gnn layer")) != GC_OK) return s;
     if (g->n_hubs) {
         if ((s = gc_check_cuda(ctx, cudaEventRecord(join, side), "join")) != GC_OK) return s;

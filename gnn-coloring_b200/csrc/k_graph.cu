@@ -9,7 +9,8 @@
 namespace {
 
 __global__ void k_degree_classes(const uint32_t *__restrict__ V, uint32_t N, uint32_t big_deg,
-                                 uint32_t chunk, uint32_t hub_deg, uint32_t warp_deg, gc::DevState *st,
+                                 uint32_t chunk, uint32_t hub_deg, uint32_t warp_deg, uint32_t gnn_warp_deg,
+                                 uint32_t thin_deg, gc::DevState *st,
                                  uint32_t *__restrict__ tasks, uint32_t task_cap,
                                  uint32_t *__restrict__ hubs, uint32_t hub_cap) {
     const uint32_t stride = gridDim.x * blockDim.x;
@@ -39,6 +40,8 @@ __global__ void k_degree_classes(const uint32_t *__restrict__ V, uint32_t N, uin
         } else if (d > warp_deg) {
             atomicAdd(&st->min_deg, 1u);  // counts the GNN warp tier
         }
+        if (d > gnn_warp_deg && d <= hub_deg) atomicAdd(&st->gnn_wide, 1u);  // counts the GNN warp tier
+        if (d <= thin_deg && d <= gnn_warp_deg) atomicAdd(&st->thin, 1u);     // counts the GNN thin tier
     }
 }
 
@@ -89,19 +92,28 @@ gc_status gc_graph_prepare(gc_graph *g) {
         g->n_big_tasks = 0;
         g->n_hubs = 0;
         g->n_vorder = 0;
+        g->n_thin = 0;
+        g->n_wide_gnn = 0;
+        g->n_giant = g->n_giant_tasks = 0;
+        g->giant_rows = 0;
         return GC_OK;
     }
     int grid = ctx->num_sms * 8;
+    // the GNN keeps its own warp tier only with the degree schedule (the graph-major order puts the
+    // split's warp tier first, so there the two tiers coincide)
+    const uint32_t gnn_wd = g->sched == GC_SCHEDULE_DEGREE ? std::max(g->gnn_warp_deg, g->warp_deg) : g->warp_deg;
     // pass 1: counts
     if ((s = gc_reset_state(ctx)) != GC_OK) return s;
     k_degree_classes<<<grid, 256, 0, ctx->stream>>>(g->V, g->N, g->hub_deg, GC_SPLIT_CHUNK, g->hub_deg,
-                                                    g->warp_deg, ctx->dstate, nullptr, 0, nullptr, 0);
+                                                    g->warp_deg, gnn_wd, ctx->gnn_thin_deg, ctx->dstate, nullptr, 0, nullptr, 0);
     ctx->launches++;
     if ((s = gc_check_launch(ctx, "degree classes")) != GC_OK) return s;
     if ((s = gc_read_state(ctx)) != GC_OK) return s;
     g->max_deg = ctx->hstate->max_color;
     uint32_t n_tasks = ctx->hstate->count, n_hubs = ctx->hstate->count2;
     g->n_wide = ctx->hstate->min_deg;
+    g->n_thin = g->sched == GC_SCHEDULE_DEGREE ? ctx->hstate->thin : 0u;
+    g->n_wide_gnn = g->sched == GC_SCHEDULE_DEGREE ? ctx->hstate->gnn_wide : g->n_wide;
     // lists: the hub list and the degree order fit in cap_N; the task list grows when needed
     if (2 * (size_t)n_tasks > g->big_cap) {
         gc_dev_free(ctx, g->big);
@@ -113,7 +125,8 @@ gc_status gc_graph_prepare(gc_graph *g) {
     // pass 2: fill
     if ((s = gc_reset_state(ctx)) != GC_OK) return s;
     k_degree_classes<<<grid, 256, 0, ctx->stream>>>(g->V, g->N, g->hub_deg, GC_SPLIT_CHUNK, g->hub_deg,
-                                                    g->warp_deg, ctx->dstate, g->big, n_tasks, g->hubs, n_hubs);
+                                                    g->warp_deg, gnn_wd, ctx->gnn_thin_deg, ctx->dstate, g->big, n_tasks,
+                                                    g->hubs, n_hubs);
     ctx->launches++;
     if ((s = gc_check_launch(ctx, "degree classes")) != GC_OK) return s;
     if ((s = gc_read_state(ctx)) != GC_OK) return s;

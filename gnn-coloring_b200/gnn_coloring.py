@@ -106,7 +106,8 @@ _sig("gc_gen_mixed_batch", C.c_int, C.c_uint32, C.c_uint64, C.c_uint32, C.c_uint
 class Tuning(C.Structure):
     """gc_tuning: what the batch autotuner may change (never a color or priority bit)."""
     _fields_ = [("warp_degree", C.c_uint32), ("hub_degree", C.c_uint32), ("schedule", C.c_int),
-                ("jp_ctas_per_sm", C.c_int), ("jp_tight", C.c_uint), ("jp_nap", C.c_uint)]
+                ("jp_ctas_per_sm", C.c_int), ("jp_tight", C.c_uint), ("jp_nap", C.c_uint),
+                ("gnn_warp_degree", C.c_uint32)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -187,6 +187,7 @@ typedef struct gc_tuning {
     int jp_ctas_per_sm;     /* resident CTAs per SM of the ordered coloring kernel */
     unsigned int jp_tight;  /* polling rounds before a coloring warp starts to sleep */
     unsigned int jp_nap;    /* first sleep of a coloring warp (ns) */
+    uint32_t gnn_warp_degree;  /* GNN layers, degree schedule: above this many neighbours a vertex gets a warp */
 } gc_tuning;
 
 /* Uploads G graphs given as one segmented CSR (layout above). */

@@ -188,10 +188,12 @@ def test_tunings_do_not_change_results(gpu_ctx, models):
     base = _check_batch_against_plain(gpu_ctx, graphs, "GNN", models[3])
     variants = []
     for sched in (gcn.GC_SCHEDULE_DEGREE, gcn.GC_SCHEDULE_SEGMENT):
-        for warp, hub, ctas, tight, nap in ((0, 16, 1, 4, 8), (16, 64, 4, 128, 32), (1024, 4096, 3, 32, 128)):
+        for warp, hub, ctas, tight, nap, gwarp in ((0, 16, 1, 4, 8, 8), (16, 64, 4, 128, 32, 64),
+                                                  (1024, 4096, 3, 32, 128, 4096)):
             t = gcn.default_tuning()
             t.schedule, t.warp_degree, t.hub_degree = sched, warp, hub
             t.jp_ctas_per_sm, t.jp_tight, t.jp_nap = ctas, tight, nap
+            t.gnn_warp_degree = gwarp
             variants.append(t)
     for t in variants:
         counts = _check_batch_against_plain(gpu_ctx, graphs, "GNN", models[3], tuning=t)
