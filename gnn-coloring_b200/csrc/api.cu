@@ -107,7 +107,7 @@ void gc_graph_free_buffers(gc_graph *g) {
     void *bufs[] = {g->key,       g->color,  g->P,        g->pc,       g->order,    g->sort_buf, g->sort_hist,
                     g->big,       g->hubs,   g->x,        g->y,        g->t01,      g->deg_rem,  g->frontier,
                     g->frontier2, g->removed, g->leaf_list, g->vorder, g->rank,     g->p64,      g->seg_voff,
-                    g->seg_stat,  g->fmask,    g->giant,    g->hub_stage};
+                    g->seg_stat,  g->fmask,    g->giant,    g->hub_stage, g->jprec};
     for (void *p : bufs) gc_dev_free(ctx, p);
 }
 

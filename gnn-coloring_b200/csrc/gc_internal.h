@@ -94,6 +94,7 @@ struct gc_graph {
     uint32_t *order = nullptr;  // vertices by descending key, ascending id on ties: the ticket order
     uint32_t *leaf_list = nullptr;  // leaves too large for one thread
     uint32_t *rank = nullptr;       // ticket of each ordered vertex (all ones elsewhere)
+    uint4 *jprec = nullptr;         // per ticket: (vertex, first CSR entry, predecessor count, 0)
     // forbidden colors 1..256 published by waiting vertices of the ordered coloring kernel:
     // GC_JP_MASK_WORDS words per vertex, each (epoch << 32 | 32 color bits); the word after the
     // last vertex's holds the epoch counter, advanced once per coloring run

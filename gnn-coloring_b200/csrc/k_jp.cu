@@ -365,10 +365,23 @@ __device__ int color_one_v(const uint32_t *__restrict__ list, uint32_t cnt, cons
 // The ordered vertices (neither sources nor leaves), one warp each, tickets taken one at a time
 // in order.  A warp waits only on vertices with smaller tickets, which are held by running warps
 // or done, so the oldest unfinished ticket always progresses.
-__global__ void __launch_bounds__(COLOR_WARPS_PER_CTA * 32) k_jp_color(const uint32_t *__restrict__ V,
+// Ticket records: rec[t] = (vertex, first CSR entry, predecessor count) of ticket t, so that a
+// warp needs one 16-byte load per ticket instead of the order -> V, pc chain.
+__global__ void k_jp_records(const uint32_t *__restrict__ order, const uint32_t *__restrict__ V,
+                             const uint32_t *__restrict__ pc, const DevState *st, uint4 *__restrict__ rec) {
+    const uint32_t n = st->ordered;
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+        const uint32_t u = order[t];
+        rec[t] = make_uint4(u, V[u], pc[u], 0u);
+    }
+}
+
+// A warp takes its next ticket only when it is free: a ticket held ahead by a warp still waiting on
+// its current vertex would stall every vertex that waits on the held one (measured several times
+// slower on R-MAT 22).
+__global__ void __launch_bounds__(COLOR_WARPS_PER_CTA * 32, 2) k_jp_color(const uint4 *__restrict__ rec,
                                                                        const uint32_t *__restrict__ P,
-                                                                       const uint32_t *__restrict__ pc,
-                                                                       const uint32_t *__restrict__ order, int *color,
+                                                                       const uint32_t *__restrict__ pc, int *color,
                                                                        DevState *st, unsigned int spin_limit,
                                                                        unsigned int tight, unsigned int nap,
                                                                        unsigned long long *fmask,
@@ -383,9 +396,10 @@ __global__ void __launch_bounds__(COLOR_WARPS_PER_CTA * 32) k_jp_color(const uin
         if (lane == 0) t = atomicAdd(&st->ticket, 1u);
         t = __shfl_sync(0xffffffffu, t, 0);
         if (t >= n) break;
-        const uint32_t u = order[t];
-        const int c = color_one_v(P + V[u], pc[u], color, forbid[warp], pending[warp], lane, st, spin_limit, tight,
-                                  nap, pc, fmask, epoch, u);
+        const uint4 r = rec[t];
+        const uint32_t u = r.x;
+        const int c = color_one_v(P + r.y, r.z, color, forbid[warp], pending[warp], lane, st, spin_limit, tight, nap,
+                                  pc, fmask, epoch, u);
         if (lane == 0) {
             if (c < 0) raise_error(st, ERR_WAIT_EXPIRED, u);
             // -1 on error is non-zero, so successors stop waiting; the host reports the error
@@ -595,6 +609,10 @@ gc_status gc_jp_color(gc_graph *g) {
     else if (g->key_kind == 100) bits = bit_length((uint64_t)g->max_deg + 1);
     if ((s = gc_sort_order_bits(g, bits, true, &ctx->dstate->ordered)) != GC_OK) return s;
 
+    if ((s = gc_alloc(ctx, &g->jprec, g->cap_N, "ticket records")) != GC_OK) return s;
+    k_jp_records<<<ctx->num_sms * 4, 256, 0, ctx->stream>>>(g->order, g->V, g->pc, ctx->dstate, g->jprec);
+    ctx->launches++;
+
     // 3. ordered coloring
     int &occupancy = ctx->color_blocks_per_sm;
     if (!occupancy) {
@@ -613,7 +631,7 @@ gc_status gc_jp_color(gc_graph *g) {
     {
         ProfScope ps(ctx, "jp_color", ctx->stream);
         k_jp_color<<<ctx->num_sms * blocks, COLOR_WARPS_PER_CTA * 32, 0, ctx->stream>>>(
-            g->V, g->P, g->pc, g->order, g->color, ctx->dstate, ctx->spin_limit, tight, nap, fmask, epoch_word);
+            g->jprec, g->P, g->pc, g->color, ctx->dstate, ctx->spin_limit, tight, nap, fmask, epoch_word);
         ctx->launches++;
     }
     // 4. leaves
