@@ -371,6 +371,8 @@ def run_ours(args):
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         result["cpu_baseline"] = cpu_baseline(N, V, E, params, md)
+    if world == 1 and not args.no_configs:
+        result["configs"] = run_configs(args, device)
     if world == 1 and not args.no_batch:
         result["batched"] = run_batched(args, device)
     if world == 1 and not args.no_serve:
@@ -383,6 +385,64 @@ def run_ours(args):
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+# ---- the other configurations: ER 65k with every heuristic, mesh-like graphs with Culberson ------
+
+def _timed_jobs(ctx, g, heur, model, recolor, reps, torch, device):
+    """Device time per job (priority + JP + recolor Culberson rounds) with CUDA events on the
+    library's stream, after one warm-up job; returns (ms, colors)."""
+    stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", device))
+    g.priority(heur, model)
+    colors = g.color(recolor)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(reps):
+        g.priority(heur, model)
+        g.color(recolor, count=False)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps, colors
+
+
+def run_configs(args, device):
+    import math
+    import torch
+    import gnn_coloring as gcn
+    ctx = gcn.Context(device)
+    models = {L: gcn.Model(ctx, *gcn.synthetic_model(L, 1000 + L)) for L in (2, 3, 4)}
+    out = {}
+    # Erdos-Renyi n = 65,536, m = 524,288, seed 1: every heuristic, one coloring
+    N, V, E = gcn.gen_er(65536, 524288, 1)
+    g = gcn.Graph(ctx, N, V, E)
+    rows = {}
+    for name in ("FF", "LF", "LLF", "SL", "SLL", "GNN2", "GNN3", "GNN4"):
+        heur, m = ("GNN", models[int(name[3])]) if name.startswith("GNN") else (name, None)
+        ms, colors = _timed_jobs(ctx, g, heur, m, 0, 10, torch, device)
+        rows[name] = {"ms": ms, "colors": colors, "edges_per_s": len(E) / (ms / 1e3)}
+    g.close()
+    out["er65k_all_heuristics"] = {"graph": "Erdos-Renyi n=65536, m=524288, seed 1", "N": N, "M": len(E),
+                                   "heuristics": rows}
+    # mesh-like graphs, GNN4 priorities + JP + 9 Culberson rounds (the reference's -c 10)
+    n = 1 << 23
+    for key, desc, gen in (
+            ("rgg2d_8m_gnn4_c10", "2D random geometric graph, n=2^23, radius for mean degree 12, seed 1",
+             lambda: gcn.gen_rgg2d(n, math.sqrt(12.0 / (math.pi * n)), 1)),
+            ("stencil27_256_gnn4_c10", "3D 27-point stencil, 256^3 vertices", lambda: gcn.gen_stencil27(256, 256, 256))):
+        N, V, E = gen()
+        g = gcn.Graph(ctx, N, V, E)
+        ms, colors = _timed_jobs(ctx, g, "GNN", models[4], 9, 3, torch, device)
+        g.priority("GNN", models[4])
+        first = g.color(0)
+        g.close()
+        out[key] = {"graph": desc, "N": N, "M": len(E), "ms_per_job": ms, "edges_per_s": len(E) / (ms / 1e3),
+                    "colors_first": first, "colors_after_9_culberson": colors}
+        del V, E
+    for m in models.values():
+        m.close()
+    ctx.close()
+    return out
 
 
 # ---- batched vs plain: many independent graphs in one launch ------------------------------------
@@ -646,6 +706,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-vs-plain leg")
+    ap.add_argument("--no-configs", action="store_true", help="skip the ER-65k and mesh-graph measurements")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving sweep")
     ap.add_argument("--batch-graphs", type=int, default=4096)
     ap.add_argument("--serve-jobs", type=int, default=300)

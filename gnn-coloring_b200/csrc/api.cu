@@ -107,7 +107,7 @@ void gc_graph_free_buffers(gc_graph *g) {
     void *bufs[] = {g->key,       g->color,  g->P,        g->pc,       g->order,    g->sort_buf, g->sort_hist,
                     g->big,       g->hubs,   g->x,        g->y,        g->t01,      g->deg_rem,  g->frontier,
                     g->frontier2, g->removed, g->leaf_list, g->vorder, g->rank,     g->p64,      g->seg_voff,
-                    g->seg_stat,  g->fmask,    g->giant,    g->hub_stage, g->jprec};
+                    g->seg_stat,  g->fmask,    g->giant,    g->hub_stage, g->jprec, g->class_first};
     for (void *p : bufs) gc_dev_free(ctx, p);
 }
 
@@ -190,6 +190,7 @@ gc_status gc_ctx_create(int device, gc_ctx **out) {
     // tuning of the coloring kernel's polling (defaults measured on B200)
     if (const char *e = getenv("GC_JP_CTAS_PER_SM")) ctx->jp_ctas_per_sm = atoi(e);
     if (const char *e = getenv("GC_JP_TIGHT")) ctx->jp_tight = (unsigned int)strtoul(e, nullptr, 10);
+    if (const char *e = getenv("GC_JP_CLASSES")) ctx->jp_classes = atoi(e) != 0;
     if (const char *e = getenv("GC_JP_DECIDE")) ctx->jp_decide = atoi(e) != 0;
     if (const char *e = getenv("GC_JP_NAP")) ctx->jp_nap = (unsigned int)strtoul(e, nullptr, 10);
     if (const char *e = getenv("GC_GNN_WARP_DEGREE")) ctx->gnn_warp_deg = (uint32_t)strtoul(e, nullptr, 10);
@@ -577,6 +578,7 @@ gc_status gc_upload_colors(gc_ctx *ctx, gc_graph *g, const int32_t *color) {
         return s;
     if ((s = gc_check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "upload colors")) != GC_OK) return s;
     g->has_colors = true;
+    g->colors_ours = false;
     return GC_OK;
 }
 

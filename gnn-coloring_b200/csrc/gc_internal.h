@@ -37,6 +37,7 @@ struct gc_ctx {
     unsigned int jp_tight = 32;          // coloring: unproductive polling rounds before sleeping
     unsigned int jp_nap = 32;            // coloring: first sleep between polling rounds (ns)
     bool jp_decide = true;               // coloring: early decisions from published forbidden colors
+    bool jp_classes = true;              // Culberson rounds: class by class instead of tickets
     int gnn_blocks_per_sm[3] = {0, 0, 0};  // resident CTAs of each GNN layer kernel
     uint32_t gnn_warp_deg = GC_GNN_WIDE_DEGREE;  // GNN: above this many neighbours a vertex gets a warp
     uint32_t gnn_thin_deg = 16;          // GNN: vertices with at most this many neighbours get one lane each
@@ -86,8 +87,10 @@ struct gc_graph {
     // priorities and colors
     uint32_t *key = nullptr;   // uint32 priority keys (float bits for GNN)
     int32_t *color = nullptr;  // 1-based colors
-    int key_kind = -1;         // gc_heuristic that produced the keys, 100 = colors (Culberson), 200 = user
+    int key_kind = -1;         // gc_heuristic that produced the keys, 100 = our colors (Culberson),
+                               // 101 = caller colors as keys, 200 = user priorities
     bool has_keys = false, has_colors = false;
+    bool colors_ours = false;  // the current colors come from this library's JP (at most max degree + 1)
     // JP workspace
     uint32_t *P = nullptr;      // predecessor lists, packed at the front of each CSR segment
     uint32_t *pc = nullptr;     // predecessor counts
@@ -95,6 +98,8 @@ struct gc_graph {
     uint32_t *leaf_list = nullptr;  // leaves too large for one thread
     uint32_t *rank = nullptr;       // ticket of each ordered vertex (all ones elsewhere)
     uint4 *jprec = nullptr;         // per ticket: (vertex, first CSR entry, predecessor count, 0)
+    uint32_t *class_first = nullptr;  // Culberson rounds: first ticket position of each key (old color)
+    size_t class_cap = 0;
     // forbidden colors 1..256 published by waiting vertices of the ordered coloring kernel:
     // GC_JP_MASK_WORDS words per vertex, each (epoch << 32 | 32 color bits); the word after the
     // last vertex's holds the epoch counter, advanced once per coloring run

@@ -26,6 +26,8 @@
 //
 // Colors are published with relaxed GPU-scope stores and read with relaxed GPU-scope loads: the
 // color value is itself the whole message, so no fences are needed.
+#include <algorithm>
+#include <vector>
 #include <cstdlib>
 
 #include "gc_internal.h"
@@ -409,6 +411,61 @@ __global__ void __launch_bounds__(COLOR_WARPS_PER_CTA * 32, 2) k_jp_color(const 
     }
 }
 
+// Culberson rounds (keys = the previous colors): the ticket order sorts the inner vertices by key, so
+// each color class is a contiguous run of it.  first[k] = the first position of key k (runs of absent
+// keys keep the fill value).
+__global__ void k_jp_class_bounds(const uint32_t *__restrict__ order, const uint32_t *__restrict__ key,
+                                  DevState *st, uint32_t *__restrict__ first, uint32_t words) {
+    const uint32_t n = st->ordered;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t k = key[order[i]];
+        if (k >= words) raise_error(st, ERR_BOUND, order[i]);
+        else if (i == 0 || key[order[i - 1]] != k) first[k] = i;
+    }
+}
+
+// One class of a Culberson round: the inner vertices order[a, b), whose key (old color) is the same.
+// A class is an independent set and its predecessors (larger old colors) are sources or vertices of
+// classes colored before it, so nothing waits: one thread per vertex with at most 62 predecessors
+// (the mex, at most 63, is a bit of a 64-bit mask); the warp colors the larger ones together.
+__global__ void __launch_bounds__(COLOR_THREADS) k_jp_class(const uint32_t *__restrict__ order, uint32_t a, uint32_t b,
+                                                           const uint32_t *__restrict__ V, const uint32_t *__restrict__ P,
+                                                           const uint32_t *__restrict__ pc, int *color, DevState *st,
+                                                           unsigned int spin_limit) {
+    __shared__ uint32_t forbid[COLOR_WARPS][32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t base = a + blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < b; base += stride) {
+        const uint32_t i = base + lane;
+        const bool valid = i < b;
+        const uint32_t u = valid ? order[i] : 0u;
+        const uint32_t cnt = valid ? pc[u] : 0u;
+        const bool big = valid && cnt > 62;
+        if (valid && !big) {
+            const uint32_t *list = P + V[u];
+            unsigned long long used = 1;  // bit 0 stands for "color 0", never free
+            for (uint32_t j = 0; j < cnt; j++) {
+                const int c = color[list[j]];
+                if (c > 0 && c < 64) used |= 1ull << c;
+            }
+            color[u] = __ffsll((long long)~used) - 1;
+        }
+        unsigned int bigs = __ballot_sync(0xffffffffu, big);
+        while (bigs) {
+            const int l = __ffs(bigs) - 1;
+            bigs &= bigs - 1;
+            const uint32_t ub = __shfl_sync(0xffffffffu, u, l), cb = __shfl_sync(0xffffffffu, cnt, l);
+            // every predecessor is colored: the bounded wait inside never runs
+            const int c = color_one(P + V[ub], cb, color, forbid[warp], lane, st, spin_limit);
+            if (lane == 0) {
+                if (c < 0) raise_error(st, ERR_WAIT_EXPIRED, ub);
+                color[ub] = c;
+            }
+            __syncwarp();
+        }
+    }
+}
+
 // Leaves (every neighbour is a predecessor) are colored after all other vertices, in parallel:
 // nothing waits on them.  One thread per leaf with a 64-bit mask for degrees up to 62 (so the mex,
 // at most degree + 1, is a bit of the mask); larger leaves are listed for the warp kernel.
@@ -432,16 +489,20 @@ __global__ void k_jp_leaves(const uint32_t *__restrict__ V, const uint32_t *__re
 
 __global__ void __launch_bounds__(COLOR_THREADS, 6) k_jp_big_leaves(const uint32_t *__restrict__ V, const uint32_t *__restrict__ E,
                                                                  const uint32_t *__restrict__ big, int *color,
-                                                                 DevState *st) {
+                                                                 DevState *st, unsigned int spin_limit) {
     __shared__ uint32_t forbid[COLOR_WARPS][32];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t n = st->big_leaves;
     const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
     for (uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += nwarps) {
         const uint32_t u = big[i];
-        // every neighbour is colored already: color_one never waits here
-        const int c = color_one(E + V[u], V[u + 1] - V[u], color, forbid[warp], lane, st, 0xffffffffu);
-        if (lane == 0) color[u] = c;
+        // every neighbour is colored already, so color_one does not wait here; its waits stay bounded
+        // all the same, and an expiry is reported rather than stored as a color
+        const int c = color_one(E + V[u], V[u + 1] - V[u], color, forbid[warp], lane, st, spin_limit);
+        if (lane == 0) {
+            if (c < 0) raise_error(st, ERR_WAIT_EXPIRED, u);
+            color[u] = c;
+        }
         __syncwarp();
     }
 }
@@ -609,6 +670,65 @@ gc_status gc_jp_color(gc_graph *g) {
     else if (g->key_kind == 100) bits = bit_length((uint64_t)g->max_deg + 1);
     if ((s = gc_sort_order_bits(g, bits, true, &ctx->dstate->ordered)) != GC_OK) return s;
 
+    // 3a. Culberson rounds: class by class, outside stream capture (it reads the class bounds back)
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing(ctx->stream, &cap);
+    if (g->key_kind == 100 && ctx->jp_classes && cap == cudaStreamCaptureStatusNone) {
+        const size_t words = (size_t)g->max_deg + 2;  // keys (old colors) are at most max_deg + 1
+        if (words > g->class_cap) {
+            gc_dev_free(ctx, g->class_first);
+            g->class_first = nullptr;
+            if ((s = gc_alloc(ctx, &g->class_first, words, "class bounds")) != GC_OK) return s;
+            g->class_cap = words;
+        }
+        if ((s = gc_check_cuda(ctx, cudaMemsetAsync(g->class_first, 0xff, 4 * words, ctx->stream), "class bounds")) !=
+            GC_OK)
+            return s;
+        k_jp_class_bounds<<<ctx->num_sms * 4, 256, 0, ctx->stream>>>(g->order, g->key, ctx->dstate, g->class_first,
+                                                                     (uint32_t)words);
+        ctx->launches++;
+        std::vector<uint32_t> first(words);
+        if ((s = gc_check_cuda(ctx, cudaMemcpyAsync(first.data(), g->class_first, 4 * words, cudaMemcpyDeviceToHost,
+                                                    ctx->stream), "class bounds")) != GC_OK)
+            return s;
+        if ((s = gc_read_state(ctx)) != GC_OK) return s;  // syncs; also brings the ordered count
+        const uint32_t n_ordered = ctx->hstate->ordered;
+        {
+            ProfScope ps(ctx, "jp_classes", ctx->stream);
+            uint32_t end = n_ordered;
+            // positions grow as keys fall: walk the keys upwards, each class ending where the next
+            // larger key's class begins, and launch in descending key order
+            std::vector<std::pair<uint32_t, uint32_t>> runs;
+            for (size_t k = 0; k < words; k++)
+                if (first[k] != 0xffffffffu) {
+                    runs.push_back({first[k], end});
+                    end = first[k];
+                }
+            for (auto it = runs.rbegin(); it != runs.rend(); ++it) {
+                const uint32_t a = it->first, b = it->second;
+                const uint32_t blocks = std::min<uint32_t>((b - a + COLOR_THREADS - 1) / COLOR_THREADS, ctx->num_sms * 8);
+                k_jp_class<<<blocks, COLOR_THREADS, 0, ctx->stream>>>(g->order, a, b, g->V, g->P, g->pc, g->color,
+                                                                     ctx->dstate, ctx->spin_limit);
+                ctx->launches++;
+            }
+        }
+        if ((s = gc_check_launch(ctx, "jp classes")) != GC_OK) return s;
+        // the leaf kernels append to the big-leaf list from a zero count, as after the ticket kernel
+        k_reset_ticket<<<1, 1, 0, ctx->stream>>>(ctx->dstate, nullptr);
+        ctx->launches++;
+        {
+            ProfScope ps(ctx, "jp_leaves", ctx->stream);
+            k_jp_leaves<<<grid, 256, 0, ctx->stream>>>(g->V, g->E, g->pc, N, g->color, g->leaf_list, ctx->dstate);
+            k_jp_big_leaves<<<ctx->num_sms * 2, COLOR_THREADS, 0, ctx->stream>>>(g->V, g->E, g->leaf_list, g->color,
+                                                                                  ctx->dstate, ctx->spin_limit);
+            ctx->launches += 2;
+        }
+        if ((s = gc_check_launch(ctx, "jp color")) != GC_OK) return s;
+        g->has_colors = true;
+        g->colors_ours = true;
+        return GC_OK;
+    }
+
     if ((s = gc_alloc(ctx, &g->jprec, g->cap_N, "ticket records")) != GC_OK) return s;
     k_jp_records<<<ctx->num_sms * 4, 256, 0, ctx->stream>>>(g->order, g->V, g->pc, ctx->dstate, g->jprec);
     ctx->launches++;
@@ -639,11 +759,12 @@ gc_status gc_jp_color(gc_graph *g) {
         ProfScope ps(ctx, "jp_leaves", ctx->stream);
         k_jp_leaves<<<grid, 256, 0, ctx->stream>>>(g->V, g->E, g->pc, N, g->color, g->leaf_list, ctx->dstate);
         k_jp_big_leaves<<<ctx->num_sms * 2, COLOR_THREADS, 0, ctx->stream>>>(g->V, g->E, g->leaf_list, g->color,
-                                                                              ctx->dstate);
+                                                                              ctx->dstate, ctx->spin_limit);
         ctx->launches += 2;
     }
     if ((s = gc_check_launch(ctx, "jp color")) != GC_OK) return s;
     g->has_colors = true;
+    g->colors_ours = true;
     return GC_OK;
 }
 
@@ -653,7 +774,9 @@ gc_status gc_keys_from_colors(gc_graph *g) {
     ProfScope ps(ctx, "culberson_keys", ctx->stream);
     k_keys_from_colors<<<ctx->num_sms * 4, 256, 0, ctx->stream>>>(g->color, g->N, g->key);
     ctx->launches++;
-    g->key_kind = 100;
+    // the library's own colors are at most max degree + 1 (narrow sort, class rounds); caller colors
+    // may be anything (full-width keys, tickets)
+    g->key_kind = g->colors_ours ? 100 : 101;
     return gc_check_launch(ctx, "culberson keys");
 }
 

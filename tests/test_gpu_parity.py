@@ -259,3 +259,40 @@ def test_cli_output_lines(golden, tmp_path):
     expect = [int(golden.get("er1500", h, "color").max()) for h in ("FF", "LF", "LLF", "SL", "SLL")]
     expect += [0, 0, 0] + [int(golden.get("er1500", f"GNN{L}", "color").max()) for L in (2, 3, 4)]
     assert vals == expect
+
+
+def test_recolor_from_caller_colors(gpu_ctx):
+    """Culberson rounds on a coloring the caller uploaded (colors far above max degree + 1): the keys
+    are the caller's colors, so the result is the greedy coloring in that order (oracle)."""
+    N, V, E = gcn.gen_rmat(1 << 12, 8, 77)
+    g = gcn.Graph(gpu_ctx, N, V, E)
+    user = (np.arange(N, dtype=np.int32) * 7 + 3)  # all distinct, so proper; up to ~28,000
+    g.set_colors(user)
+    g.recolor(1)
+    ref, _ = O.greedy_color(N, V, E, user.astype(np.float64))
+    assert np.array_equal(g.colors(), ref)
+    g.recolor(2)  # then rounds on the library's own colors
+    ref2 = ref
+    for _ in range(2):
+        ref2, _ = O.greedy_color(N, V, E, ref2.astype(np.float64))
+    assert np.array_equal(g.colors(), ref2)
+    g.close()
+
+
+@pytest.mark.parametrize("heur", ["LF", "GNN3"])
+def test_culberson_classes_match_tickets(gpu_ctx, heur):
+    """Class-by-class Culberson rounds give the same colors as the oracle's rounds, on skewed and
+    mesh-like graphs."""
+    params, md = gcn.synthetic_model(3, 1003)
+    m = gcn.Model(gpu_ctx, params, md)
+    for N, V, E in (gcn.gen_rmat(1 << 14, 16, 5), gcn.gen_stencil27(24, 24, 24)):
+        g = gcn.Graph(gpu_ctx, N, V, E)
+        g.priority("GNN" if heur == "GNN3" else heur, m if heur == "GNN3" else None)
+        g.color(4)
+        p = O.ordering("GNN" if heur == "GNN3" else heur, N, V, E, params, md)
+        c, _ = O.greedy_color(N, V, E, p)
+        for _ in range(4):
+            c, _ = O.greedy_color(N, V, E, c.astype(np.float64))
+        assert np.array_equal(g.colors(), c), (heur, N)
+        g.close()
+    m.close()
