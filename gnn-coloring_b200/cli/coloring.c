@@ -7,8 +7,8 @@
  *   NAME_i colors seconds_seq seconds_tc1 ... seconds_tcn
  * Heuristic order FF, LF, LLF, SL, SLL, GNN2, GNN3, GNN4 (LLF and SLL skipped with -f).
  * Quick mode (-q) prints "FF LF LLF SL SLL ID SDA SD GNN2 GNN3 GNN4" color counts after K-1
- * recolorings (src/main.c:135-188).  ID, SDA and SD are sequential heap orderings that this
- * library does not implement; their slots print 0, as the reference prints them with -f.
+ * recolorings (src/main.c:135-188).  ID, SDA and SD are the reference's sequential orderings, run
+ * on the host (include/incidence_degree.h); with -f they print 0, as in the reference.
  *
  * -c 0 behaves like -c 1 (a single coloring, reported as NAME_0); the reference crashes there.
  * -t and the thread counts are accepted for compatibility; every column times the GPU path.
@@ -20,6 +20,7 @@
 #include <time.h>
 #include <unistd.h>
 
+#include "incidence_degree.h"
 #include "coloring.h"
 #include "fast_io.h"
 #include "first_fit.h"
@@ -111,7 +112,7 @@ int main(int argc, char **argv) {
         void *jp = jones_plassmann_setup(N, V[N]);
         double *p = malloc(sizeof(double) * ((size_t)N + 8));
         int *color = malloc(sizeof(int) * (N ? N : 1));
-        int ff, lf, llf = 0, sl, sll = 0, gnn2, gnn3, gnn4;
+        int ff, lf, llf = 0, sl, sll = 0, id = 0, sda = 0, sd = 0, gnn2, gnn3, gnn4;
         first_fit_ordering_par(N, V, E, p);
         ff = quick_count(N, V, E, jp, p, color, K);
         largest_degree_first_ordering(N, V, E, p);
@@ -129,9 +130,15 @@ int main(int argc, char **argv) {
             llf = quick_count(N, V, E, jp, p, color, K);
             smallest_log_degree_last_ordering(N, V, E, p);
             sll = quick_count(N, V, E, jp, p, color, K);
+            incidence_degree_ordering(N, V, E, p);
+            id = quick_count(N, V, E, jp, p, color, K);
+            saturation_degree_ordering_alt(N, V, E, p);
+            sda = quick_count(N, V, E, jp, p, color, K);
+            saturation_degree_ordering(N, V, E, p);
+            sd = quick_count(N, V, E, jp, p, color, K);
         }
         if (verbose) printf("FF LF LLF SL SLL ID SDA SD GNN2 GNN3 GNN4\n");
-        printf("%d %d %d %d %d %d %d %d %d %d %d\n", ff, lf, llf, sl, sll, 0, 0, 0, gnn2, gnn3, gnn4);
+        printf("%d %d %d %d %d %d %d %d %d %d %d\n", ff, lf, llf, sl, sll, id, sda, sd, gnn2, gnn3, gnn4);
         jones_plassmann_cleanup(jp);
         free(p);
         free(color);

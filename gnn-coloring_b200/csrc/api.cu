@@ -194,6 +194,7 @@ gc_status gc_ctx_create(int device, gc_ctx **out) {
     if (const char *e = getenv("GC_JP_DECIDE")) ctx->jp_decide = atoi(e) != 0;
     if (const char *e = getenv("GC_JP_NAP")) ctx->jp_nap = (unsigned int)strtoul(e, nullptr, 10);
     if (const char *e = getenv("GC_GNN_WARP_DEGREE")) ctx->gnn_warp_deg = (uint32_t)strtoul(e, nullptr, 10);
+    if (const char *e = getenv("GC_GNN_GIANT_DEGREE")) ctx->gnn_giant_deg = (uint32_t)strtoul(e, nullptr, 10);
     if (const char *e = getenv("GC_GNN_THIN_DEGREE")) ctx->gnn_thin_deg = (uint32_t)strtoul(e, nullptr, 10);
     if (const char *e = getenv("GC_GNN_SERIAL")) ctx->gnn_serial = atoi(e) != 0;  // 1: hubs first, then the bulk
     if (s != GC_OK) {

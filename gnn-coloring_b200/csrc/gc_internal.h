@@ -40,6 +40,7 @@ struct gc_ctx {
     bool jp_classes = true;              // Culberson rounds: class by class instead of tickets
     int gnn_blocks_per_sm[3] = {0, 0, 0};  // resident CTAs of each GNN layer kernel
     uint32_t gnn_warp_deg = GC_GNN_WIDE_DEGREE;  // GNN: above this many neighbours a vertex gets a warp
+    uint32_t gnn_giant_deg = 0;          // GNN: hubs with at least this many neighbours are staged (0: automatic)
     uint32_t gnn_thin_deg = 16;          // GNN: vertices with at most this many neighbours get one lane each
     bool gnn_serial = false;             // hub CTAs beside the bulk on a high-priority stream (GC_GNN_SERIAL=1: before it)
     bool hub_smem_set[3] = {false, false, false};  // hub kernels' shared-memory limit raised

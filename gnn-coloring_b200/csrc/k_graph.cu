@@ -159,7 +159,7 @@ gc_status gc_graph_prepare(gc_graph *g) {
             return s;
         // giant hubs (the leading ones): staging offsets and gather tasks
         const uint32_t dmax = hp[2 * idx[0] + 1];
-        const uint32_t thr = std::max<uint32_t>(2 * g->hub_deg, dmax / 3);
+        const uint32_t thr = ctx->gnn_giant_deg ? ctx->gnn_giant_deg : std::max<uint32_t>(2 * g->hub_deg, dmax / 3);
         std::vector<uint32_t> gw(1, 0), tasks;
         uint64_t rows = 0;
         for (uint32_t i = 0; i < n_hubs; i++) {

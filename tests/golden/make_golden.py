@@ -10,6 +10,8 @@ oracle/_ref/libref.so, which oracle/Makefile compiles from the reference's uncha
                         for several small graphs and hand-built edge cases.  Graphs are stored too.
   golden_refmodels.npz  GNN2/3/4 priorities and colors with the reference's own model files
                         (models/m{2,3,4}.gnn); the weights themselves are not stored.
+  golden_incidence.npz  the reference's ID, SDA and SD priorities (src/incidence_degree.c) and JP
+                        colors on the same graphs
   golden_mtx.npz        the reference's CSR (mtx_parse_par + graph_sort_edges_par +
                         graph_make_simple) of small Matrix Market texts with duplicates,
                         self-loops, one-sided entries, comments and value columns.
@@ -153,9 +155,35 @@ def mtx_reference(text):
         os.unlink(path)
 
 
+INCIDENCE = ("incidence_degree_ordering", "saturation_degree_ordering_alt", "saturation_degree_ordering")
+
+
+def incidence_golden(graphs):
+    """The reference's sequential orderings (src/incidence_degree.c) and JP colors on them."""
+    lib = R.lib()
+    u32 = C.POINTER(C.c_uint32)
+    out = {}
+    for name, (N, V, E) in graphs.items():
+        Vc = np.ascontiguousarray(V, np.uint32)
+        Ec = np.ascontiguousarray(E if len(E) else np.zeros(1, np.uint32), np.uint32)
+        for fn in INCIDENCE:
+            getattr(lib, fn).argtypes = [C.c_uint32, u32, u32, C.c_void_p]
+            pbuf = R.aligned(N + 8, np.float64)
+            if N:
+                getattr(lib, fn)(N, Vc.ctypes.data_as(u32), Ec.ctypes.data_as(u32), pbuf.ctypes.data)
+            pv = pbuf[:N].copy()
+            out[f"{name}/{fn}/p"] = pv
+            out[f"{name}/{fn}/color"] = jp_color(N, V, E, pv)
+    np.savez_compressed(os.path.join(OUT, "golden_incidence.npz"), **out)
+    print("golden_incidence.npz", os.path.getsize(os.path.join(OUT, "golden_incidence.npz")), "bytes")
+
+
 def main():
     if not R.available():
         sys.exit("oracle/_ref/libref.so is missing: run `make -C oracle` with the reference tree present")
+    if "--incidence-only" in sys.argv:
+        incidence_golden({**synth_graphs(), **edge_case_graphs()})
+        return
     R.set_threads(4)
     synth_models = {L: gcn.synthetic_model(L, seed) for L, seed in SYNTH_MODEL_SEEDS.items()}
     ref_models = {L: gcn.model_read(os.path.join(R.MODELS, f"m{L}.gnn")) for L in (2, 3, 4)}
@@ -191,6 +219,7 @@ def main():
     np.savez_compressed(os.path.join(OUT, "golden_mtx.npz"), **mtx)
     for f in ("golden_synth.npz", "golden_refmodels.npz", "golden_mtx.npz"):
         print(f, os.path.getsize(os.path.join(OUT, f)), "bytes")
+    incidence_golden(graphs)
 
 
 if __name__ == "__main__":

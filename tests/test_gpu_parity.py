@@ -8,7 +8,7 @@ import numpy as np
 import pytest
 
 import gnn_coloring as gcn
-from conftest import HEURISTICS, PKG
+from conftest import GOLDEN, HEURISTICS, PKG
 from oracle import reference as R
 from oracle import restatement as O
 
@@ -257,8 +257,29 @@ def test_cli_output_lines(golden, tmp_path):
     assert q.returncode == 0, q.stderr
     vals = [int(x) for x in q.stdout.split()]
     expect = [int(golden.get("er1500", h, "color").max()) for h in ("FF", "LF", "LLF", "SL", "SLL")]
-    expect += [0, 0, 0] + [int(golden.get("er1500", f"GNN{L}", "color").max()) for L in (2, 3, 4)]
+    inc = np.load(os.path.join(GOLDEN, "golden_incidence.npz"))
+    expect += [int(inc[f"er1500/{fn}/color"].max()) for fn in
+               ("incidence_degree_ordering", "saturation_degree_ordering_alt", "saturation_degree_ordering")]
+    expect += [int(golden.get("er1500", f"GNN{L}", "color").max()) for L in (2, 3, 4)]
     assert vals == expect
+    qf = subprocess.run([os.path.join(PKG, "cli", "coloring"), "-g", path, "-q", "-f"], capture_output=True,
+                        text=True, timeout=600, env=env)
+    valsf = [int(x) for x in qf.stdout.split()]
+    assert valsf[2] == valsf[4] == valsf[5] == valsf[6] == valsf[7] == 0  # -f skips LLF, SLL, ID, SDA, SD
+
+
+def test_incidence_orderings_color_like_the_reference(gpu_ctx, golden):
+    """JP on the ID / SDA / SD priorities (host orderings) gives the reference's colors."""
+    inc = np.load(os.path.join(GOLDEN, "golden_incidence.npz"))
+    for name in golden.graphs:
+        N, V, E = golden.graph(name)
+        for fn in ("incidence_degree_ordering", "saturation_degree_ordering_alt", "saturation_degree_ordering"):
+            p = inc[f"{name}/{fn}/p"]
+            g = gcn.Graph(gpu_ctx, N, V, E)
+            g.set_priority(p)
+            g.color()
+            assert np.array_equal(g.colors(), inc[f"{name}/{fn}/color"]), (name, fn)
+            g.close()
 
 
 def test_recolor_from_caller_colors(gpu_ctx):

@@ -109,3 +109,53 @@ def test_model_format_errors(tmp_path):
     short.write_text("1056 100\n" + " ".join(["0.5"] * 100))
     with pytest.raises(gcn.GCError):
         gcn.model_read(str(short))
+
+
+# ---- the reference's sequential orderings (host code of the library) -------------------------------
+
+INCIDENCE = ("incidence_degree_ordering", "saturation_degree_ordering_alt", "saturation_degree_ordering")
+
+
+def _ordering(fn, N, V, E):
+    import ctypes as C
+    u32 = C.POINTER(C.c_uint32)
+    f = getattr(gcn.lib, fn)
+    f.argtypes = [C.c_uint32, u32, u32, C.c_void_p]
+    Vc = np.ascontiguousarray(V, np.uint32)
+    Ec = np.ascontiguousarray(E if len(E) else np.zeros(1, np.uint32), np.uint32)
+    p = np.zeros(N + 8)
+    if N:
+        f(N, Vc.ctypes.data_as(u32), Ec.ctypes.data_as(u32), p.ctypes.data)
+    return p[:N]
+
+
+def test_incidence_orderings_match_golden(golden):
+    """ID, SDA and SD priorities equal the reference's (golden vectors from src/incidence_degree.c),
+    including components reached late and a last vertex that the reference never orders (p = -1)."""
+    inc = np.load(os.path.join(os.path.dirname(__file__), "golden", "golden_incidence.npz"))
+    for name in golden.graphs:
+        N, V, E = golden.graph(name)
+        for fn in INCIDENCE:
+            assert np.array_equal(_ordering(fn, N, V, E), inc[f"{name}/{fn}/p"]), (name, fn)
+
+
+def test_incidence_orderings_match_live_reference():
+    from oracle import reference as R
+    if not R.available():
+        pytest.skip("the reference was not compiled here (oracle/_ref)")
+    import ctypes as C
+    L = R.lib()
+    u32 = C.POINTER(C.c_uint32)
+    pairs_n = 60
+    I = np.array([0, 1, 2, 10, 11, 20, 21, 22, 30, 31], np.uint32)
+    J = np.array([1, 2, 0, 11, 12, 21, 22, 20, 31, 58], np.uint32)
+    graphs = [gcn.gen_er(3000, 20000, 5), gcn.gen_rmat(1 << 12, 8, 3), gcn.gen_rmat(5000, 4, 9),
+              gcn.gen_stencil27(9, 8, 7), gcn.csr_from_pairs(pairs_n, I, J), gcn.gen_er(40, 0, 1)]
+    for N, V, E in graphs:
+        Vc = np.ascontiguousarray(V, np.uint32)
+        Ec = np.ascontiguousarray(E if len(E) else np.zeros(1, np.uint32), np.uint32)
+        for fn in INCIDENCE:
+            getattr(L, fn).argtypes = [C.c_uint32, u32, u32, C.c_void_p]
+            ref = R.aligned(N + 8, np.float64)
+            getattr(L, fn)(N, Vc.ctypes.data_as(u32), Ec.ctypes.data_as(u32), ref.ctypes.data)
+            assert np.array_equal(_ordering(fn, N, V, E), ref[:N]), (N, fn)
