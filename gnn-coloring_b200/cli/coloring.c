@@ -13,10 +13,13 @@
  * -c 0 behaves like -c 1 (a single coloring, reported as NAME_0); the reference crashes there.
  * -t and the thread counts are accepted for compatibility; every column times the GPU path.
  * GNN models are read from models/m<l>.gnn (or $GC_MODEL_DIR/m<l>.gnn).
+ * Besides Matrix Market (.mtx), -g reads the reference's other formats by extension: PACE .gr,
+ * METIS .graph and GBBS .adj (src/fast_io.c:224-437), made simple and sorted like the .mtx path.
  */
 #include <ctype.h>
 #include <stdio.h>
 #include <stdlib.h>
+#include <string.h>
 #include <time.h>
 #include <unistd.h>
 
@@ -25,6 +28,7 @@
 #include "fast_io.h"
 #include "first_fit.h"
 #include "gnn.h"
+#include "gnn_coloring.h"
 #include "largest_degree_first.h"
 #include "smallest_degree_last.h"
 
@@ -98,8 +102,18 @@ int main(int argc, char **argv) {
     }
     uint32_t N, *V, *E;
     double t0 = wall();
-    mtx_parse_par(fp, &N, &V, &E);
-    fclose(fp);
+    const size_t plen = strlen(graph_path);
+    if (plen >= 4 && strcmp(graph_path + plen - 4, ".mtx") == 0) {
+        mtx_parse_par(fp, &N, &V, &E);
+        fclose(fp);
+    } else {
+        /* .gr, .graph or .adj: the library's readers, already sorted and simple */
+        fclose(fp);
+        if (gc_read_graph(graph_path, &N, &V, &E) != GC_OK) {
+            printf("Unable to read graph %s (expected .mtx, .gr, .graph or .adj)\n", graph_path);
+            return 1;
+        }
+    }
     if (verbose) printf("Parsing took: %.4lfs, |V|=%u, |E|=%u\n", wall() - t0, N, V[N]);
     t0 = wall();
     graph_sort_edges_par(N, V, E);

@@ -358,6 +358,10 @@ void gc_serve_destroy(gc_server *s);
  * N = max(rows, cols), every entry added in both directions, adjacency sorted ascending,
  * self-loops and duplicates dropped (src/fast_io.c:68-222, 450-477).  Arrays are malloc'd. */
 gc_status gc_mtx_read(const char *path, uint32_t *N, uint32_t **V, uint32_t **E);
+/* Reads a graph by its file extension -- .mtx (Matrix Market), .gr (PACE), .graph (METIS), .adj
+ * (GBBS adjacency) -- into the simple, symmetric, sorted CSR of gc_mtx_read (the reference's
+ * readers in src/fast_io.c followed by its clean-up steps).  Arrays are malloc'd. */
+gc_status gc_read_graph(const char *path, uint32_t *N, uint32_t **V, uint32_t **E);
 /* Builds the same CSR from L 0-based vertex pairs. */
 gc_status gc_csr_from_pairs(uint32_t N, uint64_t L, const uint32_t *I, const uint32_t *J,
                             uint32_t **V, uint32_t **E);

@@ -12,6 +12,8 @@ oracle/_ref/libref.so, which oracle/Makefile compiles from the reference's uncha
                         (models/m{2,3,4}.gnn); the weights themselves are not stored.
   golden_incidence.npz  the reference's ID, SDA and SD priorities (src/incidence_degree.c) and JP
                         colors on the same graphs
+  golden_formats.npz    texts written by the reference's mtx/adj/gr/metis writers and what its
+                        adj/gr/metis readers return for them
   golden_mtx.npz        the reference's CSR (mtx_parse_par + graph_sort_edges_par +
                         graph_make_simple) of small Matrix Market texts with duplicates,
                         self-loops, one-sided entries, comments and value columns.
@@ -178,11 +180,70 @@ def incidence_golden(graphs):
     print("golden_incidence.npz", os.path.getsize(os.path.join(OUT, "golden_incidence.npz")), "bytes")
 
 
+def formats_golden():
+    """Texts written by the reference's writers and what its readers return for them (fast_io.c)."""
+    lib = R.lib()
+    libc = C.CDLL(None)
+    libc.fopen.restype = C.c_void_p
+    libc.fopen.argtypes = [C.c_char_p, C.c_char_p]
+    libc.fclose.argtypes = [C.c_void_p]
+    u32 = C.POINTER(C.c_uint32)
+    out = {}
+    cases = {"er300": gcn.gen_er(300, 1200, 11), "rmat9": gcn.gen_rmat(512, 8, 12), "stencil": gcn.gen_stencil27(4, 3, 3)}
+    cases["edgeless"] = gcn.gen_er(12, 0, 1)
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "g").encode()
+        for name, (N, V, E) in cases.items():
+            Vc = np.ascontiguousarray(V, np.uint32)
+            Ec = np.ascontiguousarray(E if len(E) else np.zeros(1, np.uint32), np.uint32)
+            W = np.arange(N, dtype=np.uint32) * 3 + 1
+            weighted = bool(np.all(np.diff(V.astype(np.int64)) > 0))  # the reader mis-reads weighted isolated vertices
+            for store, parse in (("mtx_store", None), ("adj_store", "adj_parse"), ("gr_store", "gr_parse"),
+                                 ("metis_store", "metis_parse")):
+                f = libc.fopen(path, b"wb")
+                if store == "metis_store":
+                    getattr(lib, store).argtypes = [C.c_void_p, C.c_uint32, u32, u32, C.c_void_p]
+                    getattr(lib, store)(f, N, Vc.ctypes.data_as(u32), Ec.ctypes.data_as(u32),
+                                        W.ctypes.data if weighted else None)
+                else:
+                    getattr(lib, store).argtypes = [C.c_void_p, C.c_uint32, u32, u32]
+                    getattr(lib, store)(f, N, Vc.ctypes.data_as(u32), Ec.ctypes.data_as(u32))
+                libc.fclose(f)
+                text = open(path, "rb").read()
+                key = f"{name}/{store}"
+                out[f"{key}/text"] = np.frombuffer(text, np.uint8)
+                out[f"{name}/N"], out[f"{name}/V"], out[f"{name}/E"] = np.array(N), V, E
+                if parse is None:
+                    continue
+                n, pV, pE = C.c_uint32(), u32(), u32()
+                f = libc.fopen(path, b"rb")
+                if parse == "metis_parse":
+                    pW = u32()
+                    getattr(lib, parse).argtypes = [C.c_void_p, C.POINTER(C.c_uint32), C.POINTER(u32), C.POINTER(u32),
+                                                    C.POINTER(u32)]
+                    getattr(lib, parse)(f, C.byref(n), C.byref(pV), C.byref(pE), C.byref(pW))
+                else:
+                    getattr(lib, parse).argtypes = [C.c_void_p, C.POINTER(C.c_uint32), C.POINTER(u32), C.POINTER(u32)]
+                    getattr(lib, parse)(f, C.byref(n), C.byref(pV), C.byref(pE))
+                libc.fclose(f)
+                k = n.value
+                rV = np.ctypeslib.as_array(pV, (k + 1,)).copy()
+                rE = np.ctypeslib.as_array(pE, (max(int(rV[k]), 1),))[:int(rV[k])].copy()
+                out[f"{key}/parsed_V"], out[f"{key}/parsed_E"] = rV, rE
+                if parse == "metis_parse" and weighted:
+                    out[f"{key}/parsed_W"] = np.ctypeslib.as_array(pW, (k,)).copy()
+    np.savez_compressed(os.path.join(OUT, "golden_formats.npz"), **out)
+    print("golden_formats.npz", os.path.getsize(os.path.join(OUT, "golden_formats.npz")), "bytes")
+
+
 def main():
     if not R.available():
         sys.exit("oracle/_ref/libref.so is missing: run `make -C oracle` with the reference tree present")
     if "--incidence-only" in sys.argv:
         incidence_golden({**synth_graphs(), **edge_case_graphs()})
+        return
+    if "--formats-only" in sys.argv:
+        formats_golden()
         return
     R.set_threads(4)
     synth_models = {L: gcn.synthetic_model(L, seed) for L, seed in SYNTH_MODEL_SEEDS.items()}
@@ -220,6 +281,7 @@ def main():
     for f in ("golden_synth.npz", "golden_refmodels.npz", "golden_mtx.npz"):
         print(f, os.path.getsize(os.path.join(OUT, f)), "bytes")
     incidence_golden(graphs)
+    formats_golden()
 
 
 if __name__ == "__main__":
