@@ -209,5 +209,10 @@ enum { SORT_KEEP_ALL = 0, SORT_KEEP_INNER = 1, SORT_KEEP_DEG_AT_MOST = 2 };
 gc_status gc_sort_vertices(gc_graph *g, const uint32_t *keys, int key_bits, int filter, uint32_t max_deg,
                            uint32_t *out, uint32_t *d_count);
 gc_status gc_sort_order_bits(gc_graph *g, int key_bits, bool filter, uint32_t *d_count);
+// Stable sort of n (key, value) pairs by ascending key into (kout, vout); kbuf, vbuf: n-word
+// scratch; hist: gc_sort_pairs_hist_words(n) words (k_sort.cu).
+size_t gc_sort_pairs_hist_words(uint32_t n);
+gc_status gc_sort_pairs(gc_ctx *ctx, uint32_t n, const uint32_t *kin, const uint32_t *vin, int key_bits,
+                        uint32_t *kbuf, uint32_t *vbuf, uint32_t *kout, uint32_t *vout, uint32_t *hist);
 // Segments (batch.cu): per-segment largest color and improper flag into g->seg_stat.
 gc_status gc_segment_stats(gc_graph *g);

@@ -237,3 +237,69 @@ gc_status gc_sort_vertices(gc_graph *g, const uint32_t *keys, int key_bits, int 
 gc_status gc_sort_order_bits(gc_graph *g, int key_bits, bool filter, uint32_t *d_count) {
     return gc_sort_vertices(g, g->key, key_bits, filter ? SORT_KEEP_INNER : SORT_KEEP_ALL, 0, g->order, d_count);
 }
+
+// Stable sort of n (key, value) pairs by ascending key into (kout, vout), reusing the passes above:
+// they order by the complemented key, so the keys are complemented on the way in and out.  kbuf and
+// vbuf are ping-pong buffers of n words; hist needs ntiles * 256 + 2 * 256 * 4 words and d_n one
+// device word.  key_bits: bit width of the largest key.
+namespace {
+__global__ void k_complement_into(const uint32_t *__restrict__ kin, uint32_t n, uint32_t *__restrict__ kout) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) kout[i] = ~kin[i];
+}
+}  // namespace
+
+size_t gc_sort_pairs_hist_words(uint32_t n) {
+    const uint32_t ntiles = (n + SORT_TILE - 1) / SORT_TILE;
+    return (size_t)RADIX * (ntiles ? ntiles : 1) + 4 * 2 * RADIX + 1;
+}
+
+gc_status gc_sort_pairs(gc_ctx *ctx, uint32_t n, const uint32_t *kin, const uint32_t *vin, int key_bits,
+                        uint32_t *kbuf, uint32_t *vbuf, uint32_t *kout, uint32_t *vout, uint32_t *hist) {
+    gc_status s;
+    if (n == 0) return GC_OK;
+    const uint32_t ntiles = (n + SORT_TILE - 1) / SORT_TILE;
+    const int passes = key_bits <= 0 ? 0 : (key_bits + 7) / 8;
+    uint32_t *digit_words = hist + (size_t)RADIX * ntiles;
+    uint32_t *d_n = digit_words + 4 * 2 * RADIX;
+    if (passes > 4) return gc_fail(ctx, GC_ERR_INVALID, "sort keys wider than 32 bits");
+    if ((s = gc_check_cuda(ctx, cudaMemsetAsync(digit_words, 0, sizeof(uint32_t) * 4 * 2 * RADIX, ctx->stream),
+                           "sort digit totals")) != GC_OK)
+        return s;
+    if ((s = gc_check_cuda(ctx, cudaMemcpyAsync(d_n, &n, sizeof(uint32_t), cudaMemcpyHostToDevice, ctx->stream),
+                           "sort length")) != GC_OK)
+        return s;
+    // complemented keys into the first buffer of the chain that ends in kout
+    uint32_t *kb[2] = {kbuf, kout}, *vb[2] = {vbuf, vout};
+    const int first = passes % 2 == 0 ? 1 : 0;  // buffer the complemented keys start in
+    k_complement_into<<<ctx->num_sms * 4, 256, 0, ctx->stream>>>(kin, n, kb[first]);
+    ctx->launches++;
+    if (passes == 0) {
+        if ((s = gc_check_cuda(ctx, cudaMemcpyAsync(vb[first], vin, 4ull * n, cudaMemcpyDeviceToDevice, ctx->stream),
+                               "sort values")) != GC_OK)
+            return s;
+    }
+    SortIn in{};
+    in.kin = kb[first];
+    in.vin = passes == 0 ? vb[first] : vin;
+    in.d_n = d_n;
+    in.N = n;
+    in.first = 0;
+    int cur = first;
+    for (int p = 0; p < passes; p++) {
+        const int nxt = cur ^ 1;
+        uint32_t *digit_total = digit_words + 2 * RADIX * p, *digit_base = digit_total + RADIX;
+        k_sort_hist<<<ntiles, SORT_THREADS, 0, ctx->stream>>>(in, 8 * p, RADIX - 1, hist, ntiles, digit_total);
+        k_sort_scan_digits<<<1, RADIX, 0, ctx->stream>>>(digit_total, digit_base, nullptr);
+        k_sort_scan_tiles<<<RADIX, SCAN_THREADS, 0, ctx->stream>>>(hist, ntiles, digit_base);
+        k_sort_scatter<<<ntiles, SORT_THREADS, 0, ctx->stream>>>(in, 8 * p, RADIX - 1, hist, ntiles, kb[nxt], vb[nxt]);
+        ctx->launches += 4;
+        if ((s = gc_check_launch(ctx, "pair sort")) != GC_OK) return s;
+        in.kin = kb[nxt];
+        in.vin = vb[nxt];
+        cur = nxt;
+    }
+    // the chain ends in (kout, vout); undo the complement
+    k_complement_into<<<ctx->num_sms * 4, 256, 0, ctx->stream>>>(kout, n, kout);
+    ctx->launches++;
+    return gc_check_launch(ctx, "pair sort");
+}

@@ -88,6 +88,8 @@ _sig("gc_download_colors", C.c_int, vp, vp, i32p)
 _sig("gc_download_priority", C.c_int, vp, vp, f64p)
 # host helpers
 _sig("gc_mtx_read", C.c_int, C.c_char_p, u32p, C.POINTER(u32p), C.POINTER(u32p))
+_sig("gc_graph_load_mtx", C.c_int, vp, C.c_char_p, C.POINTER(vp))
+_sig("gc_mtx_read_device", C.c_int, vp, C.c_char_p, u32p, C.POINTER(u32p), C.POINTER(u32p))
 _sig("gc_mtx_write", C.c_int, C.c_char_p, C.c_uint32, u32p, u32p)
 _sig("gc_csr_from_pairs", C.c_int, C.c_uint32, C.c_uint64, u32p, u32p, C.POINTER(u32p), C.POINTER(u32p))
 _sig("gc_model_read", C.c_int, C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(f32p))
@@ -297,6 +299,15 @@ def mtx_read(path: str):
     return _take_csr(N.value, Vp, Ep)
 
 
+def mtx_read_device(ctx: "Context", path: str):
+    """gc_mtx_read's CSR, built on the device (gc_mtx_read_device)."""
+    N = C.c_uint32()
+    Vp, Ep = u32p(), u32p()
+    ctx.check(lib.gc_mtx_read_device(ctx.h, str(path).encode(), C.byref(N), C.byref(Vp), C.byref(Ep)),
+              f"mtx_read_device {path}")
+    return _take_csr(N.value, Vp, Ep)
+
+
 def mtx_write(path: str, N: int, V: np.ndarray, E: np.ndarray):
     V = np.ascontiguousarray(V, np.uint32)
     E = np.ascontiguousarray(E, np.uint32)
@@ -423,6 +434,17 @@ class Model:
 
 
 class Graph:
+    @classmethod
+    def load_mtx(cls, ctx: Context, path: str) -> "Graph":
+        """A Matrix Market file parsed and turned into a CSR on the device (gc_graph_load_mtx)."""
+        h = vp()
+        ctx.check(lib.gc_graph_load_mtx(ctx.h, str(path).encode(), C.byref(h)), f"load_mtx {path}")
+        g = cls.__new__(cls)
+        g.ctx, g.h, g.V, g.E = ctx, h, None, None
+        g.N = int(lib.gc_graph_num_vertices(h))
+        _live_objects.add(g)
+        return g
+
     def __init__(self, ctx: Context, N: int, V: np.ndarray, E: np.ndarray):
         self.ctx = ctx
         self.V = np.ascontiguousarray(V, np.uint32)

@@ -352,6 +352,17 @@ const char *gc_serve_last_error(gc_server *s);
 /* Waits for all jobs, stops the lanes and frees everything. */
 void gc_serve_destroy(gc_server *s);
 
+/* ---- Matrix Market on the device ------------------------------------------------------------ */
+
+/* Reads a Matrix Market file into a device-resident graph with the CSR of gc_mtx_read, built on the
+ * GPU: the host reads the header and streams the data lines to the device; line splitting,
+ * parsing, symmetrisation, sorting and de-duplication run there (src/fast_io.c:33-222, 450-477 are
+ * the rules).  Lines with fewer than two numbers are skipped; an entry outside 1..N is
+ * GC_ERR_FORMAT, as is a file with fewer entries than its header announces. */
+gc_status gc_graph_load_mtx(gc_ctx *ctx, const char *path, gc_graph **g);
+/* The same CSR back on the host (arrays malloc'd; free with gc_host_free). */
+gc_status gc_mtx_read_device(gc_ctx *ctx, const char *path, uint32_t *N, uint32_t **V, uint32_t **E);
+
 /* ---- host-side graph preparation (no device involved) --------------------------------------- */
 
 /* Reads a Matrix Market file into a simple, symmetric, sorted CSR with the reference's rules:
