@@ -13,8 +13,10 @@
  * -c 0 behaves like -c 1 (a single coloring, reported as NAME_0); the reference crashes there.
  * -t and the thread counts are accepted for compatibility; every column times the GPU path.
  * GNN models are read from models/m<l>.gnn (or $GC_MODEL_DIR/m<l>.gnn).
- * Besides Matrix Market (.mtx), -g reads the reference's other formats by extension: PACE .gr,
- * METIS .graph and GBBS .adj (src/fast_io.c:224-437), made simple and sorted like the .mtx path.
+ * Matrix Market (.mtx) files are parsed on the GPU (gc_mtx_read_device: the CSR of the reference's
+ * mtx_parse_par + graph_sort_edges_par + graph_make_simple, src/main.c:106-127).  Besides .mtx, -g
+ * reads the reference's other formats by extension: PACE .gr, METIS .graph and GBBS .adj
+ * (src/fast_io.c:224-437), made simple and sorted like the .mtx path.
  */
 #include <ctype.h>
 #include <stdio.h>
@@ -104,8 +106,18 @@ int main(int argc, char **argv) {
     double t0 = wall();
     const size_t plen = strlen(graph_path);
     if (plen >= 4 && strcmp(graph_path + plen - 4, ".mtx") == 0) {
-        mtx_parse_par(fp, &N, &V, &E);
+        /* Matrix Market: parsed and turned into the sorted, simple CSR on the GPU */
         fclose(fp);
+        gc_ctx *io = NULL;
+        const char *dev = getenv("GC_DEVICE");
+        gc_status st = gc_ctx_create(dev ? atoi(dev) : 0, &io);
+        if (st == GC_OK) st = gc_mtx_read_device(io, graph_path, &N, &V, &E);
+        if (st != GC_OK) {
+            printf("Unable to read graph %s: %s%s%s\n", graph_path, gc_status_string(st), io ? ": " : "",
+                   io ? gc_last_error(io) : "");
+            return 1;
+        }
+        gc_ctx_destroy(io);
     } else {
         /* .gr, .graph or .adj: the library's readers, already sorted and simple */
         fclose(fp);
