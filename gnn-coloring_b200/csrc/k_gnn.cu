@@ -13,11 +13,19 @@
 //   ((t0+t1)+(t2+t3)) + ((t4+t5)+(t6+t7))                                  (dense_kernel_output)
 // and the key is that float's bit pattern (the sum is >= +0, so bit order = value order).
 //
-// Mapping: lane = feature.  A half-warp owns one regular vertex: it loads 16 neighbour ids at
-// a time, then 16 neighbour rows (64 B each, coalesced), then adds them in CSR order.  Vertices
-// with more than GC_GNN_HUB_DEGREE neighbours get a whole CTA that streams neighbour rows into
-// shared memory with cp.async while one half-warp runs the sequential FP32 chain; those CTAs run
-// on a second stream so the long chains overlap the bulk of the layer.
+// Mapping, by degree (the degree order built at upload):
+//   - thin tier (at most 16 neighbours): one vertex per lane;
+//   - quad tier: four lanes per vertex, a float4 of the row each, eight vertices per warp;
+//   - warp tier (more than GC_GNN_WIDE_DEGREE neighbours): a warp per vertex, rows staged in
+//     shared memory;
+//   - hubs (more than GC_GNN_HUB_DEGREE): a CTA per hub that streams neighbour rows into shared
+//     memory with cp.async while one thread per feature runs the sequential FP32 chain; the
+//     largest hubs read rows that k_gnn_hub_gather first copies into a contiguous buffer.  Hub
+//     CTAs run on a second stream, so the long chains overlap the bulk of the layer.
+// Neighbour rows are read with __ldg: a layer never writes the features it reads.  In an A/B on
+// R-MAT 22 (GNN3) the explicit read-only load made the bulk hidden and output layers about 6 %
+// faster than the plain loads the compiler emits here; the step time did not change, since the
+// hub chains bound each layer.
 //
 // Compiled without fast-math; every add, divide and FMA is an explicit round-to-nearest
 // intrinsic so the compiler cannot contract or reassociate them.
@@ -117,7 +125,7 @@ __device__ __forceinline__ void warp_vertex(uint32_t u, const uint32_t *__restri
         const uint32_t e = nxt;
         nxt = c + 32 + lane < d ? ld_stream(E + beg + c + 32 + lane) : 0u;
         if (MODE == MODE_INPUT) {
-            const float2 t = c + lane < d ? t01[e] : make_float2(0.0f, 0.0f);
+            const float2 t = c + lane < d ? __ldg(t01 + e) : make_float2(0.0f, 0.0f);
             reinterpret_cast<float2 *>(slab)[lane] = t;
             __syncwarp();
             const uint32_t cnt = min(32u, d - c);
@@ -130,7 +138,7 @@ __device__ __forceinline__ void warp_vertex(uint32_t u, const uint32_t *__restri
             for (int j = 0; j < 4; j++) {
                 const int m = j * 8 + (lane >> 2);  // this lane fetches features 4q..4q+3 of row m
                 const uint32_t v = __shfl_sync(FULL, e, m);
-                r[j] = c + m < d ? X4[(size_t)v * 4 + q] : zero4;
+                r[j] = c + m < d ? __ldg(X4 + (size_t)v * 4 + q) : zero4;
             }
 #pragma unroll
             for (int j = 0; j < 4; j++) reinterpret_cast<float4 *>(slab)[(j * 8 + (lane >> 2)) * 4 + q] = r[j];
@@ -226,7 +234,7 @@ __global__ void __launch_bounds__(GNN_THREADS, 4) k_gnn_layer(const uint32_t *__
             float s0 = 0.0f, s1 = 0.0f;
             for (uint32_t c = 0; c < dmax; c += 4) {
                 float2 t = make_float2(0.0f, 0.0f);
-                if (c + q < d) t = t01[ld_stream(E + beg + c + q)];
+                if (c + q < d) t = __ldg(t01 + ld_stream(E + beg + c + q));
 #pragma unroll
                 for (int k = 0; k < 4; k++) {
                     const float a0 = __shfl_sync(FULL, t.x, qbase + k);
@@ -257,14 +265,14 @@ __global__ void __launch_bounds__(GNN_THREADS, 4) k_gnn_layer(const uint32_t *__
 #pragma unroll
                 for (int k = 0; k < 8; k++) {
                     const uint32_t v = __shfl_sync(FULL, k < 4 ? e0 : e1, qbase + (k & 3));
-                    r[k] = c + k < d ? X4[(size_t)v * 4 + q] : zero4;
+                    r[k] = c + k < d ? __ldg(X4 + (size_t)v * 4 + q) : zero4;
                 }
 #pragma unroll
                 for (int k = 0; k < 8; k++)
                     if (c + k < d) s = add4(s, r[k]);
             }
             if (fd > 0.0f) s = make_float4(__fdiv_rn(s.x, fd), __fdiv_rn(s.y, fd), __fdiv_rn(s.z, fd), __fdiv_rn(s.w, fd));
-            const float4 self = valid ? X4[(size_t)u * 4 + q] : zero4;
+            const float4 self = valid ? __ldg(X4 + (size_t)u * 4 + q) : zero4;
             out = dense_quad<MODE>(W4, b4, q, qbase, FULL, s, self, 0.0f, 0.0f, 0.0f, 0.0f);
         }
         if (MODE == MODE_OUTPUT) {
@@ -310,10 +318,10 @@ __global__ void __launch_bounds__(THIN_THREADS, 3) k_gnn_thin(const uint32_t *__
         for (int j = 0; j < FEAT; j++) c[j] = sW[2 * FEAT * FEAT + j];
         if (MODE == MODE_INPUT) {
             float s0 = 0.0f, s1 = 0.0f;
-            float2 tn = d ? t01[__ldg(E + beg)] : make_float2(0.0f, 0.0f);
+            float2 tn = d ? __ldg(t01 + __ldg(E + beg)) : make_float2(0.0f, 0.0f);
             for (uint32_t k = 0; k < dmax; k++) {
                 const float2 t = tn;
-                if (k + 1 < d) tn = t01[__ldg(E + beg + k + 1)];
+                if (k + 1 < d) tn = __ldg(t01 + __ldg(E + beg + k + 1));
                 if (k < d) {
                     s0 = __fadd_rn(s0, t.x);
                     s1 = __fadd_rn(s1, t.y);
@@ -346,7 +354,7 @@ __global__ void __launch_bounds__(THIN_THREADS, 3) k_gnn_thin(const uint32_t *__
             {
                 const uint32_t v0 = d ? __ldg(E + beg) : 0u;
 #pragma unroll
-                for (int p = 0; p < 4; p++) rn[p] = d ? X4[(size_t)v0 * 4 + p] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                for (int p = 0; p < 4; p++) rn[p] = d ? __ldg(X4 + (size_t)v0 * 4 + p) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
             }
             for (uint32_t k = 0; k < dmax; k++) {
                 float4 r[4];
@@ -356,7 +364,7 @@ __global__ void __launch_bounds__(THIN_THREADS, 3) k_gnn_thin(const uint32_t *__
                     const uint32_t v = vnext;
                     vnext = k + 2 < d ? __ldg(E + beg + k + 2) : 0u;
 #pragma unroll
-                    for (int p = 0; p < 4; p++) rn[p] = X4[(size_t)v * 4 + p];
+                    for (int p = 0; p < 4; p++) rn[p] = __ldg(X4 + (size_t)v * 4 + p);
                 }
                 if (k < d) {
 #pragma unroll
@@ -375,7 +383,7 @@ __global__ void __launch_bounds__(THIN_THREADS, 3) k_gnn_thin(const uint32_t *__
             float self[FEAT];
 #pragma unroll
             for (int p = 0; p < 4; p++) {
-                const float4 s4 = valid ? X4[(size_t)u * 4 + p] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                const float4 s4 = valid ? __ldg(X4 + (size_t)u * 4 + p) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
                 self[4 * p + 0] = s4.x;
                 self[4 * p + 1] = s4.y;
                 self[4 * p + 2] = s4.z;
@@ -500,7 +508,7 @@ __global__ void __launch_bounds__(256) k_gnn_hub_gather(const uint32_t *__restri
         const size_t off = giant[slot];
         if (MODE == MODE_INPUT) {
             float2 *dst = reinterpret_cast<float2 *>(stage) + off;
-            for (uint32_t r = r0 + lane; r < rend; r += 32) dst[r] = t01[ld_stream(E + base + r)];
+            for (uint32_t r = r0 + lane; r < rend; r += 32) dst[r] = __ldg(t01 + ld_stream(E + base + r));
         } else {
             const float4 *X4 = reinterpret_cast<const float4 *>(x);
             float4 *dst = reinterpret_cast<float4 *>(stage) + off * 4;
@@ -511,7 +519,7 @@ __global__ void __launch_bounds__(256) k_gnn_hub_gather(const uint32_t *__restri
                 for (int k = 0; k < 4; k++) v[k] = r + 8 * k < rend ? E[base + r + 8 * k] : 0u;
 #pragma unroll
                 for (int k = 0; k < 4; k++)
-                    if (r + 8 * k < rend) val[k] = X4[(size_t)v[k] * 4 + q];
+                    if (r + 8 * k < rend) val[k] = __ldg(X4 + (size_t)v[k] * 4 + q);
 #pragma unroll
                 for (int k = 0; k < 4; k++)
                     if (r + 8 * k < rend) dst[(size_t)(r + 8 * k) * 4 + q] = val[k];

@@ -58,8 +58,8 @@ __global__ void __launch_bounds__(256) k_jp_split(const uint32_t *__restrict__ V
             for (uint32_t c = 0; c < d; c += 64) {
                 const uint32_t ia = c + lane, ib = c + 32 + lane;
                 const uint32_t va = ia < d ? ld_stream(E + beg + ia) : 0u, vb = ib < d ? ld_stream(E + beg + ib) : 0u;
-                const bool pa = ia < d && precedes(key[va], va, ku, u);
-                const bool pb = ib < d && precedes(key[vb], vb, ku, u);
+                const bool pa = ia < d && precedes(__ldg(key + va), va, ku, u);
+                const bool pb = ib < d && precedes(__ldg(key + vb), vb, ku, u);
                 const unsigned int ma = __ballot_sync(0xffffffffu, pa);
                 if (pa) P[beg + cnt + __popc(ma & lt)] = va;
                 cnt += __popc(ma);
@@ -81,7 +81,7 @@ __global__ void __launch_bounds__(256) k_jp_split(const uint32_t *__restrict__ V
         for (uint32_t c = 0; c < dmax; c += 4) {
             const uint32_t i = c + q;
             const uint32_t v = i < d ? ld_stream(E + beg + i) : 0u;
-            const bool p = i < d && precedes(key[v], v, ku, u);
+            const bool p = i < d && precedes(__ldg(key + v), v, ku, u);
             const unsigned int qm = (__ballot_sync(0xffffffffu, p) >> qbase) & 0xfu;
             if (p) P[beg + cnt + __popc(qm & qlt)] = v;
             cnt += __popc(qm);
@@ -117,8 +117,8 @@ __global__ void __launch_bounds__(SPLIT_WARPS * 32) k_jp_split_big(const uint32_
         for (uint32_t i0 = e0; i0 < end; i0 += 64) {
             const uint32_t ia = i0 + lane, ib = i0 + 32 + lane;
             const uint32_t va = ia < end ? ld_stream(E + ia) : 0u, vb = ib < end ? ld_stream(E + ib) : 0u;
-            const bool pa = ia < end && precedes(key[va], va, ku, u);
-            const bool pb = ib < end && precedes(key[vb], vb, ku, u);
+            const bool pa = ia < end && precedes(__ldg(key + va), va, ku, u);
+            const bool pb = ib < end && precedes(__ldg(key + vb), vb, ku, u);
             const unsigned int ma = __ballot_sync(0xffffffffu, pa);
             if (pa) mine[cnt + __popc(ma & lt)] = va;
             cnt += __popc(ma);
@@ -182,7 +182,7 @@ __device__ int color_one(const uint32_t *__restrict__ list, uint32_t cnt, const 
 #pragma unroll
             for (int q = 0; q < LOADS; q++) {
                 const uint32_t j = j0 + q * 32 + lane;
-                v[q] = j < cnt ? list[j] : 0xffffffffu;
+                v[q] = j < cnt ? __ldg(list + j) : 0xffffffffu;
             }
 #pragma unroll
             for (int q = 0; q < LOADS; q++) c[q] = v[q] != 0xffffffffu ? ld_relaxed(color + v[q]) : -1;
@@ -217,7 +217,7 @@ __device__ int color_one(const uint32_t *__restrict__ list, uint32_t cnt, const 
             while (w && !gave_up) {
                 const int k = __ffsll((long long)w) - 1;
                 w &= w - 1;
-                const int cc = ld_relaxed(color + list[(uint32_t)k * 32 + lane]);
+                const int cc = ld_relaxed(color + __ldg(list + (uint32_t)k * 32 + lane));
                 if (cc) {
                     mark(fb, cc, window);
                     waiting &= ~(1ull << k);
@@ -272,7 +272,7 @@ __device__ int color_one_v(const uint32_t *__restrict__ list, uint32_t cnt, cons
 #pragma unroll
             for (int q = 0; q < LOADS; q++) {
                 const uint32_t j = j0 + q * 32 + lane;
-                v[q] = j < cnt ? list[j] : 0xffffffffu;
+                v[q] = j < cnt ? __ldg(list + j) : 0xffffffffu;
             }
 #pragma unroll
             for (int q = 0; q < LOADS; q++) c[q] = v[q] != 0xffffffffu ? ld_relaxed(color + v[q]) : -1;
