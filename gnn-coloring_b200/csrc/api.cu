@@ -91,6 +91,18 @@ __global__ void k_check_csr(const uint32_t *__restrict__ V, const uint32_t *__re
         if (E[i] >= N) gc::raise_error(st, gc::ERR_BOUND, i);
 }
 
+// The two halves of k_check_csr, for uploads that check V before E has arrived.
+__global__ void k_check_offsets(const uint32_t *__restrict__ V, uint32_t N, uint32_t M, gc::DevState *st) {
+    for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < N; u += gridDim.x * blockDim.x) {
+        uint32_t a = V[u], b = V[u + 1];
+        if (b < a || b > M) gc::raise_error(st, gc::ERR_BOUND, u);
+    }
+}
+__global__ void k_check_ids(const uint32_t *__restrict__ E, uint32_t N, uint32_t M, gc::DevState *st) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < M; i += gridDim.x * blockDim.x)
+        if (E[i] >= N) gc::raise_error(st, gc::ERR_BOUND, i);
+}
+
 __global__ void k_keys_to_double(const uint32_t *__restrict__ key, uint32_t N, int float_bits, double *__restrict__ p) {
     for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < N; u += gridDim.x * blockDim.x)
         p[u] = float_bits ? (double)__uint_as_float(key[u]) : (double)key[u];
@@ -149,6 +161,84 @@ gc_status gc_graph_finish_upload(gc_graph *g) {
         return s == GC_ERR_DEVICE ? gc_fail(ctx, GC_ERR_INVALID, "malformed CSR: V not monotone or E out of range") : s;
     return gc_graph_prepare(g);
 }
+
+gc_status gc_copy_stream(gc_ctx *ctx) {
+    if (ctx->copy_stream) return GC_OK;
+    gc_status s = gc_check_cuda(ctx, cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking), "copy stream");
+    if (s == GC_OK)
+        s = gc_check_cuda(ctx, cudaEventCreateWithFlags(&ctx->ev_copy_fence, cudaEventDisableTiming), "copy events");
+    if (s == GC_OK)
+        s = gc_check_cuda(ctx, cudaEventCreateWithFlags(&ctx->ev_copy_done, cudaEventDisableTiming), "copy events");
+    return s;
+}
+
+bool gc_is_pinned(const void *host_ptr) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, host_ptr) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
+namespace {
+
+// Upload of a CSR whose E is page-locked host memory: E goes up on the copy stream while V is
+// checked and the graph prepared on the context's stream (preparation reads V only); E is checked
+// once it has arrived.  Returns only after the copy has finished, so the caller may reuse E.
+gc_status reupload_overlapped(gc_ctx *ctx, gc_graph *g, const uint32_t *V, const uint32_t *E) {
+    const uint32_t N = g->N, M = g->M;
+    gc_status s = gc_copy_stream(ctx);
+    if (s != GC_OK) return s;
+    g->has_keys = g->has_colors = false;
+    g->key_kind = -1;
+    // E may still be read by earlier work on the context's stream
+    if ((s = gc_check_cuda(ctx, cudaEventRecord(ctx->ev_copy_fence, ctx->stream), "upload E")) != GC_OK) return s;
+    if ((s = gc_check_cuda(ctx, cudaStreamWaitEvent(ctx->copy_stream, ctx->ev_copy_fence, 0), "upload E")) != GC_OK)
+        return s;
+    if ((s = gc_check_cuda(ctx, cudaMemcpyAsync(g->E, E, sizeof(uint32_t) * (size_t)M, cudaMemcpyHostToDevice,
+                                                ctx->copy_stream), "upload E")) != GC_OK)
+        return s;
+    if ((s = gc_check_cuda(ctx, cudaEventRecord(ctx->ev_copy_done, ctx->copy_stream), "upload E")) != GC_OK) {
+        cudaStreamSynchronize(ctx->copy_stream);
+        return s;
+    }
+    s = gc_check_cuda(ctx, cudaMemcpyAsync(g->V, V, sizeof(uint32_t) * ((size_t)N + 1), cudaMemcpyHostToDevice,
+                                           ctx->stream), "upload V");
+    if (s == GC_OK) s = gc_reset_state(ctx);
+    if (s == GC_OK) {
+        k_check_offsets<<<ctx->num_sms * 4, 256, 0, ctx->stream>>>(g->V, N, M, ctx->dstate);
+        ctx->launches++;
+        s = gc_check_launch(ctx, "csr check");
+    }
+    if (s == GC_OK && (s = gc_read_state(ctx)) == GC_ERR_DEVICE)
+        s = gc_fail(ctx, GC_ERR_INVALID, "malformed CSR: V not monotone or E out of range");
+    if (s == GC_OK) s = gc_graph_prepare(g);
+    // from here on the context's stream follows the copy
+    const gc_status w = gc_check_cuda(ctx, cudaStreamWaitEvent(ctx->stream, ctx->ev_copy_done, 0), "upload E");
+    if (w != GC_OK) {
+        cudaStreamSynchronize(ctx->copy_stream);
+        return s != GC_OK ? s : w;
+    }
+    if (s != GC_OK) {
+        cudaStreamSynchronize(ctx->copy_stream);
+        return s;
+    }
+    if ((s = gc_reset_state(ctx)) == GC_OK) {
+        k_check_ids<<<ctx->num_sms * 4, 256, 0, ctx->stream>>>(g->E, N, M, ctx->dstate);
+        ctx->launches++;
+        s = gc_check_launch(ctx, "csr check");
+    }
+    if (s != GC_OK) {
+        cudaStreamSynchronize(ctx->copy_stream);
+        return s;
+    }
+    if ((s = gc_read_state(ctx)) != GC_OK)
+        return s == GC_ERR_DEVICE ? gc_fail(ctx, GC_ERR_INVALID, "malformed CSR: V not monotone or E out of range") : s;
+    return GC_OK;
+}
+
+}  // namespace
 
 
 extern "C" {
@@ -229,6 +319,12 @@ static void ctx_release(gc_ctx *ctx) {
         cudaEventDestroy(r.b);
     }
     for (auto e : ctx->prof_pool) cudaEventDestroy(e);
+    if (ctx->copy_stream) {
+        cudaStreamSynchronize(ctx->copy_stream);
+        cudaStreamDestroy(ctx->copy_stream);
+    }
+    if (ctx->ev_copy_fence) cudaEventDestroy(ctx->ev_copy_fence);
+    if (ctx->ev_copy_done) cudaEventDestroy(ctx->ev_copy_done);
     if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
     if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
     if (ctx->dstate) cudaFree(ctx->dstate);
@@ -342,6 +438,7 @@ gc_status gc_graph_reupload(gc_ctx *ctx, gc_graph *g, uint32_t N, const uint32_t
     if (N > g->cap_N || M > g->cap_M) return gc_fail(ctx, GC_ERR_INVALID, "graph exceeds the allocated capacity");
     g->N = N;
     g->M = M;
+    if (M && !ctx->pool && gc_is_pinned(E)) return reupload_overlapped(ctx, g, V, E);
     if ((s = gc_check_cuda(ctx, cudaMemcpyAsync(g->V, V, sizeof(uint32_t) * ((size_t)N + 1), cudaMemcpyHostToDevice,
                                                 ctx->stream), "upload V")) != GC_OK)
         return s;
@@ -614,6 +711,37 @@ gc_status gc_download_priority(gc_ctx *ctx, gc_graph *g, double *p) {
                            "download priorities")) != GC_OK)
         return s;
     return gc_check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "download priorities");
+}
+
+gc_status gc_download_priority_begin(gc_ctx *ctx, gc_graph *g, double *p, int *pending) {
+    if (!ctx || !g || !pending || (g->N && !p)) return GC_ERR_INVALID;
+    *pending = 0;
+    if (!g->has_keys) return gc_fail(ctx, GC_ERR_STATE, "no priorities computed");
+    if (g->key_kind == 200 || g->N == 0 || ctx->pool || !gc_is_pinned(p)) return gc_download_priority(ctx, g, p);
+    DeviceGuard dg(ctx);
+    gc_status s;
+    if ((s = gc_copy_stream(ctx)) != GC_OK) return s;
+    if ((s = gc_alloc(ctx, &g->p64, (size_t)g->cap_N, "priority staging")) != GC_OK) return s;
+    k_keys_to_double<<<ctx->num_sms * 4, 256, 0, ctx->stream>>>(g->key, g->N, g->key_kind == GC_GNN ? 1 : 0, g->p64);
+    ctx->launches++;
+    if ((s = gc_check_launch(ctx, "priority widening")) != GC_OK) return s;
+    if ((s = gc_check_cuda(ctx, cudaEventRecord(ctx->ev_copy_fence, ctx->stream), "download priorities")) != GC_OK)
+        return s;
+    if ((s = gc_check_cuda(ctx, cudaStreamWaitEvent(ctx->copy_stream, ctx->ev_copy_fence, 0), "download priorities")) !=
+        GC_OK)
+        return s;
+    if ((s = gc_check_cuda(ctx, cudaMemcpyAsync(p, g->p64, sizeof(double) * g->N, cudaMemcpyDeviceToHost,
+                                                ctx->copy_stream), "download priorities")) != GC_OK)
+        return s;
+    *pending = 1;
+    return GC_OK;
+}
+
+gc_status gc_download_priority_wait(gc_ctx *ctx) {
+    if (!ctx) return GC_ERR_INVALID;
+    DeviceGuard dg(ctx);
+    return ctx->copy_stream ? gc_check_cuda(ctx, cudaStreamSynchronize(ctx->copy_stream), "download priorities")
+                            : GC_OK;
 }
 
 }  // extern "C"

@@ -32,6 +32,8 @@ struct gc_ctx {
     cudaStream_t stream = nullptr;
     cudaStream_t side_stream = nullptr;  // GNN hub CTAs run here, overlapping the bulk of a layer
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    cudaStream_t copy_stream = nullptr;  // host copies that overlap work on `stream` (created on first use)
+    cudaEvent_t ev_copy_fence = nullptr, ev_copy_done = nullptr;
     int color_blocks_per_sm = 0;         // resident CTAs of the coloring kernel (occupancy query)
     int jp_ctas_per_sm = 2;              // CTAs per SM of the coloring kernel: fewer pollers beat more lookahead (measured)
     unsigned int jp_tight = 32;          // coloring: unproductive polling rounds before sleeping
@@ -176,6 +178,8 @@ gc_status gc_check_launch(gc_ctx *ctx, const char *what);
 gc_status gc_read_state(gc_ctx *ctx);  // syncs, copies DevState, reports device errors
 gc_status gc_check_hstate(gc_ctx *ctx);  // reports device errors of an already copied DevState
 gc_status gc_reset_state(gc_ctx *ctx);
+gc_status gc_copy_stream(gc_ctx *ctx);  // creates ctx->copy_stream and its events once
+bool gc_is_pinned(const void *host_ptr);  // page-locked (or registered) host memory
 template <typename T>
 gc_status gc_alloc(gc_ctx *ctx, T **p, size_t count, const char *what) {
     if (*p) return GC_OK;

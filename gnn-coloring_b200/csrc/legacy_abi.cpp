@@ -21,6 +21,7 @@
 #include "first_fit.h"
 #include "gnn.h"
 #include "gnn_coloring.h"
+#include "overlap.h"
 #include "largest_degree_first.h"
 #include "runner.h"
 #include "smallest_degree_last.h"
@@ -161,8 +162,12 @@ void heuristic_internal(uint32_t N, const uint32_t *V, const uint32_t *E, void *
     std::lock_guard<std::recursive_mutex> lk(g_mu);
     HeurState *H = (HeurState *)hs;
     ColorState *C = (ColorState *)cs;
-    priority_into(C, N, V, E, H->h, H->model, p);
+    priority_into(C, N, V, E, H->h, H->model, nullptr);
+    // the priorities come down while the coloring runs (page-locked p; otherwise before it)
+    int pending = 0;
+    if (p) check(gc_download_priority_begin(ctx(), C->g, p, &pending), "priority download");
     color_into(C, color);
+    if (pending) check(gc_download_priority_wait(ctx()), "priority download");
 }
 
 void *heuristic_setup(gc_heuristic h, int l) {
