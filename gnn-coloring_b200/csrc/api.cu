@@ -119,7 +119,8 @@ void gc_graph_free_buffers(gc_graph *g) {
     void *bufs[] = {g->key,       g->color,  g->P,        g->pc,       g->order,    g->sort_buf, g->sort_hist,
                     g->big,       g->hubs,   g->x,        g->y,        g->t01,      g->deg_rem,  g->frontier,
                     g->frontier2, g->removed, g->leaf_list, g->vorder, g->rank,     g->p64,      g->seg_voff,
-                    g->seg_stat,  g->fmask,    g->giant,    g->hub_stage, g->jprec, g->class_first};
+                    g->seg_stat,  g->fmask,    g->giant,    g->hub_stage, g->jprec, g->class_first,
+                    g->gnn_ctr};
     for (void *p : bufs) gc_dev_free(ctx, p);
 }
 
@@ -284,6 +285,7 @@ gc_status gc_ctx_create(int device, gc_ctx **out) {
     if (const char *e = getenv("GC_JP_DECIDE")) ctx->jp_decide = atoi(e) != 0;
     if (const char *e = getenv("GC_JP_NAP")) ctx->jp_nap = (unsigned int)strtoul(e, nullptr, 10);
     if (const char *e = getenv("GC_GNN_WARP_DEGREE")) ctx->gnn_warp_deg = (uint32_t)strtoul(e, nullptr, 10);
+    if (const char *e = getenv("GC_GNN_HUB_SMS")) ctx->gnn_hub_sms = atoi(e);
     if (const char *e = getenv("GC_GNN_GIANT_DEGREE")) ctx->gnn_giant_deg = (uint32_t)strtoul(e, nullptr, 10);
     if (const char *e = getenv("GC_GNN_THIN_DEGREE")) ctx->gnn_thin_deg = (uint32_t)strtoul(e, nullptr, 10);
     if (const char *e = getenv("GC_GNN_SERIAL")) ctx->gnn_serial = atoi(e) != 0;  // 1: hubs first, then the bulk

@@ -44,6 +44,7 @@ struct gc_ctx {
     uint32_t gnn_warp_deg = GC_GNN_WIDE_DEGREE;  // GNN: above this many neighbours a vertex gets a warp
     uint32_t gnn_giant_deg = 0;          // GNN: hubs with at least this many neighbours are staged (0: automatic)
     uint32_t gnn_thin_deg = 16;          // GNN: vertices with at most this many neighbours get one lane each
+    int gnn_hub_sms = -1;                // GNN: SMs left to giant-hub CTAs (-1: one per giant hub, 0: none; GC_GNN_HUB_SMS)
     bool gnn_serial = false;             // hub CTAs beside the bulk on a high-priority stream (GC_GNN_SERIAL=1: before it)
     bool hub_smem_set[3] = {false, false, false};  // hub kernels' shared-memory limit raised
     cudaMemPool_t pool = nullptr;        // when set, graph buffers are stream-ordered allocations from this pool
@@ -124,6 +125,7 @@ struct gc_graph {
     uint64_t giant_rows = 0;         // staging rows
     float *hub_stage = nullptr;      // GNN: giant_rows + 2 rows of 16 floats (allocated on first use)
     uint64_t hub_stage_rows = 0;
+    uint32_t *gnn_ctr = nullptr;     // GNN: 8 work counters when SMs are reserved for giant hubs
     uint32_t *vorder = nullptr;      // the other vertices by descending degree (GNN schedule)
     uint32_t n_vorder = 0;
     uint32_t n_wide = 0;             // leading vorder entries with more than GC_GNN_WARP_DEGREE neighbours

@@ -59,6 +59,22 @@ __global__ void k_gnn_table0(const uint32_t *__restrict__ V, uint32_t N, float f
 
 constexpr unsigned int FULL = 0xffffffffu;
 
+__device__ __forceinline__ uint32_t sm_id() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%smid;" : "=r"(r));
+    return r;
+}
+
+// Bulk work handed out by an atomic counter, `grab` items per warp at a time (used when some SMs
+// are left to the giant-hub CTAs, so that the CTAs that do start cover all the work).
+constexpr uint32_t GNN_GRAB = 8;
+constexpr uint32_t GNN_HEAVY = 16384;  // leading four-lane items handed out one at a time
+__device__ __forceinline__ uint32_t grab_work(uint32_t *ctr, uint32_t n, int lane) {
+    uint32_t b = 0;
+    if (lane == 0) b = atomicAdd(ctr, n);
+    return __shfl_sync(0xffffffffu, b, 0);
+}
+
 __device__ __forceinline__ float4 add4(float4 s, float4 r) {
     return make_float4(__fadd_rn(s.x, r.x), __fadd_rn(s.y, r.y), __fadd_rn(s.z, r.z), __fadd_rn(s.w, r.w));
 }
@@ -199,7 +215,11 @@ __global__ void __launch_bounds__(GNN_THREADS, 4) k_gnn_layer(const uint32_t *__
                                                               const uint32_t *__restrict__ vorder, uint32_t n_wide,
                                                               uint32_t n_vorder, const float2 *__restrict__ t01,
                                                               const float *__restrict__ x, float *__restrict__ y,
-                                                              uint32_t *__restrict__ key, const float *__restrict__ Wb) {
+                                                              uint32_t *__restrict__ key, const float *__restrict__ Wb,
+                                                              uint32_t *work_ctr, uint32_t reserve) {
+    // an SM left to the giant-hub CTAs: the whole CTA leaves, except the grid's last CTA, which
+    // stays wherever it runs, so the counter's work is done whatever the placement
+    if (reserve && sm_id() < reserve && blockIdx.x != gridDim.x - 1) return;
     __shared__ __align__(16) float sW[LAYER_PARAMS];
     __shared__ __align__(16) float slabs[GNN_THREADS / 32][32 * FEAT];
     for (int i = threadIdx.x; i < LAYER_PARAMS; i += blockDim.x) sW[i] = Wb[i];
@@ -215,11 +235,11 @@ __global__ void __launch_bounds__(GNN_THREADS, 4) k_gnn_layer(const uint32_t *__
     float *slab = slabs[threadIdx.x >> 5];
     const uint32_t n_items = n_wide + (n_vorder - n_wide + 7) / 8;
 
-    for (uint32_t it = warp; it < n_items; it += nwarps) {
+    auto item = [&](uint32_t it) {
         if (it < n_wide) {
             warp_vertex<MODE>(vorder[it], V, E, t01, x, y, key, W4, sW, slab, lane);
             __syncwarp();
-            continue;
+            return;
         }
         const uint32_t g0 = n_wide + (it - n_wide) * 8;
         const uint32_t slot = g0 + (lane >> 2);
@@ -281,6 +301,39 @@ __global__ void __launch_bounds__(GNN_THREADS, 4) k_gnn_layer(const uint32_t *__
         } else if (valid) {
             Y4[(size_t)u * 4 + q] = out;
         }
+    };
+    // Dynamic hand-out (work_ctr): items are sorted heaviest first, so the warp-tier vertices
+    // (work_ctr[0]) and the leading GNN_HEAVY four-lane items (work_ctr[1]) go one at a time and
+    // spread over the warps; the rest go GNN_GRAB at a time (work_ctr[2]).  Otherwise a fixed
+    // stride.  One call site, so the item body is inlined once.
+    const uint32_t heavy_end = min(n_items, n_wide + GNN_HEAVY);
+    uint32_t phase = 0, cur = 0, end = 0, sit = warp;
+    for (;;) {
+        uint32_t it;
+        if (work_ctr) {
+            while (cur == end && phase < 3) {
+                if (phase == 0) {
+                    const uint32_t x = grab_work(work_ctr, 1u, lane);
+                    if (x < n_wide) cur = x, end = x + 1;
+                    else phase = 1;
+                } else if (phase == 1) {
+                    const uint32_t x = n_wide + grab_work(work_ctr + 1, 1u, lane);
+                    if (x < heavy_end) cur = x, end = x + 1;
+                    else phase = 2;
+                } else {
+                    const uint32_t x = heavy_end + grab_work(work_ctr + 2, GNN_GRAB, lane);
+                    if (x < n_items) cur = x, end = min(x + GNN_GRAB, n_items);
+                    else phase = 3;
+                }
+            }
+            if (cur == end) break;
+            it = cur++;
+        } else {
+            if (sit >= n_items) break;
+            it = sit;
+            sit += nwarps;
+        }
+        item(it);
     }
 }
 
@@ -298,7 +351,11 @@ __global__ void __launch_bounds__(THIN_THREADS, 3) k_gnn_thin(const uint32_t *__
                                                               const uint32_t *__restrict__ vorder, uint32_t first,
                                                               uint32_t n_vorder, const float2 *__restrict__ t01,
                                                               const float *__restrict__ x, float *__restrict__ y,
-                                                              uint32_t *__restrict__ key, const float *__restrict__ Wb) {
+                                                              uint32_t *__restrict__ key, const float *__restrict__ Wb,
+                                                              uint32_t *work_ctr, uint32_t reserve) {
+    // an SM left to the giant-hub CTAs: the whole CTA leaves, except the grid's last CTA, which
+    // stays wherever it runs, so the counter's work is done whatever the placement
+    if (reserve && sm_id() < reserve && blockIdx.x != gridDim.x - 1) return;
     __shared__ __align__(16) float sW[LAYER_PARAMS];
     for (int i = threadIdx.x; i < LAYER_PARAMS; i += blockDim.x) sW[i] = Wb[i];
     __syncthreads();
@@ -306,7 +363,7 @@ __global__ void __launch_bounds__(THIN_THREADS, 3) k_gnn_thin(const uint32_t *__
     const float4 *X4 = reinterpret_cast<const float4 *>(x);
     const int lane = threadIdx.x & 31;
     const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint32_t base = first + blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < n_vorder; base += stride) {
+    auto group = [&](uint32_t base) {  // the 32 vertices vorder[base, base + 32), one per lane
         const uint32_t slot = base + lane;
         const bool valid = slot < n_vorder;
         const uint32_t u = valid ? vorder[slot] : 0u;
@@ -404,7 +461,7 @@ __global__ void __launch_bounds__(THIN_THREADS, 3) k_gnn_thin(const uint32_t *__
         }
 #pragma unroll
         for (int j = 0; j < FEAT; j++) c[j] = relu(c[j]);
-        if (!valid) continue;
+        if (!valid) return;
         if (MODE == MODE_OUTPUT) {
             // t_k = o_k + o_{k+8}, then ((t0+t1)+(t2+t3)) + ((t4+t5)+(t6+t7))  (dense_kernel_output)
             float t[8];
@@ -418,6 +475,24 @@ __global__ void __launch_bounds__(THIN_THREADS, 3) k_gnn_thin(const uint32_t *__
 #pragma unroll
             for (int p = 0; p < 4; p++) Y4[p] = make_float4(c[4 * p], c[4 * p + 1], c[4 * p + 2], c[4 * p + 3]);
         }
+    };
+    // one call site, so the group body is inlined once
+    const uint32_t n_groups = (n_vorder - first + 31) / 32;
+    uint32_t base = first + blockIdx.x * blockDim.x + (threadIdx.x & ~31u), gi = 0, gend = 0;
+    for (;;) {
+        if (work_ctr) {
+            if (gi == gend) {
+                gi = grab_work(work_ctr, GNN_GRAB, lane);
+                if (gi >= n_groups) break;
+                gend = min(gi + GNN_GRAB, n_groups);
+            }
+            base = first + gi * 32;
+            gi++;
+        } else if (base >= n_vorder) {
+            break;
+        }
+        group(base);
+        if (!work_ctr) base += stride;
     }
 }
 
@@ -528,7 +603,7 @@ __global__ void __launch_bounds__(256) k_gnn_hub_gather(const uint32_t *__restri
     }
 }
 
-// Giant hubs (blockIdx.x < n_giant: the leading, largest hubs) read their rows from the staging
+// Giant hubs (hub slots below n_giant: the leading, largest hubs) read their rows from the staging
 // buffer: one bulk copy per stage by the producer's lane 0.  The others gather rows with cp.async.
 template <int MODE>
 __global__ void __launch_bounds__(HUB_THREADS) k_gnn_hub(const uint32_t *__restrict__ V, const uint32_t *__restrict__ E,
@@ -537,31 +612,54 @@ __global__ void __launch_bounds__(HUB_THREADS) k_gnn_hub(const uint32_t *__restr
                                                          float *__restrict__ y, uint32_t *__restrict__ key,
                                                          const float *__restrict__ Wb, DevState *st,
                                                          const float *__restrict__ staged_rows,
-                                                         const uint32_t *__restrict__ giant, uint32_t n_giant) {
+                                                         const uint32_t *__restrict__ giant, uint32_t n_giant,
+                                                         uint32_t n_hubs, uint32_t *hub_ctr, uint32_t reserve) {
     constexpr int ROW = (MODE == MODE_INPUT) ? 2 : FEAT;  // floats per staged row
     extern __shared__ __align__(16) float stage[];         // HUB_STAGES * HUB_ROWS * ROW floats
     __shared__ __align__(16) float sW[LAYER_PARAMS];
     __shared__ __align__(8) uint64_t full[HUB_STAGES], empty[HUB_STAGES];
+    __shared__ uint32_t hub_slot;
     for (int i = threadIdx.x; i < LAYER_PARAMS; i += blockDim.x) sW[i] = Wb[i];
     if (threadIdx.x == 0) {
-        for (int i = 0; i < HUB_STAGES; i++) {
-            // staged: the producer's expect-tx arrival, completed by the bulk copy's bytes;
-            // otherwise one copy-completion arrival per producer lane
-            mbar_init(&full[i], blockIdx.x < n_giant ? 1 : 32);
-            mbar_init(&empty[i], 1);  // the consumer's release
+        // Which hub: blockIdx.x, or with hub_ctr the next giant hub (hub_ctr[0]) on a reserved SM and
+        // the next other hub (hub_ctr[1]) elsewhere, each falling back to the other list; a grid of
+        // n_hubs CTAs takes every hub exactly once wherever its CTAs land.
+        uint32_t h = blockIdx.x;
+        if (hub_ctr) {
+            const bool mine = sm_id() < reserve;
+            h = 0xffffffffu;
+            for (int pass = 0; pass < 2 && h == 0xffffffffu; pass++) {
+                if ((pass == 0) == mine) {
+                    const uint32_t gi = atomicAdd(&hub_ctr[0], 1u);
+                    if (gi < n_giant) h = gi;
+                } else {
+                    const uint32_t oi = atomicAdd(&hub_ctr[1], 1u) + n_giant;
+                    if (oi < n_hubs) h = oi;
+                }
+            }
         }
+        hub_slot = h;
+        if (h != 0xffffffffu)
+            for (int i = 0; i < HUB_STAGES; i++) {
+                // staged: the producer's expect-tx arrival, completed by the bulk copy's bytes;
+                // otherwise one copy-completion arrival per producer lane
+                mbar_init(&full[i], h < n_giant ? 1 : 32);
+                mbar_init(&empty[i], 1);  // the consumer's release
+            }
     }
     __syncthreads();
-    const uint32_t u = hubs[blockIdx.x];
+    const uint32_t hi = hub_slot;
+    if (hi == 0xffffffffu) return;
+    const uint32_t u = hubs[hi];
     const uint32_t beg = V[u], end = V[u + 1], d = end - beg;
     const uint32_t nchunks = (d + HUB_ROWS - 1) / HUB_ROWS;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
-    const bool staged = blockIdx.x < n_giant;
+    const bool staged = hi < n_giant;
     if (warp == 1 && staged) {
         if (lane == 0) {
             constexpr uint32_t ROWB = ROW * sizeof(float);  // 64 bytes (8 in the input layer)
-            const char *src = reinterpret_cast<const char *>(staged_rows) + (size_t)giant[blockIdx.x] * ROWB;
+            const char *src = reinterpret_cast<const char *>(staged_rows) + (size_t)giant[hi] * ROWB;
             for (uint32_t c = 0; c < nchunks; c++) {
                 const uint32_t s = c % HUB_STAGES;
                 if (c >= HUB_STAGES && !mbar_wait(&empty[s], ((c / HUB_STAGES) - 1) & 1u, st)) return;
@@ -702,9 +800,15 @@ __global__ void __launch_bounds__(HUB_THREADS) k_gnn_hub(const uint32_t *__restr
 
 template <int MODE>
 gc_status launch_layer(gc_graph *g, const float *Wb, const float *x, float *y, cudaStream_t side,
-                       cudaEvent_t fork, cudaEvent_t join) {
+                       cudaEvent_t fork, cudaEvent_t join, uint32_t reserve) {
     gc_ctx *ctx = g->ctx;
     gc_status s;
+    // with reserve > 0: SMs 0..reserve-1 are left to the giant-hub CTAs; counters, zeroed here for
+    // each layer, hand out giant hubs, other hubs, bulk items (three) and thin groups
+    uint32_t *ctr = reserve ? g->gnn_ctr : nullptr;
+    if (reserve && (s = gc_check_cuda(ctx, cudaMemsetAsync(ctr, 0, 8 * sizeof(uint32_t), ctx->stream),
+                                      "gnn work counters")) != GC_OK)
+        return s;
     if (g->n_hubs) {
         constexpr int ROW = (MODE == MODE_INPUT) ? 2 : FEAT;
         const size_t smem = (size_t)HUB_STAGES * HUB_ROWS * ROW * sizeof(float);
@@ -727,7 +831,8 @@ gc_status launch_layer(gc_graph *g, const float *Wb, const float *x, float *y, c
             ctx->launches++;
         }
         k_gnn_hub<MODE><<<g->n_hubs, HUB_THREADS, smem, side>>>(g->V, g->E, g->hubs, g->t01, x, y, g->key, Wb,
-                                                                ctx->dstate, g->hub_stage, g->giant, g->n_giant);
+                                                                ctx->dstate, g->hub_stage, g->giant, g->n_giant,
+                                                                g->n_hubs, reserve ? ctr : nullptr, reserve);
         ctx->launches++;
         if ((s = gc_check_launch(ctx, "gnn hub layer")) != GC_OK) return s;
     }
@@ -745,13 +850,15 @@ gc_status launch_layer(gc_graph *g, const float *Wb, const float *x, float *y, c
         const uint32_t first_thin = g->n_vorder - g->n_thin;
         if (first_thin) {
             k_gnn_layer<MODE><<<ctx->num_sms * blocks, GNN_THREADS, 0, ctx->stream>>>(
-                g->V, g->E, g->vorder, g->n_wide_gnn, first_thin, g->t01, x, y, g->key, Wb);
+                g->V, g->E, g->vorder, g->n_wide_gnn, first_thin, g->t01, x, y, g->key, Wb, reserve ? ctr + 2 : nullptr,
+                reserve);
             ctx->launches++;
         }
         if (g->n_thin) {
             const uint32_t grid = std::min<uint32_t>((uint32_t)ctx->num_sms * 3, (g->n_thin + THIN_THREADS - 1) / THIN_THREADS);
             k_gnn_thin<MODE><<<grid, THIN_THREADS, 0, ctx->stream>>>(g->V, g->E, g->vorder, first_thin, g->n_vorder,
-                                                                     g->t01, x, y, g->key, Wb);
+                                                                     g->t01, x, y, g->key, Wb,
+                                                                     reserve ? ctr + 5 : nullptr, reserve);
             ctx->launches++;
         }
     }
@@ -780,6 +887,16 @@ gc_status gc_priority_gnn(gc_graph *g, const gc_model *m) {
         if ((s = gc_alloc(ctx, &g->hub_stage, (size_t)(g->giant_rows + 2) * FEAT, "giant hub rows")) != GC_OK) return s;
         g->hub_stage_rows = g->giant_rows + 2;
     }
+    // SMs left to the giant hubs' CTAs (ctx->gnn_hub_sms: -1 one per giant hub, 0 none, n: SMs
+    // 0..n-1).  Beside the L1-bound bulk CTAs a giant hub's FP32 chain ran about twice as slow as
+    // alone; with its own SM and the bulk handed out by counters, GNN3 + JP on R-MAT 22 took
+    // 7.9-8.1 ms per job instead of 9.1 (B200, 23 giant hubs).
+    uint32_t reserve = 0;
+    if (ctx->gnn_hub_sms != 0 && g->n_giant) {
+        reserve = ctx->gnn_hub_sms > 0 ? (uint32_t)ctx->gnn_hub_sms : g->n_giant;
+        reserve = std::min<uint32_t>(reserve, (uint32_t)ctx->num_sms / 6);
+    }
+    if (reserve && (s = gc_alloc(ctx, &g->gnn_ctr, 8, "gnn work counters")) != GC_OK) return s;
     if (ctx->side_stream == nullptr) {
         int lo = 0, hi = 0;
         cudaDeviceGetStreamPriorityRange(&lo, &hi);
@@ -804,11 +921,11 @@ gc_status gc_priority_gnn(gc_graph *g, const gc_model *m) {
     for (int l = 0; l < L; l++) {
         const float *Wb = m->d_param + (size_t)l * LAYER_PARAMS;
         if (l == 0)
-            s = launch_layer<MODE_INPUT>(g, Wb, nullptr, y, ctx->side_stream, ctx->ev_fork, ctx->ev_join);
+            s = launch_layer<MODE_INPUT>(g, Wb, nullptr, y, ctx->side_stream, ctx->ev_fork, ctx->ev_join, reserve);
         else if (l < L - 1)
-            s = launch_layer<MODE_HIDDEN>(g, Wb, x, y, ctx->side_stream, ctx->ev_fork, ctx->ev_join);
+            s = launch_layer<MODE_HIDDEN>(g, Wb, x, y, ctx->side_stream, ctx->ev_fork, ctx->ev_join, reserve);
         else
-            s = launch_layer<MODE_OUTPUT>(g, Wb, x, nullptr, ctx->side_stream, ctx->ev_fork, ctx->ev_join);
+            s = launch_layer<MODE_OUTPUT>(g, Wb, x, nullptr, ctx->side_stream, ctx->ev_fork, ctx->ev_join, reserve);
         if (s != GC_OK) return s;
         float *t = x;
         x = y;
