@@ -21,7 +21,8 @@
 //   - hubs (more than GC_GNN_HUB_DEGREE): a CTA per hub that streams neighbour rows into shared
 //     memory with cp.async while one thread per feature runs the sequential FP32 chain; the
 //     largest hubs read rows that k_gnn_hub_gather first copies into a contiguous buffer.  Hub
-//     CTAs run on a second stream, so the long chains overlap the bulk of the layer.
+//     CTAs run on a second stream, so the long chains overlap the bulk of the layer, and each
+//     giant hub's CTA gets an SM of its own (the bulk CTAs leave the first SMs to them).
 // Neighbour rows are read with __ldg: a layer never writes the features it reads.  In an A/B on
 // R-MAT 22 (GNN3) the explicit read-only load made the bulk hidden and output layers about 6 %
 // faster than the plain loads the compiler emits here; the step time did not change, since the
@@ -65,8 +66,8 @@ __device__ __forceinline__ uint32_t sm_id() {
     return r;
 }
 
-// Bulk work handed out by an atomic counter, `grab` items per warp at a time (used when some SMs
-// are left to the giant-hub CTAs, so that the CTAs that do start cover all the work).
+// Bulk work handed out by an atomic counter, n items per warp at a time (used when some SMs are
+// left to the giant-hub CTAs, so that the CTAs that do start cover all the work).
 constexpr uint32_t GNN_GRAB = 8;
 constexpr uint32_t GNN_HEAVY = 16384;  // leading four-lane items handed out one at a time
 __device__ __forceinline__ uint32_t grab_work(uint32_t *ctr, uint32_t n, int lane) {
