@@ -286,6 +286,8 @@ gc_status gc_ctx_create(int device, gc_ctx **out) {
     if (const char *e = getenv("GC_JP_NAP")) ctx->jp_nap = (unsigned int)strtoul(e, nullptr, 10);
     if (const char *e = getenv("GC_GNN_WARP_DEGREE")) ctx->gnn_warp_deg = (uint32_t)strtoul(e, nullptr, 10);
     if (const char *e = getenv("GC_GNN_HUB_SMS")) ctx->gnn_hub_sms = atoi(e);
+    if (const char *e = getenv("GC_GNN_GRAB")) ctx->gnn_grab = std::max<uint32_t>(1u, (uint32_t)strtoul(e, nullptr, 10));
+    if (const char *e = getenv("GC_GNN_HEAVY")) ctx->gnn_heavy = (uint32_t)strtoul(e, nullptr, 10);
     if (const char *e = getenv("GC_GNN_GIANT_DEGREE")) ctx->gnn_giant_deg = (uint32_t)strtoul(e, nullptr, 10);
     if (const char *e = getenv("GC_GNN_THIN_DEGREE")) ctx->gnn_thin_deg = (uint32_t)strtoul(e, nullptr, 10);
     if (const char *e = getenv("GC_GNN_SERIAL")) ctx->gnn_serial = atoi(e) != 0;  // 1: hubs first, then the bulk

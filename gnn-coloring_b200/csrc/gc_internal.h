@@ -44,6 +44,8 @@ struct gc_ctx {
     uint32_t gnn_warp_deg = GC_GNN_WIDE_DEGREE;  // GNN: above this many neighbours a vertex gets a warp
     uint32_t gnn_giant_deg = 0;          // GNN: hubs with at least this many neighbours are staged (0: automatic)
     uint32_t gnn_thin_deg = 16;          // GNN: vertices with at most this many neighbours get one lane each
+    uint32_t gnn_grab = 2;               // GNN counter hand-out: items per grab (GC_GNN_GRAB; 1-2 best, 8 +4 %, 16 +17 %)
+    uint32_t gnn_heavy = 16384;          // GNN counter hand-out: leading four-lane items taken singly (GC_GNN_HEAVY)
     int gnn_hub_sms = -1;                // GNN: SMs left to giant-hub CTAs (-1: one per giant hub, 0: none; GC_GNN_HUB_SMS)
     bool gnn_serial = false;             // hub CTAs beside the bulk on a high-priority stream (GC_GNN_SERIAL=1: before it)
     bool hub_smem_set[3] = {false, false, false};  // hub kernels' shared-memory limit raised

@@ -67,9 +67,8 @@ __device__ __forceinline__ uint32_t sm_id() {
 }
 
 // Bulk work handed out by an atomic counter, n items per warp at a time (used when some SMs are
-// left to the giant-hub CTAs, so that the CTAs that do start cover all the work).
-constexpr uint32_t GNN_GRAB = 8;
-constexpr uint32_t GNN_HEAVY = 16384;  // leading four-lane items handed out one at a time
+// left to the giant-hub CTAs, so that the CTAs that do start cover all the work; the sizes are the
+// context's gnn_grab and gnn_heavy).
 __device__ __forceinline__ uint32_t grab_work(uint32_t *ctr, uint32_t n, int lane) {
     uint32_t b = 0;
     if (lane == 0) b = atomicAdd(ctr, n);
@@ -217,7 +216,8 @@ __global__ void __launch_bounds__(GNN_THREADS, 4) k_gnn_layer(const uint32_t *__
                                                               uint32_t n_vorder, const float2 *__restrict__ t01,
                                                               const float *__restrict__ x, float *__restrict__ y,
                                                               uint32_t *__restrict__ key, const float *__restrict__ Wb,
-                                                              uint32_t *work_ctr, uint32_t reserve) {
+                                                              uint32_t *work_ctr, uint32_t reserve, uint32_t grab,
+                                                              uint32_t heavy) {
     // an SM left to the giant-hub CTAs: the whole CTA leaves, except the grid's last CTA, which
     // stays wherever it runs, so the counter's work is done whatever the placement
     if (reserve && sm_id() < reserve && blockIdx.x != gridDim.x - 1) return;
@@ -304,10 +304,10 @@ __global__ void __launch_bounds__(GNN_THREADS, 4) k_gnn_layer(const uint32_t *__
         }
     };
     // Dynamic hand-out (work_ctr): items are sorted heaviest first, so the warp-tier vertices
-    // (work_ctr[0]) and the leading GNN_HEAVY four-lane items (work_ctr[1]) go one at a time and
-    // spread over the warps; the rest go GNN_GRAB at a time (work_ctr[2]).  Otherwise a fixed
+    // (work_ctr[0]) and the leading `heavy` four-lane items (work_ctr[1]) go one at a time and
+    // spread over the warps; the rest go `grab` at a time (work_ctr[2]).  Otherwise a fixed
     // stride.  One call site, so the item body is inlined once.
-    const uint32_t heavy_end = min(n_items, n_wide + GNN_HEAVY);
+    const uint32_t heavy_end = min(n_items, n_wide + heavy);
     uint32_t phase = 0, cur = 0, end = 0, sit = warp;
     for (;;) {
         uint32_t it;
@@ -322,8 +322,8 @@ __global__ void __launch_bounds__(GNN_THREADS, 4) k_gnn_layer(const uint32_t *__
                     if (x < heavy_end) cur = x, end = x + 1;
                     else phase = 2;
                 } else {
-                    const uint32_t x = heavy_end + grab_work(work_ctr + 2, GNN_GRAB, lane);
-                    if (x < n_items) cur = x, end = min(x + GNN_GRAB, n_items);
+                    const uint32_t x = heavy_end + grab_work(work_ctr + 2, grab, lane);
+                    if (x < n_items) cur = x, end = min(x + grab, n_items);
                     else phase = 3;
                 }
             }
@@ -353,7 +353,7 @@ __global__ void __launch_bounds__(THIN_THREADS, 3) k_gnn_thin(const uint32_t *__
                                                               uint32_t n_vorder, const float2 *__restrict__ t01,
                                                               const float *__restrict__ x, float *__restrict__ y,
                                                               uint32_t *__restrict__ key, const float *__restrict__ Wb,
-                                                              uint32_t *work_ctr, uint32_t reserve) {
+                                                              uint32_t *work_ctr, uint32_t reserve, uint32_t grab) {
     // an SM left to the giant-hub CTAs: the whole CTA leaves, except the grid's last CTA, which
     // stays wherever it runs, so the counter's work is done whatever the placement
     if (reserve && sm_id() < reserve && blockIdx.x != gridDim.x - 1) return;
@@ -483,9 +483,9 @@ __global__ void __launch_bounds__(THIN_THREADS, 3) k_gnn_thin(const uint32_t *__
     for (;;) {
         if (work_ctr) {
             if (gi == gend) {
-                gi = grab_work(work_ctr, GNN_GRAB, lane);
+                gi = grab_work(work_ctr, grab, lane);
                 if (gi >= n_groups) break;
-                gend = min(gi + GNN_GRAB, n_groups);
+                gend = min(gi + grab, n_groups);
             }
             base = first + gi * 32;
             gi++;
@@ -852,14 +852,15 @@ gc_status launch_layer(gc_graph *g, const float *Wb, const float *x, float *y, c
         if (first_thin) {
             k_gnn_layer<MODE><<<ctx->num_sms * blocks, GNN_THREADS, 0, ctx->stream>>>(
                 g->V, g->E, g->vorder, g->n_wide_gnn, first_thin, g->t01, x, y, g->key, Wb, reserve ? ctr + 2 : nullptr,
-                reserve);
+                reserve, ctx->gnn_grab, ctx->gnn_heavy);
             ctx->launches++;
         }
         if (g->n_thin) {
             const uint32_t grid = std::min<uint32_t>((uint32_t)ctx->num_sms * 3, (g->n_thin + THIN_THREADS - 1) / THIN_THREADS);
             k_gnn_thin<MODE><<<grid, THIN_THREADS, 0, ctx->stream>>>(g->V, g->E, g->vorder, first_thin, g->n_vorder,
                                                                      g->t01, x, y, g->key, Wb,
-                                                                     reserve ? ctr + 5 : nullptr, reserve);
+                                                                     reserve ? ctr + 5 : nullptr, reserve,
+                                                                     ctx->gnn_grab);
             ctx->launches++;
         }
     }
