@@ -3,18 +3,23 @@
 
 Workload (one "step" = one coloring job): R-MAT scale 22 (4,194,304 vertices), edge factor 16,
 a/b/c/d = 0.57/0.19/0.19/0.05, seed 2, symmetrised, deduplicated, loops removed; GNN3 priorities
-with seeded synthetic GraphSAGE-16 weights (the reference's layout and value range), then JP.
-Metric: colored edges/s = |E| (directed CSR length, the reference's |E|) / job time.
+with the reference's own trained weights (models/m3.gnn, copied beside the compiled reference by
+oracle/Makefile; seeded synthetic weights of the same layout only where that file is absent), then
+JP.  Metric: colored edges/s = |E| (directed CSR length, the reference's |E|) / job time.
 
   value   device-resident: CSR on the GPU, CUDA events on the library's stream around K steps
           of gc_priority(GNN3) + gc_color; E (513 MB) is larger than L2, so no flush is needed.
+          Per-graph preparation (once per upload) is reported beside it as prep_ms.
   e2e     the reference-facing call with host buffers: gnn_internal_par(N, V, E, ad, jp, p, color)
           from pinned memory, H2D of V/E and D2H of p/colors inside every timed step.
   roofline  the dominant kernel's algorithmic bytes per launch / its average event-timed
           duration, against MEASURED_PEAKS.json's HBM copy bandwidth.
-  cpu_baseline  the reference's own OpenMP code (oracle/_ref) on the host cores, same job.
+  cpu_baseline  the reference's own OpenMP code (oracle/_ref) on the host cores, same job; its
+          p and colors are the parity check of the GPU result (`parity`), and the other
+          workloads (`configs`) are checked the same way, Culberson round by round.
 
---impl reference runs the reference's own CPU implementation of the same job (rank 0 only).
+--impl reference runs the reference's own CPU implementation of the same job (rank 0 only), in a
+process that never loads libgnncolor.so.
 --gpus N > 1 runs N independent replicas, one per GPU (the path does not shard): weak scaling.
 """
 from __future__ import annotations
@@ -39,23 +44,88 @@ for p in (ROOT, PKG):
 
 METRIC = "GNN3+JP colored edges/s"
 UNIT = "edges/s"
-MODEL_SEED = 1003  # synthetic GNN3 weights (same seed as the golden vectors)
+MODEL_SEED = 1003  # synthetic GNN3 weights (seed 1000 + layers), only where the reference's model files are absent
+REF_MODELS = os.path.join(ROOT, "oracle", "_ref", "models")
+GRAPHS = {
+    "rmat22": ("R-MAT scale 22, ef 16, a/b/c=0.57/0.19/0.19, seed 2", 22),
+    "rmat18": ("R-MAT scale 18, ef 16, a/b/c=0.57/0.19/0.19, seed 2", 18),
+    "er65k": ("Erdos-Renyi n=65536, m=524288, seed 1", None),
+}
+
+
+def model_file(layers: int):
+    """The reference's own trained weights, models/m{L}.gnn (copied beside the compiled reference by
+    oracle/Makefile), or None where they are absent."""
+    path = os.path.join(REF_MODELS, f"m{layers}.gnn")
+    return path if os.path.exists(path) else None
+
+
+def model_desc(layers: int) -> str:
+    if model_file(layers):
+        return f"models/m{layers}.gnn (the reference's GNN{layers} weights)"
+    return f"synthetic GraphSAGE-16 weights ({layers} layers, seed {1000 + layers}, md 100)"
+
+
+def bench_config(workload_name: str, N: int, M: int) -> dict:
+    """The `config` dict, identical in both arms."""
+    return {"workload": f"{workload_name}_gnn3_jp", "graph": GRAPHS[workload_name][0], "N": N, "M": M,
+            "heuristic": "GNN3", "model": model_desc(3),
+            "l2": "inputs larger than L2 (E is %.0f MB); no flush" % (4 * M / 1e6)}
 
 
 def workload(name: str):
     import gnn_coloring as gcn
-    if name == "rmat22":
-        N, V, E = gcn.gen_rmat(1 << 22, 16, 2)
-        desc = "R-MAT scale 22, ef 16, a/b/c=0.57/0.19/0.19, seed 2"
-    elif name == "rmat18":
-        N, V, E = gcn.gen_rmat(1 << 18, 16, 2)
-        desc = "R-MAT scale 18, ef 16, a/b/c=0.57/0.19/0.19, seed 2"
-    elif name == "er65k":
-        N, V, E = gcn.gen_er(65536, 524288, 1)
-        desc = "Erdos-Renyi n=65536, m=524288, seed 1"
+    desc, scale = GRAPHS[name]
+    if scale is not None:
+        N, V, E = gcn.gen_rmat(1 << scale, 16, 2)
     else:
-        raise SystemExit(f"unknown workload {name}")
+        N, V, E = gcn.gen_er(65536, 524288, 1)
     return desc, N, V, E
+
+
+def workload_reference(name: str):
+    """The same graph without loading the library: the library's R-MAT samples restated in numpy
+    (synthgen), turned into a CSR by the reference's own mtx_to_graph_par, graph_sort_edges_par and
+    graph_make_simple."""
+    import synthgen
+    from oracle import reference as R
+    desc, scale = GRAPHS[name]
+    I, J = synthgen.rmat_samples(1 << scale, 16, 2)
+    V, E = R.csr_from_samples(1 << scale, I, J)
+    return desc, 1 << scale, V, E
+
+
+def cpu_info() -> dict:
+    model = None
+    try:
+        with open("/proc/cpuinfo") as f:
+            for ln in f:
+                if ln.startswith("model name"):
+                    model = ln.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    try:
+        nproc = len(os.sched_getaffinity(0))
+    except AttributeError:
+        nproc = os.cpu_count() or 1
+    return {"cpu_model": model, "nproc": nproc}
+
+
+def source_hash() -> str:
+    """SHA-256 over the library's kernel and host sources and build flags: the ncu traffic figures
+    are used only when they were captured on a build of these exact sources."""
+    import hashlib
+    h = hashlib.sha256()
+    files = []
+    for d in (os.path.join(PKG, "csrc"), os.path.join(ROOT, "include")):
+        files += [os.path.join(d, f) for f in os.listdir(d)]
+    files.append(os.path.join(PKG, "Makefile"))
+    for path in sorted(files, key=lambda x: os.path.relpath(x, ROOT)):
+        h.update(os.path.relpath(path, ROOT).encode())
+        with open(path, "rb") as f:
+            h.update(f.read())
+    return h.hexdigest()
 
 
 # Algorithmic (compulsory) HBM bytes per launch of each kernel group, M = directed edges,
@@ -169,104 +239,123 @@ def barrier(world: int):
 
 # ---- the reference's CPU implementation -------------------------------------------------------
 
-def reference_job_runner(N, V, E, params, md):
-    """Sets up the reference's own gnn_setup / jones_plassmann_setup (models/m3.gnn written to a
-    scratch directory, as src/gnn.c:24-25 reads it from the working directory) and returns a
-    callable running its f_par, gnn_internal_par (src/gnn.c:78-83), once."""
-    import gnn_coloring as gcn
-    from oracle import reference as R
-    L = R.lib()
-    L.gnn_setup.argtypes = [C.c_uint32, C.c_uint32]
-    L.gnn_setup.restype = C.c_void_p
-    L.gnn_internal_par.argtypes = [C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
-    L.gnn_cleanup.argtypes = [C.c_void_p]
-    work = tempfile.mkdtemp(prefix="gnnref_")
-    os.makedirs(os.path.join(work, "models"), exist_ok=True)
-    gcn.model_write(os.path.join(work, "models", "m3.gnn"), params, md)
-    C.c_int.in_dll(L, "layers").value = 3
-    cwd = os.getcwd()
-    os.chdir(work)
-    try:
-        ad = L.gnn_setup(N, int(V[N]))
-    finally:
-        os.chdir(cwd)
-    jp = L.jones_plassmann_setup(N, int(V[N]))
-    Vc = np.ascontiguousarray(V, np.uint32)
-    Ec = np.ascontiguousarray(E, np.uint32)
-    p = R.aligned(N + 8, np.float64)
-    color = np.zeros(N, np.int32)
-
-    def run():
-        L.gnn_internal_par(N, Vc.ctypes.data, Ec.ctypes.data, ad, jp, p.ctypes.data, color.ctypes.data)
-        return color
-
-    return run
-
-
 def run_reference(args):
-    world, rank, local = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
+    """The reference's own gnn_internal_par (src/gnn.c:78-83) with its own models/m3.gnn, on all
+    host cores.  This process never loads libgnncolor.so: the graph comes from synthgen and the
+    reference's CSR construction."""
+    rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    import gnn_coloring as gcn
     from oracle import reference as R
-    desc, N, V, E = workload(args.workload)
-    M = int(V[N])
-    params, md = gcn.synthetic_model(3, MODEL_SEED)
-    if not R.available():
-        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libref.so was not built (reference "
-                                                                "sources absent where build() ran)"}))
+    if not (R.available() and R.has_models()):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libref.so and the reference's models were "
+                                                              "not built (reference sources absent where build() ran)"}))
         return
-    cores = os.cpu_count() or 1
+    if GRAPHS[args.workload][1] is None:
+        print(json.dumps({"impl": "reference", "unavailable": f"--impl reference generates R-MAT workloads only "
+                                                              f"(asked: {args.workload})"}))
+        return
+    t0 = time.perf_counter()
+    desc, N, V, E = workload_reference(args.workload)
+    gen_s = time.perf_counter() - t0
+    M = int(V[N])
+    info = cpu_info()
+    cores = info["nproc"]
     R.set_threads(cores)
-    run = reference_job_runner(N, V, E, params, md)
+    job = R.GnnJob(N, V, E, 3)
     for _ in range(args.warmup):
-        run()
+        job.run()
     times = []
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        run()
+        job.run()
         times.append(time.perf_counter() - t0)
+    colors = int(job.color[:N].max()) if N else 0
+    job.close()
     total = sum(times)
     value = M * len(times) / total
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * total / len(times), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
-        "config": {"workload": f"{args.workload}_gnn3_jp", "graph": desc, "N": N, "M": M,
-                   "heuristic": "GNN3", "threads": cores},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
+        "config": bench_config(args.workload, N, M), "colors": colors, "graph_generation_s": gen_s,
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference", **info,
                          "sample": f"{args.steps} full GNN3+JP jobs through the reference's gnn_internal_par "
-                                   f"(src/gnn.c:78-83), OpenMP over {cores} threads"},
+                                   f"(src/gnn.c:78-83) with its models/m3.gnn, OpenMP over {cores} threads"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
 
 
-def cpu_baseline(N, V, E, params, md, budget_s: float = 20.0):
+def cpu_baseline(N, V, E, budget_s: float = 20.0):
+    """The reference's gnn_internal_par on the same graph, timed on all host cores; also returns its
+    last p and colors, which the GPU result is checked against."""
     from oracle import reference as R
-    cores = os.cpu_count() or 1
-    if R.available():
-        R.set_threads(cores)
-        run = reference_job_runner(N, V, E, params, md)
-        run()  # warm-up
-        times = []
-        t_start = time.perf_counter()
-        while len(times) < 3 and time.perf_counter() - t_start < budget_s:
-            t0 = time.perf_counter()
-            run()
-            times.append(time.perf_counter() - t0)
-        return {"value": int(V[N]) * len(times) / sum(times), "unit": UNIT, "cores": cores, "kind": "reference",
-                "sample": f"{len(times)} full GNN3+JP jobs on the same graph (reference gnn_internal_par, "
-                          f"{cores} OpenMP threads), best-effort within {budget_s:.0f} s"}
-    # port: the scalar restatement on one core, on a smaller graph of the same family
+    info = cpu_info()
+    cores = info["nproc"]
+    if not (R.available() and R.has_models()):
+        return {"value": None, "unit": UNIT, "cores": cores, "kind": "reference", **info,
+                "sample": "unavailable: oracle/_ref was not built"}, None, None
+    R.set_threads(cores)
+    job = R.GnnJob(N, V, E, 3)
+    job.run()  # warm-up
+    times = []
+    t_start = time.perf_counter()
+    while len(times) < 3 and time.perf_counter() - t_start < budget_s:
+        t0 = time.perf_counter()
+        job.run()
+        times.append(time.perf_counter() - t0)
+    p, c = job.p[:N].copy(), job.color[:N].copy()
+    job.close()
+    return ({"value": int(V[N]) * len(times) / sum(times), "unit": UNIT, "cores": cores, "kind": "reference", **info,
+             "sample": f"{len(times)} full GNN3+JP jobs on the same graph (reference gnn_internal_par with its "
+                       f"models/m3.gnn, {cores} OpenMP threads), best-effort within {budget_s:.0f} s"}, p, c)
+
+
+def parity_entry(p_gpu, c_gpu, p_ref, c_ref, what: str) -> dict:
+    if p_ref is None:
+        return {"checked": False, "why": "reference not built"}
+    return {"checked": True, "against": what,
+            "p_bits_equal": bool(np.array_equal(np.asarray(p_gpu, np.float64).view(np.uint64),
+                                                np.asarray(p_ref, np.float64).view(np.uint64))),
+            "colors_equal": bool(np.array_equal(c_gpu, c_ref)), "colors": int(c_gpu.max()) if len(c_gpu) else 0,
+            "colors_reference": int(c_ref.max()) if len(c_ref) else 0}
+
+
+def prep_time_ms(ctx, N, V, E, reps: int = 3) -> float:
+    """Per-graph preparation (CSR check, degree classes, hub lists, degree-sorted schedule, split
+    tasks) of a device-resident CSR: gc_graph_wrap_device on a device copy of V and E, which runs
+    exactly that preparation.  Median wall time of `reps` calls; not part of `value`."""
+    import torch
     import gnn_coloring as gcn
-    from oracle import restatement as O
-    n2, V2, E2 = gcn.gen_rmat(1 << 18, 16, 2)
-    t0 = time.perf_counter()
-    p = O.ordering("GNN", n2, V2, E2, params, md)
-    O.greedy_color(n2, V2, E2, p)
-    dt = time.perf_counter() - t0
-    return {"value": int(V2[n2]) / dt, "unit": UNIT, "cores": 1, "kind": "port",
-            "sample": "1 GNN3+JP job on R-MAT scale 18 (same generator) with the scalar oracle"}
+    dV = torch.from_numpy(np.ascontiguousarray(V).view(np.int32)).cuda()
+    dE = torch.from_numpy(np.ascontiguousarray(E).view(np.int32)).cuda()
+    torch.cuda.synchronize()
+    ts = []
+    for _ in range(reps):
+        h = C.c_void_p()
+        t0 = time.perf_counter()
+        ctx.check(gcn.lib.gc_graph_wrap_device(ctx.h, N, int(V[N]), dV.data_ptr(), dE.data_ptr(), C.byref(h)),
+                  "wrap device graph")
+        ctx.sync()
+        ts.append(1e3 * (time.perf_counter() - t0))
+        gcn.lib.gc_graph_free(h)
+    del dV, dE
+    return float(statistics.median(ts))
+
+
+def ncu_traffic(workload_name: str, kernel: str):
+    """DRAM bytes per launch of `kernel` from profiles/ncu_traffic.json, when that file was captured
+    on a build of the current sources; None otherwise."""
+    tpath = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    try:
+        with open(tpath) as f:
+            d = json.load(f)
+    except Exception:
+        return None, "no capture"
+    if d.get("source_sha256") != source_hash():
+        return None, "capture is of other sources"
+    v = d.get(workload_name, {}).get(kernel)
+    return (v["dram_bytes_per_launch"] if isinstance(v, dict) else v), "ncu capture of this build"
 
 
 # ---- our arm -------------------------------------------------------------------------------------
@@ -279,10 +368,9 @@ def run_ours(args):
     torch.cuda.set_device(device)
     desc, N, V, E = workload(args.workload)
     M = int(V[N])
-    params, md = gcn.synthetic_model(3, MODEL_SEED)
 
     ctx = gcn.Context(device)
-    model = gcn.Model(ctx, params, md)
+    model = _model(ctx, gcn, 3)
     g = gcn.Graph(ctx, N, V, E)
     stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", device))
 
@@ -294,6 +382,7 @@ def run_ours(args):
         step()
     colors_used = g.validate()
     assert colors_used > 0, "invalid coloring"
+    p_gpu, c_gpu = g.priorities(), g.colors()
 
     sampler = ClockSampler(device)
     sampler.start()
@@ -316,6 +405,7 @@ def run_ours(args):
     elapsed_ms = max_over_ranks(elapsed_ms, world, torch.device("cuda", device))
     ms_per_step = elapsed_ms / args.steps
     value = world * M * args.steps / (elapsed_ms / 1e3)
+    same_after = bool(np.array_equal(g.colors(), c_gpu))
 
     # per-kernel durations: event pairs on each kernel's own stream over a few more steps
     gcn.lib.gc_prof_enable(ctx.h, 1)
@@ -338,53 +428,98 @@ def run_ours(args):
         per_launch_ms = kernels[dominant]["ms_per_step"] / max(kernels[dominant]["launches_per_step"], 1)
         alg = algorithmic_bytes(dominant, N, M, P)
         achieved = alg / (per_launch_ms / 1e3) / 1e9
-        traffic = None
-        tpath = os.path.join(ROOT, "profiles", "ncu_traffic.json")
-        if os.path.exists(tpath):
-            try:
-                with open(tpath) as f:
-                    traffic = json.load(f).get(args.workload, {}).get(dominant)
-            except Exception:
-                traffic = None
+        traffic, traffic_src = ncu_traffic(args.workload, dominant)
         roofline = {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                     "frac": achieved / hbm_peak, "peak_kind": f"{peak_kind} (copy bandwidth)",
-                    "algorithmic_bytes_per_launch": alg, "ms_per_launch": per_launch_ms, "traffic": traffic}
+                    "algorithmic_bytes_per_launch": alg, "ms_per_launch": per_launch_ms, "traffic": traffic,
+                    "traffic_source": traffic_src}
     job_bytes = step_bytes(N, M)
     step_roof = {"algorithmic_bytes": job_bytes, "achieved_gbs": job_bytes / (ms_per_step / 1e3) / 1e9,
                  "frac": job_bytes / (ms_per_step / 1e3) / 1e9 / hbm_peak}
+    prep_ms = prep_time_ms(ctx, N, V, E) if world == 1 else None
 
     # e2e through the reference-facing entry point with host buffers
     e2e = None
     if not args.no_e2e:
-        e2e = run_e2e(args, N, V, E, params, md, torch)
+        e2e = run_e2e(args, N, V, E, torch)
 
     result = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": max(3, args.warmup), "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
-        "config": {"workload": f"{args.workload}_gnn3_jp", "graph": desc, "N": N, "M": M, "heuristic": "GNN3",
-                   "model": f"synthetic GraphSAGE-16 weights (3 layers, seed {MODEL_SEED}, md 100)",
-                   "l2": "inputs larger than L2 (E is %.0f MB); no flush" % (4 * M / 1e6),
-                   "parallelism": "replicas" if world > 1 else "single GPU", "colors": colors_used},
+        "vs_baseline": None, "dtype": "fp32", "data": "synthetic", "config": bench_config(args.workload, N, M),
+        "parallelism": "replicas" if world > 1 else "single GPU", "colors": colors_used,
+        "prep_ms": prep_ms,
+        "prep_note": "per-graph preparation of a resident CSR (degree classes, hub lists, degree order, split "
+                     "tasks); once per upload, outside `value`, inside `e2e`",
         "gpu_launches": launches, "clocks": clocks, "roofline": roofline, "step_roofline": step_roof,
         "kernels": kernels, "e2e": e2e,
     }
+    parity = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        result["cpu_baseline"] = cpu_baseline(N, V, E, params, md)
+        base, p_ref, c_ref = cpu_baseline(N, V, E)
+        result["cpu_baseline"] = base
+        parity = parity_entry(p_gpu, c_gpu, p_ref, c_ref, "reference gnn_internal_par (oracle/_ref), same graph "
+                                                           "and model")
+        parity["colors_same_after_timed_steps"] = same_after
+        result["parity"] = parity
     if world == 1 and not args.no_configs:
         result["configs"] = run_configs(args, device)
     if world == 1 and not args.no_batch:
         result["batched"] = run_batched(args, device)
     if world == 1 and not args.no_serve:
         result["serving"] = run_serving(args, device)
+    result["summary"] = summary_of(result)
     if rank == 0:
         print(json.dumps(result))
+        print(json.dumps(result["summary"]), file=sys.stderr)
     g.close()
     model.close()
     ctx.close()
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+    bad = [k for k, v in parity_flags(result) if not v]
+    if bad:
+        raise SystemExit(f"parity failed: {bad}")
+
+
+def parity_flags(result):
+    """(name, ok) for every parity check the run made."""
+    out = []
+    par = result.get("parity")
+    if par and par.get("checked"):
+        out.append(("headline", par["p_bits_equal"] and par["colors_equal"] and par["colors_same_after_timed_steps"]))
+    for name, cfg in (result.get("configs") or {}).items():
+        par = cfg.get("parity") if isinstance(cfg, dict) else None
+        if par and par.get("checked"):
+            out.append((name, bool(par.get("all_equal"))))
+    for name, r in ((result.get("batched") or {}).get("heuristics") or {}).items():
+        out.append((f"batched_{name}", bool(r.get("colors_identical"))))
+    srv = result.get("serving")
+    if srv:
+        out.append(("serving", bool(srv.get("color_counts_identical_to_alone"))))
+    return out
+
+
+def summary_of(result) -> dict:
+    """A short digest placed last in the JSON line (and on stderr), so that a truncated tail of the
+    output still shows the headline, e2e, the batched and served speed-ups and the parity checks."""
+    s = {"value": result["value"], "ms_per_step": result["ms_per_step"],
+         "e2e": (result.get("e2e") or {}).get("value"), "prep_ms": result.get("prep_ms"),
+         "roofline_frac": (result.get("roofline") or {}).get("frac"),
+         "step_roofline_frac": result["step_roofline"]["frac"],
+         "cpu_baseline": (result.get("cpu_baseline") or {}).get("value")}
+    b = result.get("batched")
+    if b:
+        s["batched"] = {k: {"speedup": round(v.get("speedup", 0), 2), "colors_identical": v.get("colors_identical")}
+                        for k, v in b["heuristics"].items()}
+    srv = result.get("serving")
+    if srv:
+        s["served"] = {f: {"speedup_edges_per_s": round(srv[f]["speedup_edges_per_s"], 2),
+                           "speedup_jobs_per_s": round(srv[f]["speedup_jobs_per_s"], 2)}
+                       for f in ("host_csr", "resident_csr") if f in srv}
+    s["parity"] = {k: v for k, v in parity_flags(result)}
+    return s
 
 
 # ---- the other configurations: ER 65k with every heuristic, mesh-like graphs with Culberson ------
@@ -406,24 +541,62 @@ def _timed_jobs(ctx, g, heur, model, recolor, reps, torch, device):
     return e0.elapsed_time(e1) / reps, colors
 
 
+def _model(ctx, gcn, L: int):
+    """The GNN{L} model: the reference's own file where present, else seeded synthetic weights."""
+    path = model_file(L)
+    return gcn.Model.load(ctx, path) if path else gcn.Model(ctx, *gcn.synthetic_model(L, 1000 + L))
+
+
+def _models(ctx, gcn):
+    return {L: _model(ctx, gcn, L) for L in (2, 3, 4)}
+
+
+def _reference_result(name, N, V, E):
+    """The reference's p and colors for one heuristic (None where the reference was not built)."""
+    from oracle import reference as R
+    if not (R.available() and R.has_models()):
+        return None, None
+    R.set_threads(cpu_info()["nproc"])
+    if name.startswith("GNN"):
+        job = R.GnnJob(N, V, E, int(name[3:]))
+        c = job.run()[:N].copy()
+        p = job.p[:N].copy()
+        job.close()
+        return p, c
+    if name in ("SL", "SLL"):
+        return R.peel_par(name, N, V, E)
+    p = R.ordering(name, N, V, E)
+    return p, R.jp_color(N, V, E, p)
+
+
 def run_configs(args, device):
+    """The other workloads on the device-resident path, each checked against the reference's own
+    code on the same graph and weights: Erdos-Renyi n = 65,536 with every heuristic, and the mesh
+    graphs with GNN4 + JP + 9 Culberson rounds (the reference's -c 10), compared round by round."""
     import math
     import torch
     import gnn_coloring as gcn
+    from oracle import reference as R
     ctx = gcn.Context(device)
-    models = {L: gcn.Model(ctx, *gcn.synthetic_model(L, 1000 + L)) for L in (2, 3, 4)}
+    models = _models(ctx, gcn)
     out = {}
     # Erdos-Renyi n = 65,536, m = 524,288, seed 1: every heuristic, one coloring
     N, V, E = gcn.gen_er(65536, 524288, 1)
     g = gcn.Graph(ctx, N, V, E)
-    rows = {}
+    rows, all_eq = {}, True
     for name in ("FF", "LF", "LLF", "SL", "SLL", "GNN2", "GNN3", "GNN4"):
         heur, m = ("GNN", models[int(name[3])]) if name.startswith("GNN") else (name, None)
         ms, colors = _timed_jobs(ctx, g, heur, m, 0, 10, torch, device)
-        rows[name] = {"ms": ms, "colors": colors, "edges_per_s": len(E) / (ms / 1e3)}
+        g.priority(heur, m)
+        g.color()
+        p_ref, c_ref = _reference_result(name, N, V, E)
+        par = parity_entry(g.priorities(), g.colors(), p_ref, c_ref, "reference (oracle/_ref)")
+        all_eq = all_eq and (not par["checked"] or (par["p_bits_equal"] and par["colors_equal"]))
+        rows[name] = {"ms": ms, "colors": colors, "edges_per_s": len(E) / (ms / 1e3), "parity": par}
     g.close()
     out["er65k_all_heuristics"] = {"graph": "Erdos-Renyi n=65536, m=524288, seed 1", "N": N, "M": len(E),
-                                   "heuristics": rows}
+                                   "models": {L: model_desc(L) for L in (2, 3, 4)}, "heuristics": rows,
+                                   "parity": {"checked": R.available() and R.has_models(), "all_equal": all_eq}}
     # mesh-like graphs, GNN4 priorities + JP + 9 Culberson rounds (the reference's -c 10)
     n = 1 << 23
     for key, desc, gen in (
@@ -435,9 +608,35 @@ def run_configs(args, device):
         ms, colors = _timed_jobs(ctx, g, "GNN", models[4], 9, 3, torch, device)
         g.priority("GNN", models[4])
         first = g.color(0)
+        p_gpu = g.priorities()
+        rounds = [g.colors()]
+        for _ in range(9):
+            g.recolor(1)
+            rounds.append(g.colors())
         g.close()
-        out[key] = {"graph": desc, "N": N, "M": len(E), "ms_per_job": ms, "edges_per_s": len(E) / (ms / 1e3),
-                    "colors_first": first, "colors_after_9_culberson": colors}
+        entry = {"graph": desc, "N": N, "M": len(E), "model": model_desc(4), "ms_per_job": ms,
+                 "edges_per_s": len(E) / (ms / 1e3), "colors_first": first, "colors_after_9_culberson": colors}
+        if R.available() and R.has_models():
+            R.set_threads(cpu_info()["nproc"])
+            t0 = time.perf_counter()
+            job = R.GnnJob(N, V, E, 4)
+            ref_rounds = [job.run()[:N].copy()]
+            p_ref = job.p[:N].copy()
+            for _ in range(9):
+                ref_rounds.append(job.culberson()[:N].copy())
+            job.close()
+            ref_s = time.perf_counter() - t0
+            eq = [bool(np.array_equal(a, b)) for a, b in zip(rounds, ref_rounds)]
+            p_eq = bool(np.array_equal(p_gpu.view(np.uint64), p_ref.view(np.uint64)))
+            entry["parity"] = {"checked": True, "against": "reference gnn_internal_par + 9 x (p := color, "
+                                                            "jones_plassmann_internal), oracle/_ref",
+                               "p_bits_equal": p_eq, "colors_equal_per_round": eq,
+                               "colors_per_round": [int(c.max()) for c in rounds],
+                               "colors_per_round_reference": [int(c.max()) for c in ref_rounds],
+                               "all_equal": p_eq and all(eq), "reference_s_incl_setup": ref_s}
+        else:
+            entry["parity"] = {"checked": False, "why": "reference not built"}
+        out[key] = entry
         del V, E
     for m in models.values():
         m.close()
@@ -460,12 +659,11 @@ def run_batched(args, device):
     gen_s = time.perf_counter() - t0
     N, M = int(voff[G]), int(V[int(voff[G])])
     ctx = gcn.Context(device)
-    params2, md2 = gcn.synthetic_model(2, MODEL_SEED)
-    model = gcn.Model(ctx, params2, md2)
+    model = _model(ctx, gcn, 2)
     heurs = [("GNN2", "GNN", model), ("LF", "LF", None)]
     out = {"workload": f"{G} mixed graphs: n log-uniform [1000, 200000]; even seeds Erdos-Renyi avg degree "
                        f"U[8,32], odd seeds R-MAT ef 8; seeds 1000..{999 + G}",
-           "G": G, "N": N, "M": M, "host_generation_s": gen_s, "heuristics": {}}
+           "G": G, "N": N, "M": M, "model": model_desc(2), "host_generation_s": gen_s, "heuristics": {}}
     b = gcn.Batch(ctx, voff, V, E)
     batch_colors = {}
     for name, h, m in heurs:
@@ -593,7 +791,7 @@ def run_serving(args, device):
     t0 = time.perf_counter()
     pool = serving_pool()
     gen_s = time.perf_counter() - t0
-    params3, md3 = gcn.synthetic_model(3, MODEL_SEED)
+    params3, md3 = gcn.model_read(model_file(3)) if model_file(3) else gcn.synthetic_model(3, MODEL_SEED)
     J = args.serve_jobs
     base_jobs = serving_jobs(pool, J, 99)
     ctx = gcn.Context(device)
@@ -655,12 +853,15 @@ def run_serving(args, device):
             "color_counts_identical_to_alone": same1 and same2}
 
 
-def run_e2e(args, N, V, E, params, md, torch):
+def run_e2e(args, N, V, E, torch):
     import gnn_coloring as gcn
     M = int(V[N])
-    work = tempfile.mkdtemp(prefix="gnne2e_")
-    gcn.model_write(os.path.join(work, "m3.gnn"), params, md)
-    os.environ["GC_MODEL_DIR"] = work
+    if model_file(3):
+        os.environ["GC_MODEL_DIR"] = REF_MODELS
+    else:
+        work = tempfile.mkdtemp(prefix="gnne2e_")
+        gcn.model_write(os.path.join(work, "m3.gnn"), *gcn.synthetic_model(3, MODEL_SEED))
+        os.environ["GC_MODEL_DIR"] = work
     os.environ["GC_DEVICE"] = str(torch.cuda.current_device())
     lib = gcn.lib
     C.c_int.in_dll(lib, "layers").value = 3

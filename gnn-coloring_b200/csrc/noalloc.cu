@@ -18,7 +18,13 @@
 //     element it reads before reading it, so nothing has to start at zero; but two calls whose
 //     kernels overlap on a device (different streams, or different host threads) race on it.
 //   - the first call on a device looks up the array's device address (cudaGetSymbolAddress) with
-//     that device current; make that first call before any stream capture.
+//     that device current, and loads every kernel of this entry point (cudaFuncGetAttributes on
+//     each), so that under CUDA's lazy module loading a later call -- say a 3-layer model after a
+//     2-layer one -- loads no code and allocates nothing; make that first call before any stream
+//     capture.
+//   - each kernel launch is checked through the status cudaLaunchKernelEx returns for that launch:
+//     an error left pending by the caller's earlier work is neither reported as this call's nor
+//     cleared.
 #include <mutex>
 
 #include "gc_device.cuh"
@@ -35,6 +41,7 @@ static __device__ __align__(256) float g_noalloc_scratch[SCRATCH_FLOATS];
 constexpr int MAX_DEVICES = 64;
 std::mutex g_setup_mu;
 float *g_scratch_addr[MAX_DEVICES] = {};
+int g_sms[MAX_DEVICES] = {};
 
 enum : int { NA_INPUT = 0, NA_HIDDEN = 1, NA_OUTPUT = 2 };
 
@@ -113,21 +120,45 @@ __global__ void __launch_bounds__(256) k_na_layer(const uint32_t *__restrict__ V
     }
 }
 
-// Device address of the scratch array for the current device, looked up once per device.
-gc_status scratch_for_current_device(float **out, int *dev_out) {
+// Device address of the scratch array for the current device, looked up once per device; the same
+// first call loads this entry point's kernels and reads the SM count.
+gc_status scratch_for_current_device(float **out, int *sms_out) {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= MAX_DEVICES) return GC_ERR_CUDA;
-    *dev_out = dev;
     std::lock_guard<std::mutex> lk(g_setup_mu);
     if (!g_scratch_addr[dev]) {
         void *ptr = nullptr;
-        if (cudaGetSymbolAddress(&ptr, g_noalloc_scratch) != cudaSuccess || !ptr) {
-            cudaGetLastError();
+        cudaFuncAttributes fa;
+        int sms = 0;
+        bool ok = cudaGetSymbolAddress(&ptr, g_noalloc_scratch) == cudaSuccess && ptr;
+        ok = ok && cudaFuncGetAttributes(&fa, k_na_table0) == cudaSuccess;
+        ok = ok && cudaFuncGetAttributes(&fa, k_na_layer<NA_INPUT>) == cudaSuccess;
+        ok = ok && cudaFuncGetAttributes(&fa, k_na_layer<NA_HIDDEN>) == cudaSuccess;
+        ok = ok && cudaFuncGetAttributes(&fa, k_na_layer<NA_OUTPUT>) == cudaSuccess;
+        ok = ok && cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && sms > 0;
+        if (!ok) {
+            cudaGetLastError();  // the failed set-up call's own error
             return GC_ERR_CUDA;
         }
+        g_sms[dev] = sms;
         g_scratch_addr[dev] = static_cast<float *>(ptr);
     }
     *out = g_scratch_addr[dev];
+    *sms_out = g_sms[dev];
+    return GC_OK;
+}
+
+// One launch, checked by the status of that launch alone.
+template <typename... KArgs, typename... Args>
+gc_status launch(void (*kernel)(KArgs...), int grid, cudaStream_t st, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(256);
+    cfg.stream = st;
+    if (cudaLaunchKernelEx(&cfg, kernel, args...) != cudaSuccess) {
+        cudaGetLastError();  // this launch's error, not the caller's
+        return GC_ERR_CUDA;
+    }
     return GC_OK;
 }
 
@@ -140,26 +171,28 @@ extern "C" gc_status gc_gnn_priority_noalloc(uint32_t N, const uint32_t *dV, con
     if (N == 0) return GC_OK;
     if (!dV || !dE || !dp) return GC_ERR_INVALID;
     float *scratch = nullptr;
-    int dev = 0;
-    gc_status s = scratch_for_current_device(&scratch, &dev);
+    int sms = 0;
+    gc_status s = scratch_for_current_device(&scratch, &sms);
     if (s != GC_OK) return s;
     float *xa = scratch, *ya = scratch + (size_t)MAX_V * FEAT;
     float2 *t01 = reinterpret_cast<float2 *>(scratch + 2 * (size_t)MAX_V * FEAT);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const int L = params / LAYER_PARAMS;
-    int sms = 0;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int grid = (sms > 0 ? sms : 1) * 8;
-    k_na_table0<<<grid, 256, 0, st>>>(dV, N, (float)md, t01);
+    const int grid = sms * 8;
+    if ((s = launch(k_na_table0, grid, st, dV, N, (float)md, t01)) != GC_OK) return s;
     float *x = xa, *y = ya;
-    for (int l = 0; l < L; l++) {
+    const float2 *t = t01;
+    const float *none_in = nullptr;
+    float *none_out = nullptr;
+    for (int l = 0; l < L && s == GC_OK; l++) {
         const float *Wb = dparam + (size_t)l * LAYER_PARAMS;
-        if (l == 0) k_na_layer<NA_INPUT><<<grid, 256, 0, st>>>(dV, dE, N, t01, nullptr, y, nullptr, Wb);
-        else if (l < L - 1) k_na_layer<NA_HIDDEN><<<grid, 256, 0, st>>>(dV, dE, N, t01, x, y, nullptr, Wb);
-        else k_na_layer<NA_OUTPUT><<<grid, 256, 0, st>>>(dV, dE, N, t01, x, nullptr, dp, Wb);
+        const float *xc = x;
+        if (l == 0) s = launch(k_na_layer<NA_INPUT>, grid, st, dV, dE, N, t, none_in, y, none_out, Wb);
+        else if (l < L - 1) s = launch(k_na_layer<NA_HIDDEN>, grid, st, dV, dE, N, t, xc, y, none_out, Wb);
+        else s = launch(k_na_layer<NA_OUTPUT>, grid, st, dV, dE, N, t, xc, none_out, dp, Wb);
         float *tmp = x;
         x = y;
         y = tmp;
     }
-    return cudaGetLastError() == cudaSuccess ? GC_OK : GC_ERR_CUDA;
+    return s;
 }

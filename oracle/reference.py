@@ -165,6 +165,85 @@ def greedy_color(N: int, V, E, p) -> np.ndarray:
     return out
 
 
+def has_models() -> bool:
+    return all(os.path.exists(os.path.join(MODELS, f"m{L}.gnn")) for L in (2, 3, 4))
+
+
+class GnnJob:
+    """The reference's GNN heuristic as its runner drives it: gnn_setup reads models/m{L}.gnn
+    relative to the working directory (src/gnn.c:24-25), so the call runs from _ref/, where
+    oracle/Makefile copies the reference's model files; gnn_internal_par (gnn.c:78-83) then gives
+    p and the JP colors, and each Culberson round sets p := color and re-runs
+    jones_plassmann_internal (src/runner.c:139-152)."""
+
+    def __init__(self, N: int, V, E, layers: int):
+        L = lib()
+        L.gnn_setup.argtypes = [C.c_uint32, C.c_uint32]
+        L.gnn_setup.restype = vp
+        L.gnn_internal_par.argtypes = [C.c_uint32, vp, vp, vp, vp, vp, vp]
+        L.gnn_cleanup.argtypes = [vp]
+        self.N = N
+        self.V = np.ascontiguousarray(V, np.uint32)
+        self.E = np.ascontiguousarray(E, np.uint32) if len(E) else np.zeros(1, np.uint32)
+        M = int(self.V[N])
+        C.c_int.in_dll(L, "layers").value = int(layers)
+        cwd = os.getcwd()
+        os.chdir(os.path.join(HERE, "_ref"))
+        try:
+            self.ad = L.gnn_setup(N, M)
+        finally:
+            os.chdir(cwd)
+        self.jp = L.jones_plassmann_setup(N, M)
+        self.p = aligned(N + 8, np.float64)
+        self.color = np.zeros(max(N, 1), np.int32)
+
+    def run(self):
+        """One f_par call: GNN priorities + JP.  Returns the colors (a view, overwritten by the next
+        call)."""
+        lib().gnn_internal_par(self.N, self.V.ctypes.data, self.E.ctypes.data, self.ad, self.jp,
+                               self.p.ctypes.data, self.color.ctypes.data)
+        return self.color
+
+    def culberson(self):
+        """One recoloring round: p := color, then the reference's JP."""
+        self.p[:self.N] = self.color[:self.N]
+        lib().jones_plassmann_internal(self.N, self.V.ctypes.data_as(u32p), self.E.ctypes.data_as(u32p), self.jp,
+                                       self.p.ctypes.data, self.color.ctypes.data_as(i32p))
+        return self.color
+
+    def close(self):
+        if self.ad:
+            lib().gnn_cleanup(self.ad)
+            lib().jones_plassmann_cleanup(self.jp)
+            self.ad = None
+
+
+def csr_from_samples(N: int, I, J):
+    """The reference's own graph construction from 0-based edge samples: mtx_to_graph_par (both
+    directions of every entry, src/fast_io.c:171-202), graph_sort_edges_par and graph_make_simple
+    (fast_io.c:450-477).  Returns (V, E) as numpy copies."""
+    L = lib()
+    fn = L.mtx_to_graph_par
+    fn.argtypes = [C.c_uint32, u32p, u32p, C.c_uint32, C.POINTER(u32p), C.POINTER(u32p)]
+    L.graph_sort_edges_par.argtypes = [C.c_uint32, u32p, u32p]
+    L.graph_make_simple.argtypes = [C.c_uint32, u32p, C.POINTER(u32p)]
+    I1 = np.ascontiguousarray(I, np.uint32) + np.uint32(1)
+    J1 = np.ascontiguousarray(J, np.uint32) + np.uint32(1)
+    Vp, Ep = u32p(), u32p()
+    fn(len(I1), I1.ctypes.data_as(u32p), J1.ctypes.data_as(u32p), N, C.byref(Vp), C.byref(Ep))
+    del I1, J1
+    L.graph_sort_edges_par(N, Vp, Ep)
+    L.graph_make_simple(N, Vp, C.byref(Ep))
+    V = np.ctypeslib.as_array(Vp, shape=(N + 1,)).copy()
+    M = int(V[N])
+    E = np.ctypeslib.as_array(Ep, shape=(max(M, 1),))[:M].copy()
+    libc = C.CDLL(None)
+    libc.free.argtypes = [vp]
+    libc.free(C.cast(Vp, vp))
+    libc.free(C.cast(Ep, vp))
+    return V, E
+
+
 def validate(N: int, V, E, color) -> int:
     L = lib()
     V, E, Vp, Ep = _csr(V, E)

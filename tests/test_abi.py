@@ -68,3 +68,18 @@ def test_cli_starts():
     assert r.returncode == 1 and "Unable to open file" in r.stdout
     r = subprocess.run([exe, "-x"], capture_output=True, text=True, timeout=30)
     assert r.returncode == 1
+
+
+REF_MAIN = os.path.join(ROOT, "oracle", "_ref", "coloring_main")
+
+
+def test_reference_main_links_against_the_library_alone():
+    """INTEGRATION.md option 2: the reference's unmodified src/main.c, compiled against include/ and
+    linked against libgnncolor.so (oracle/Makefile builds it where the reference sources exist),
+    needs nothing else of the reference and starts without a GPU."""
+    if not os.path.exists(REF_MAIN):
+        pytest.skip("the reference's main.c was not compiled here (reference sources absent at build time)")
+    ldd = subprocess.run(["ldd", REF_MAIN], capture_output=True, text=True, timeout=60).stdout
+    assert "libgnncolor.so" in ldd and "libref" not in ldd, ldd
+    r = subprocess.run([REF_MAIN, "-h"], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 0 and r.stdout.startswith("GNN-based greedy graph coloring")

@@ -268,6 +268,36 @@ def test_cli_output_lines(golden, tmp_path):
     assert valsf[2] == valsf[4] == valsf[5] == valsf[6] == valsf[7] == 0  # -f skips LLF, SLL, ID, SDA, SD
 
 
+def test_reference_main_prints_what_the_cli_prints(golden, tmp_path):
+    """INTEGRATION.md option 2 on the GPU: the reference's own main.c linked against this library
+    prints the same lines as cli/coloring (names, color counts, column count; times masked), in
+    runner mode with Culberson and in quick mode."""
+    ref_main = os.path.join(os.path.dirname(R.PATH), "coloring_main")
+    if not os.path.exists(ref_main):
+        pytest.skip("the reference's main.c was not compiled here (reference sources absent at build time)")
+    for L in (2, 3, 4):
+        gcn.model_write(str(tmp_path / f"m{L}.gnn"), *golden.model(L))
+    N, V, E = golden.graph("er1500")
+    path = str(tmp_path / "g.mtx")
+    gcn.mtx_write(path, N, V, E)
+    env = dict(os.environ, GC_MODEL_DIR=str(tmp_path))
+
+    def run(exe, *args):
+        r = subprocess.run([exe, "-g", path, *args], capture_output=True, text=True, timeout=600, env=env)
+        assert r.returncode == 0, (exe, r.stderr)
+        return r.stdout
+
+    def masked(out):
+        return [ln.split(" ")[:2] + [len(ln.split(" "))] for ln in out.rstrip("\n").split("\n")]
+
+    cli = os.path.join(PKG, "cli", "coloring")
+    a, b = run(ref_main, "-c", "3", "1", "4"), run(cli, "-c", "3", "1", "4")
+    assert masked(a) == masked(b)
+    assert len(masked(a)) == 8 * 3
+    assert run(ref_main, "-q") == run(cli, "-q")
+    assert run(ref_main, "-q", "-f") == run(cli, "-q", "-f")
+
+
 def test_incidence_orderings_color_like_the_reference(gpu_ctx, golden):
     """JP on the ID / SDA / SD priorities (host orderings) gives the reference's colors."""
     inc = np.load(os.path.join(GOLDEN, "golden_incidence.npz"))

@@ -159,3 +159,24 @@ def test_incidence_orderings_match_live_reference():
             ref = R.aligned(N + 8, np.float64)
             getattr(L, fn)(N, Vc.ctypes.data_as(u32), Ec.ctypes.data_as(u32), ref.ctypes.data)
             assert np.array_equal(_ordering(fn, N, V, E), ref[:N]), (N, fn)
+
+
+def test_numpy_rmat_samples_give_the_library_graph():
+    """The reference arm of bench.py builds its graph without the library: synthgen's numpy R-MAT
+    samples, turned into a CSR by the reference's own mtx_to_graph_par + graph_sort_edges_par +
+    graph_make_simple.  That CSR must be the library's gen_rmat graph exactly."""
+    import synthgen
+    from oracle import reference as R
+    if not R.available():
+        pytest.skip("oracle/_ref/libref.so not built")
+    for scale, seed, ef in ((10, 2, 16), (13, 7, 16), (12, 5, 8.5)):
+        n = 1 << scale
+        I, J = synthgen.rmat_samples(n, ef, seed, workers=1)
+        V, E = R.csr_from_samples(n, I, J)
+        _, V2, E2 = gcn.gen_rmat(n, ef, seed)
+        assert np.array_equal(V, V2) and np.array_equal(E, E2), (scale, seed)
+    # non-power-of-two n: samples with an id >= n are dropped, as the library does
+    I, J = synthgen.rmat_samples(3000, 8, 11, workers=1)
+    V, E = R.csr_from_samples(3000, I, J)
+    _, V2, E2 = gcn.gen_rmat(3000, 8, 11)
+    assert np.array_equal(V, V2) and np.array_equal(E, E2)

@@ -4,7 +4,8 @@ path that cannot afford cudaMalloc's implicit synchronisation).
 
 It must give exactly the priorities of the regular entry point, gc_priority(GC_GNN) (tolerance 0,
 as every GraphSAGE parity test here), on two calls in a row with different graphs and models --
-the second call reuses the shared scratch array the first one left behind -- and it must refuse
+the second call reuses the shared scratch array the first one left behind and, being the first to
+run a hidden layer, must load no code and allocate nothing -- and it must refuse
 graphs larger than its fixed scratch.  Inputs and outputs are device buffers the test allocates
 itself, as such a caller would."""
 import ctypes as C
@@ -54,9 +55,11 @@ def noalloc_priorities(N, V, E, params, md):
 
 
 def test_noalloc_matches_regular_entry_point_twice(gpu_ctx):
+    # The 2-layer model first: the second call is the first to run a hidden layer, so it would load
+    # that kernel (and allocate for its code) if the first call had not loaded every kernel.
     cases = [
-        (gcn.gen_rmat(1 << 15, 16, 7), gcn.synthetic_model(3, 1003)),   # hubs, many isolated vertices
-        (gcn.gen_er(20000, 100000, 3), gcn.synthetic_model(2, 1002)),   # smaller graph, other model
+        (gcn.gen_er(20000, 100000, 3), gcn.synthetic_model(2, 1002)),   # no hidden layer
+        (gcn.gen_rmat(1 << 15, 16, 7), gcn.synthetic_model(3, 1003)),   # hubs, isolated vertices, a hidden layer
     ]
     for call, ((N, V, E), (params, md)) in enumerate(cases):
         assert N <= MAX_V
