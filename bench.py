@@ -760,7 +760,14 @@ def _sweep(srv, pool, J, replay, alone_counts):
             c = alone_counts.get((id(gr), h))
             if c is not None and c != inf["colors"]:
                 same = False
+        by_class = {}
+        for cls, lo, hi in (("small", 0, 1 << 17), ("rmat20", 1 << 17, 1 << 21), ("rmat24", 1 << 21, 1 << 32)):
+            lat = [inf["latency_ms"] for inf in infos if lo < inf["N"] + 1 <= hi]
+            if lat:
+                by_class[cls] = {"jobs": len(lat), "p50_ms": float(np.percentile(lat, 50)),
+                                 "p99_ms": float(np.percentile(lat, 99))}
         sweep.append({"offered_jobs_per_s": rate, "jobs": Jr, "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
+                      "by_size": by_class,
                       "max_ms": st["max_ms"], "edges_per_s": st["edges_per_s"],
                       "jobs_per_s": st["completed"] / st["span_s"] if st["span_s"] else None,
                       "passes": st["launches"], "batched_jobs": st["batched_jobs"],

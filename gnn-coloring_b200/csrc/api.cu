@@ -120,7 +120,7 @@ void gc_graph_free_buffers(gc_graph *g) {
                     g->big,       g->hubs,   g->x,        g->y,        g->t01,      g->deg_rem,  g->frontier,
                     g->frontier2, g->removed, g->leaf_list, g->vorder, g->rank,     g->p64,      g->seg_voff,
                     g->seg_stat,  g->fmask,    g->giant,    g->hub_stage, g->jprec, g->class_first,
-                    g->gnn_ctr};
+                    g->gnn_ctr,   g->giant_aux, g->jpsplit, g->part_tiles};
     for (void *p : bufs) gc_dev_free(ctx, p);
 }
 
@@ -283,6 +283,9 @@ gc_status gc_ctx_create(int device, gc_ctx **out) {
     if (const char *e = getenv("GC_JP_TIGHT")) ctx->jp_tight = (unsigned int)strtoul(e, nullptr, 10);
     if (const char *e = getenv("GC_JP_CLASSES")) ctx->jp_classes = atoi(e) != 0;
     if (const char *e = getenv("GC_JP_DECIDE")) ctx->jp_decide = atoi(e) != 0;
+    if (const char *e = getenv("GC_JP_LIGHT_WARPS")) ctx->jp_light_warps = atoi(e);
+    if (const char *e = getenv("GC_JP_CORE"))
+        ctx->jp_core_max = std::min<uint32_t>((uint32_t)strtoul(e, nullptr, 10), 32768u);
     if (const char *e = getenv("GC_JP_NAP")) ctx->jp_nap = (unsigned int)strtoul(e, nullptr, 10);
     if (const char *e = getenv("GC_GNN_WARP_DEGREE")) ctx->gnn_warp_deg = (uint32_t)strtoul(e, nullptr, 10);
     if (const char *e = getenv("GC_GNN_HUB_SMS")) ctx->gnn_hub_sms = atoi(e);

@@ -24,7 +24,10 @@ struct DevState {
     unsigned int big_leaves;  // coloring: leaves with too many neighbours for one thread
     unsigned int thin;        // preparation: vertices with at most the GNN thin-tier degree
     unsigned int gnn_wide;    // preparation: vertices in the GNN warp tier
-    unsigned int pad[4];
+    unsigned int ticket_light;  // coloring: next ticket of the light stream
+    unsigned int n_heavy;       // coloring: tickets of the heavy stream (after the core)
+    unsigned int n_light;       // coloring: tickets of the light stream (after the core)
+    unsigned int pad;
 };
 
 enum DevErr : unsigned int {

@@ -40,6 +40,9 @@ struct gc_ctx {
     unsigned int jp_nap = 32;            // coloring: first sleep between polling rounds (ns)
     bool jp_decide = true;               // coloring: early decisions from published forbidden colors
     bool jp_classes = true;              // Culberson rounds: class by class instead of tickets
+    uint32_t jp_core_max = 32768;        // coloring: first tickets colored inside one cluster (0: off; GC_JP_CORE)
+    int jp_core_cluster = -1;            // CTAs of that cluster (16 or 8; 0: unavailable; -1: not yet queried)
+    int jp_light_warps = 2;              // coloring: warps per CTA on the light stream (0: no split; GC_JP_LIGHT_WARPS)
     int gnn_blocks_per_sm[3] = {0, 0, 0};  // resident CTAs of each GNN layer kernel
     uint32_t gnn_warp_deg = GC_GNN_WIDE_DEGREE;  // GNN: above this many neighbours a vertex gets a warp
     uint32_t gnn_giant_deg = 0;          // GNN: hubs with at least this many neighbours are staged (0: automatic)
@@ -76,10 +79,11 @@ struct ProfScope {
 // pass, this many edges per warp task.
 constexpr uint32_t GC_SPLIT_CHUNK = 1024;  // edges per warp task (shared-memory buffer per warp)
 constexpr int GC_JP_MASK_WORDS = 8;        // published forbidden colors: 8 x 32 = colors 1..256
-// Giant hubs: hubs with at least max(2 * hub degree, largest hub degree / 3) neighbours.  One SM
-// gathers scattered 64-byte rows at only about 11 GB/s, so before each GNN layer all SMs copy these
-// hubs' neighbour rows, in CSR order, into a contiguous staging buffer that the hub's chain then
-// streams with bulk copies.  GC_GIANT_TASK rows per gather task; at most GC_GIANT_MAX_ROWS rows.
+// Giant hubs: hubs with at least max(2 * hub degree, largest hub degree / 3) neighbours.  Before each
+// GNN layer all SMs copy these hubs' neighbour rows, in CSR order, into a staging buffer with one
+// column per feature (each hub's columns padded to a multiple of 32 rows); one warp per hub and
+// feature then evaluates the column's FP32 chain exactly, 1,024 values per step.  GC_GIANT_TASK rows
+// per gather task; at most GC_GIANT_MAX_ROWS rows.
 constexpr uint32_t GC_GIANT_TASK = 2048;
 constexpr uint64_t GC_GIANT_MAX_ROWS = 1ull << 25;
 
@@ -102,8 +106,10 @@ struct gc_graph {
     uint32_t *pc = nullptr;     // predecessor counts
     uint32_t *order = nullptr;  // vertices by descending key, ascending id on ties: the ticket order
     uint32_t *leaf_list = nullptr;  // leaves too large for one thread
-    uint32_t *rank = nullptr;       // ticket of each ordered vertex (all ones elsewhere)
+    uint32_t *rank = nullptr;       // ticket of each core vertex (valid for the core tickets only)
     uint4 *jprec = nullptr;         // per ticket: (vertex, first CSR entry, predecessor count, 0)
+    uint4 *jpsplit = nullptr;       // the tickets after the core: heavy stream from the front, light from the back
+    uint32_t *part_tiles = nullptr; // heavy tickets per tile of the split (prefix)
     uint32_t *class_first = nullptr;  // Culberson rounds: first ticket position of each key (old color)
     size_t class_cap = 0;
     // forbidden colors 1..256 published by waiting vertices of the ordered coloring kernel:
@@ -119,15 +125,18 @@ struct gc_graph {
     size_t big_cap = 0;              // words allocated for `big`
     uint32_t *hubs = nullptr;        // vertices with deg > GC_GNN_HUB_DEGREE, by descending degree
     uint32_t n_hubs = 0;
-    // the leading n_giant hubs are giant: giant[0..n_giant] their staging row offsets (even, so
-    // 8-byte rows start 16-byte aligned), then n_giant_tasks (hub slot, first row) gather tasks
+    // the leading n_giant hubs are giant: giant[0..n_giant] their staging row offsets (multiples of
+    // 32: hub h's 16 columns start at 16 * giant[h] floats and are giant[h + 1] - giant[h] rows
+    // long), then n_giant_tasks (hub slot, first row) gather tasks
     uint32_t n_giant = 0, n_giant_tasks = 0;
     uint32_t *giant = nullptr;
     size_t giant_cap = 0;            // words allocated for `giant`
     uint64_t giant_rows = 0;         // staging rows
-    float *hub_stage = nullptr;      // GNN: giant_rows + 2 rows of 16 floats (allocated on first use)
+    float *hub_stage = nullptr;      // GNN: giant_rows x 16 floats, feature columns (allocated on first use)
     uint64_t hub_stage_rows = 0;
-    uint32_t *gnn_ctr = nullptr;     // GNN: 8 work counters when SMs are reserved for giant hubs
+    uint32_t *giant_aux = nullptr;   // GNN: per giant hub 16 feature sums, then one completion counter each
+    size_t giant_aux_cap = 0;
+    uint32_t *gnn_ctr = nullptr;     // GNN: 8 work counters (bulk hand-out)
     uint32_t *vorder = nullptr;      // the other vertices by descending degree (GNN schedule)
     uint32_t n_vorder = 0;
     uint32_t n_wide = 0;             // leading vorder entries with more than GC_GNN_WARP_DEGREE neighbours

@@ -548,25 +548,16 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned int parity, De
 __device__ __forceinline__ void cp_async_8(void *smem, const void *gmem) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(smem)), "l"(gmem) : "memory");
 }
-// A contiguous block by the TMA engine: `bytes` (a multiple of 16; both addresses 16-byte aligned)
-// from global to this CTA's shared memory, completing `bytes` of the mbarrier's transaction count.
-__device__ __forceinline__ void bulk_g2s(void *smem, const void *gmem, unsigned int bytes, uint64_t *bar) {
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                     smem_u32(smem)),
-                 "l"(gmem), "r"(bytes), "r"(smem_u32(bar))
-                 : "memory");
-}
-__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, unsigned int bytes) {
-    asm volatile("{\n .reg .b64 st;\n mbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n}" ::"r"(smem_u32(bar)),
-                 "r"(bytes)
-                 : "memory");
-}
 __device__ __forceinline__ void cp_async_16(void *smem, const void *gmem) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(smem)), "l"(gmem) : "memory");
 }
 
-// Giant hubs' neighbour rows, in CSR order, into the staging buffer: all SMs, one warp per task of
-// GC_GIANT_TASK rows; four lanes per 64-byte row (one lane per 8-byte input-layer row).
+// Giant hubs' neighbour rows, in CSR order, into the staging buffer, one column per feature: hub
+// slot h owns the block of 16 columns starting at 16 * giant[h], each giant[h + 1] - giant[h] floats
+// long (its degree rounded up to 32), so that one warp later streams one feature's column with
+// coalesced loads.  All SMs, one warp per task of GC_GIANT_TASK rows.  Hidden and output layers:
+// four lanes per 64-byte row (one float4 each), eight rows per instruction; input layer: a lane per
+// row and two columns (deg/md, id/N).
 template <int MODE>
 __global__ void __launch_bounds__(256) k_gnn_hub_gather(const uint32_t *__restrict__ V, const uint32_t *__restrict__ E,
                                                         const uint32_t *__restrict__ hubs,
@@ -581,13 +572,17 @@ __global__ void __launch_bounds__(256) k_gnn_hub_gather(const uint32_t *__restri
         const uint32_t slot = tasks[2 * t], r0 = tasks[2 * t + 1];
         const uint32_t u = hubs[slot], base = V[u], d = V[u + 1] - base;
         const uint32_t rend = min(d, r0 + GC_GIANT_TASK);
-        const size_t off = giant[slot];
+        const size_t dp = giant[slot + 1] - giant[slot];
+        float *cols = stage + (size_t)FEAT * giant[slot];
         if (MODE == MODE_INPUT) {
-            float2 *dst = reinterpret_cast<float2 *>(stage) + off;
-            for (uint32_t r = r0 + lane; r < rend; r += 32) dst[r] = __ldg(t01 + ld_stream(E + base + r));
+            for (uint32_t r = r0 + lane; r < rend; r += 32) {
+                const float2 tv = __ldg(t01 + ld_stream(E + base + r));
+                cols[r] = tv.x;
+                cols[dp + r] = tv.y;
+            }
         } else {
             const float4 *X4 = reinterpret_cast<const float4 *>(x);
-            float4 *dst = reinterpret_cast<float4 *>(stage) + off * 4;
+            float *c0 = cols + (size_t)(4 * q) * dp;
             for (uint32_t r = r0 + (lane >> 2); r < rend; r += 32) {
                 uint32_t v[4];
                 float4 val[4];
@@ -598,80 +593,185 @@ __global__ void __launch_bounds__(256) k_gnn_hub_gather(const uint32_t *__restri
                     if (r + 8 * k < rend) val[k] = __ldg(X4 + (size_t)v[k] * 4 + q);
 #pragma unroll
                 for (int k = 0; k < 4; k++)
-                    if (r + 8 * k < rend) dst[(size_t)(r + 8 * k) * 4 + q] = val[k];
+                    if (r + 8 * k < rend) {
+                        const uint32_t rr = r + 8 * k;
+                        c0[rr] = val[k].x;
+                        c0[dp + rr] = val[k].y;
+                        c0[2 * dp + rr] = val[k].z;
+                        c0[3 * dp + rr] = val[k].w;
+                    }
             }
         }
     }
 }
 
-// Giant hubs (hub slots below n_giant: the leading, largest hubs) read their rows from the staging
-// buffer: one bulk copy per stage by the producer's lane 0.  The others gather rows with cp.async.
+// The reference's neighbour sum s = (((+0 + a_0) + a_1) + ...) + a_{n-1} in FP32, round to nearest
+// even, for a column of n values a_i >= +0 (ReLU outputs, deg/md, id/N: never negative), with the
+// whole warp, 1,024 values per step.  Bit-identical to the serial chain, by this argument:
+//   While s lies in the binade [2^e, 2^(e+1)), s = m * u with u = 2^(e-23) and an integer m in
+//   [2^23, 2^24).  Adding a >= 0 rounds m + a/u to an integer: with a/u = q + r (q integer,
+//   0 <= r < 1) the result is m + q for r < 1/2 and m + q + 1 for r > 1/2, whatever m is; only an
+//   exact tie (r = 1/2) depends on m (to even).  So as long as every partial sum stays below
+//   2^(e+1), i.e. m plus all increments stays below 2^24, the step's result is m + (the integer
+//   sum of the increments), and integer addition is associative.  The increments are exact: a/u is
+//   a scaling by a power of two.
+// A step falls back to the serial chain (shuffles broadcast the values; every lane adds them in
+// order, so s stays warp-uniform) when that does not hold: s below 2^-103 (grid or its inverse not
+// a normal float, e.g. the first step from +0) or infinite, a value with a/u >= 2^24 (or Inf/NaN), an exact tie
+// anywhere in the step, or a step that would carry s into the next binade.  Partial sums are
+// clamped at 2^24, which already means "fall back".  Each lane loads its next step's values while
+// the current ones are summed.
+__device__ __forceinline__ float exact_column_sum(const float *__restrict__ col, uint32_t n, int lane) {
+    constexpr uint32_t STEP = 1024, TOP = 1u << 24;
+    float s = 0.0f;
+    float nx[32];
+#pragma unroll
+    for (int j = 0; j < 32; j++) {
+        const uint32_t i = 32 * j + lane;
+        nx[j] = i < n ? __ldcg(col + i) : 0.0f;
+    }
+    for (uint32_t c0 = 0; c0 < n; c0 += STEP) {
+        const uint32_t cn = min(STEP, n - c0);
+        float a[32];
+#pragma unroll
+        for (int j = 0; j < 32; j++) a[j] = nx[j];
+        if (c0 + STEP < n) {
+#pragma unroll
+            for (int j = 0; j < 32; j++) {
+                const uint32_t i = c0 + STEP + 32 * j + lane;
+                nx[j] = i < n ? __ldcg(col + i) : 0.0f;
+            }
+        }
+        const uint32_t be = (__float_as_uint(s) >> 23) & 0xffu;  // biased exponent of s
+        if (be >= 24u && be < 255u) {
+            const float scale = __uint_as_float((277u - be) << 23);  // 1/u = 2^(23-e), e = be - 127
+            const float unscale = __uint_as_float((be - 23u) << 23);  // u = 2^(e-23)
+            const uint32_t m = __float2uint_rz(__fmul_rn(s, scale));
+            uint32_t acc = 0;
+            bool bad = false;
+#pragma unroll
+            for (int j = 0; j < 32; j++) {
+                const float xv = __fmul_rn(a[j], scale);
+                const bool ok = xv < 16777216.0f;  // false for >= 2^24, Inf and NaN
+                const float xs = ok ? xv : 0.0f;
+                const float qf = floorf(xs);
+                const float r = __fsub_rn(xs, qf);  // exact: xs < 2^24
+                bad |= !ok || r == 0.5f;
+                acc += __float2uint_rz(qf) + (r > 0.5f ? 1u : 0u);  // at most 32 * 2^24
+            }
+            if (!__any_sync(FULL, bad)) {
+                const uint32_t tot = __reduce_add_sync(FULL, min(acc, TOP));
+                const uint32_t mend = m + tot;
+                if (mend < TOP) {
+                    s = __fmul_rn(__uint2float_rn(mend), unscale);
+                    continue;
+                }
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < 32; j++) {
+            if (32u * j >= cn) break;
+#pragma unroll 8
+            for (int k = 0; k < 32; k++) {
+                const float t = __shfl_sync(FULL, a[j], k);
+                if (32u * j + k < cn) s = __fadd_rn(s, t);
+            }
+        }
+    }
+    return s;
+}
+
+// Giant hubs' layer: one warp per (hub, feature) -- two features in the input layer -- sums the
+// hub's staged column with exact_column_sum; the hub's last warp to finish (a counter per hub,
+// zeroed before the layer) runs the dense part: mean, 32 x 16 FMA chain in order, ReLU, and in the
+// output layer the reference's fixed-tree sum into the key.
+template <int MODE>
+__global__ void __launch_bounds__(128) k_gnn_giant_chain(const uint32_t *__restrict__ V, const uint32_t *__restrict__ hubs,
+                                                         const uint32_t *__restrict__ giant, uint32_t n_giant,
+                                                         const float *__restrict__ stage, const float2 *__restrict__ t01,
+                                                         const float *__restrict__ x, float *__restrict__ y,
+                                                         uint32_t *__restrict__ key, const float *__restrict__ Wb,
+                                                         float *__restrict__ sums, uint32_t *__restrict__ done) {
+    constexpr int NF = (MODE == MODE_INPUT) ? 2 : FEAT;
+    const int lane = threadIdx.x & 31;
+    const uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (w >= n_giant * NF) return;
+    const uint32_t h = w / NF, f = w % NF;
+    const uint32_t u = hubs[h], d = V[u + 1] - V[u];
+    const size_t dp = giant[h + 1] - giant[h];
+    const float sum = exact_column_sum(stage + (size_t)FEAT * giant[h] + f * dp, d, lane);
+    uint32_t last = 0;
+    if (lane == 0) {
+        sums[h * FEAT + f] = sum;
+        __threadfence();
+        last = atomicAdd(done + h, 1u) == NF - 1;
+    }
+    if (!__shfl_sync(FULL, last, 0)) return;
+    __threadfence();
+    const float fd = __uint2float_rn(d);
+    const int j = lane & 15;
+    float c = __ldg(Wb + 2 * FEAT * FEAT + j);
+    if (MODE == MODE_INPUT) {
+        float s0 = __ldcg(sums + h * FEAT), s1 = __ldcg(sums + h * FEAT + 1);
+        if (fd > 0.0f) {
+            s0 = __fdiv_rn(s0, fd);
+            s1 = __fdiv_rn(s1, fd);
+        }
+        const float2 self = t01[u];
+#pragma unroll
+        for (int i = 0; i < 32; i++) {
+            const float a = i < 8 ? s0 : (i < 16 ? s1 : (i < 24 ? self.x : self.y));
+            c = __fmaf_rn(__ldg(Wb + i * FEAT + j), a, c);
+        }
+    } else {
+        float nb = __ldcg(sums + h * FEAT + j);
+        if (fd > 0.0f) nb = __fdiv_rn(nb, fd);
+        const float self = x[(size_t)u * FEAT + j];
+#pragma unroll
+        for (int i = 0; i < 32; i++) {
+            const float a = __shfl_sync(FULL, i < FEAT ? nb : self, i & 15);
+            c = __fmaf_rn(__ldg(Wb + i * FEAT + j), a, c);
+        }
+    }
+    const float o = relu(c);
+    if (MODE == MODE_OUTPUT) {
+        // t_k = o_k + o_{k+8}, then ((t0+t1)+(t2+t3)) + ((t4+t5)+(t6+t7))
+        const float t = __fadd_rn(o, __shfl_sync(FULL, o, (lane + 8) & 31));
+        float tk[8];
+#pragma unroll
+        for (int k = 0; k < 8; k++) tk[k] = __shfl_sync(FULL, t, k);
+        const float p = __fadd_rn(__fadd_rn(__fadd_rn(tk[0], tk[1]), __fadd_rn(tk[2], tk[3])),
+                                  __fadd_rn(__fadd_rn(tk[4], tk[5]), __fadd_rn(tk[6], tk[7])));
+        if (lane == 0) key[u] = __float_as_uint(p);
+    } else if (lane < FEAT) {
+        y[(size_t)u * FEAT + lane] = o;
+    }
+}
+
+// The other hubs (slots n_giant .. n_hubs - 1): one CTA each gathers the rows with cp.async.
 template <int MODE>
 __global__ void __launch_bounds__(HUB_THREADS) k_gnn_hub(const uint32_t *__restrict__ V, const uint32_t *__restrict__ E,
                                                          const uint32_t *__restrict__ hubs,
                                                          const float2 *__restrict__ t01, const float *__restrict__ x,
                                                          float *__restrict__ y, uint32_t *__restrict__ key,
-                                                         const float *__restrict__ Wb, DevState *st,
-                                                         const float *__restrict__ staged_rows,
-                                                         const uint32_t *__restrict__ giant, uint32_t n_giant,
-                                                         uint32_t n_hubs, uint32_t *hub_ctr, uint32_t reserve) {
+                                                         const float *__restrict__ Wb, DevState *st, uint32_t first) {
     constexpr int ROW = (MODE == MODE_INPUT) ? 2 : FEAT;  // floats per staged row
     extern __shared__ __align__(16) float stage[];         // HUB_STAGES * HUB_ROWS * ROW floats
     __shared__ __align__(16) float sW[LAYER_PARAMS];
     __shared__ __align__(8) uint64_t full[HUB_STAGES], empty[HUB_STAGES];
-    __shared__ uint32_t hub_slot;
     for (int i = threadIdx.x; i < LAYER_PARAMS; i += blockDim.x) sW[i] = Wb[i];
     if (threadIdx.x == 0) {
-        // Which hub: blockIdx.x, or with hub_ctr the next giant hub (hub_ctr[0]) on a reserved SM and
-        // the next other hub (hub_ctr[1]) elsewhere, each falling back to the other list; a grid of
-        // n_hubs CTAs takes every hub exactly once wherever its CTAs land.
-        uint32_t h = blockIdx.x;
-        if (hub_ctr) {
-            const bool mine = sm_id() < reserve;
-            h = 0xffffffffu;
-            for (int pass = 0; pass < 2 && h == 0xffffffffu; pass++) {
-                if ((pass == 0) == mine) {
-                    const uint32_t gi = atomicAdd(&hub_ctr[0], 1u);
-                    if (gi < n_giant) h = gi;
-                } else {
-                    const uint32_t oi = atomicAdd(&hub_ctr[1], 1u) + n_giant;
-                    if (oi < n_hubs) h = oi;
-                }
-            }
+        for (int i = 0; i < HUB_STAGES; i++) {
+            mbar_init(&full[i], 32);  // one copy-completion arrival per producer lane
+            mbar_init(&empty[i], 1);  // the consumer's release
         }
-        hub_slot = h;
-        if (h != 0xffffffffu)
-            for (int i = 0; i < HUB_STAGES; i++) {
-                // staged: the producer's expect-tx arrival, completed by the bulk copy's bytes;
-                // otherwise one copy-completion arrival per producer lane
-                mbar_init(&full[i], h < n_giant ? 1 : 32);
-                mbar_init(&empty[i], 1);  // the consumer's release
-            }
     }
     __syncthreads();
-    const uint32_t hi = hub_slot;
-    if (hi == 0xffffffffu) return;
-    const uint32_t u = hubs[hi];
+    const uint32_t u = hubs[first + blockIdx.x];
     const uint32_t beg = V[u], end = V[u + 1], d = end - beg;
     const uint32_t nchunks = (d + HUB_ROWS - 1) / HUB_ROWS;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
-    const bool staged = hi < n_giant;
-    if (warp == 1 && staged) {
-        if (lane == 0) {
-            constexpr uint32_t ROWB = ROW * sizeof(float);  // 64 bytes (8 in the input layer)
-            const char *src = reinterpret_cast<const char *>(staged_rows) + (size_t)giant[hi] * ROWB;
-            for (uint32_t c = 0; c < nchunks; c++) {
-                const uint32_t s = c % HUB_STAGES;
-                if (c >= HUB_STAGES && !mbar_wait(&empty[s], ((c / HUB_STAGES) - 1) & 1u, st)) return;
-                const uint32_t rows = min((uint32_t)HUB_ROWS, d - c * HUB_ROWS);
-                const uint32_t bytes = (rows * ROWB + 15u) & ~15u;  // an odd 8-byte row count reads one pad row
-                mbar_arrive_expect_tx(&full[s], bytes);
-                bulk_g2s(stage + (size_t)s * HUB_ROWS * ROW, src + (size_t)c * HUB_ROWS * ROWB, bytes, &full[s]);
-            }
-        }
-        return;
-    }
     if (warp == 1) {
         // producer: ids HUB_ID_AHEAD stages ahead in registers, rows via cp.async
         uint32_t ids[HUB_ID_AHEAD][4];
@@ -728,14 +828,7 @@ __global__ void __launch_bounds__(HUB_THREADS) k_gnn_hub(const uint32_t *__restr
     float acc = 0.0f;
     for (uint32_t c = 0; c < nchunks; c++) {
         const uint32_t s = c % HUB_STAGES;
-        if (!mbar_wait(&full[s], (c / HUB_STAGES) & 1u, st)) {
-            // staged: the bulk copies already issued into this CTA's shared memory must land
-            // before it exits (each wait again bounded); the producer stops at its next wait
-            if (staged)
-                for (uint32_t k = c + 1; k < nchunks && k < c + HUB_STAGES; k++)
-                    mbar_wait(&full[k % HUB_STAGES], (k / HUB_STAGES) & 1u, st);
-            return;
-        }
+        if (!mbar_wait(&full[s], (c / HUB_STAGES) & 1u, st)) return;  // the producer stops at its next wait
         const float *buf = stage + (size_t)s * HUB_ROWS * ROW;
         const uint32_t cnt = min((uint32_t)HUB_ROWS, end - (beg + c * HUB_ROWS));
         if (lane < ROW) {
@@ -804,14 +897,15 @@ gc_status launch_layer(gc_graph *g, const float *Wb, const float *x, float *y, c
                        cudaEvent_t fork, cudaEvent_t join, uint32_t reserve) {
     gc_ctx *ctx = g->ctx;
     gc_status s;
-    // with reserve > 0: SMs 0..reserve-1 are left to the giant-hub CTAs; counters, zeroed here for
-    // each layer, hand out giant hubs, other hubs, bulk items (three) and thin groups
-    uint32_t *ctr = reserve ? g->gnn_ctr : nullptr;
-    if (reserve && (s = gc_check_cuda(ctx, cudaMemsetAsync(ctr, 0, 8 * sizeof(uint32_t), ctx->stream),
-                                      "gnn work counters")) != GC_OK)
+    // counters, zeroed here for each layer: bulk items (2..4), thin groups (5); with reserve > 0 the
+    // bulk CTAs that start on SMs 0..reserve-1 leave those SMs to the giant hubs' chains
+    uint32_t *ctr = g->gnn_ctr;
+    if ((s = gc_check_cuda(ctx, cudaMemsetAsync(ctr, 0, 8 * sizeof(uint32_t), ctx->stream), "gnn work counters")) !=
+        GC_OK)
         return s;
     if (g->n_hubs) {
         constexpr int ROW = (MODE == MODE_INPUT) ? 2 : FEAT;
+        constexpr uint32_t NF = (MODE == MODE_INPUT) ? 2 : FEAT;
         const size_t smem = (size_t)HUB_STAGES * HUB_ROWS * ROW * sizeof(float);
         if (!ctx->hub_smem_set[MODE]) {  // once per context: keeps the call out of captured sequences
             if ((s = gc_check_cuda(ctx, cudaFuncSetAttribute(k_gnn_hub<MODE>,
@@ -826,15 +920,28 @@ gc_status launch_layer(gc_graph *g, const float *Wb, const float *x, float *y, c
         ProfScope ps(ctx, MODE == MODE_INPUT ? "gnn_hub_input" : (MODE == MODE_HIDDEN ? "gnn_hub_hidden" : "gnn_hub_output"),
                      side);
         if (g->n_giant) {
-            ProfScope pg(ctx, "gnn_hub_gather", side);
-            k_gnn_hub_gather<MODE><<<ctx->num_sms * 4, 256, 0, side>>>(g->V, g->E, g->hubs, g->giant, g->n_giant,
-                                                                        g->n_giant_tasks, g->t01, x, g->hub_stage);
+            float *sums = reinterpret_cast<float *>(g->giant_aux);
+            uint32_t *done = g->giant_aux + (size_t)FEAT * g->n_giant;
+            if ((s = gc_check_cuda(ctx, cudaMemsetAsync(done, 0, sizeof(uint32_t) * g->n_giant, side),
+                                   "giant hub counters")) != GC_OK)
+                return s;
+            {
+                ProfScope pg(ctx, "gnn_giant_gather", side);
+                k_gnn_hub_gather<MODE><<<ctx->num_sms * 4, 256, 0, side>>>(g->V, g->E, g->hubs, g->giant, g->n_giant,
+                                                                            g->n_giant_tasks, g->t01, x, g->hub_stage);
+                ctx->launches++;
+            }
+            ProfScope pc(ctx, "gnn_giant_chain", side);
+            const uint32_t warps = g->n_giant * NF;
+            k_gnn_giant_chain<MODE><<<(warps + 3) / 4, 128, 0, side>>>(g->V, g->hubs, g->giant, g->n_giant, g->hub_stage,
+                                                                       g->t01, x, y, g->key, Wb, sums, done);
             ctx->launches++;
         }
-        k_gnn_hub<MODE><<<g->n_hubs, HUB_THREADS, smem, side>>>(g->V, g->E, g->hubs, g->t01, x, y, g->key, Wb,
-                                                                ctx->dstate, g->hub_stage, g->giant, g->n_giant,
-                                                                g->n_hubs, reserve ? ctr : nullptr, reserve);
-        ctx->launches++;
+        if (g->n_hubs > g->n_giant) {
+            k_gnn_hub<MODE><<<g->n_hubs - g->n_giant, HUB_THREADS, smem, side>>>(
+                g->V, g->E, g->hubs, g->t01, x, y, g->key, Wb, ctx->dstate, g->n_giant);
+            ctx->launches++;
+        }
         if ((s = gc_check_launch(ctx, "gnn hub layer")) != GC_OK) return s;
     }
     int &blocks = ctx->gnn_blocks_per_sm[MODE];
@@ -851,15 +958,14 @@ gc_status launch_layer(gc_graph *g, const float *Wb, const float *x, float *y, c
         const uint32_t first_thin = g->n_vorder - g->n_thin;
         if (first_thin) {
             k_gnn_layer<MODE><<<ctx->num_sms * blocks, GNN_THREADS, 0, ctx->stream>>>(
-                g->V, g->E, g->vorder, g->n_wide_gnn, first_thin, g->t01, x, y, g->key, Wb, reserve ? ctr + 2 : nullptr,
-                reserve, ctx->gnn_grab, ctx->gnn_heavy);
+                g->V, g->E, g->vorder, g->n_wide_gnn, first_thin, g->t01, x, y, g->key, Wb, ctr + 2, reserve,
+                ctx->gnn_grab, ctx->gnn_heavy);
             ctx->launches++;
         }
         if (g->n_thin) {
             const uint32_t grid = std::min<uint32_t>((uint32_t)ctx->num_sms * 3, (g->n_thin + THIN_THREADS - 1) / THIN_THREADS);
             k_gnn_thin<MODE><<<grid, THIN_THREADS, 0, ctx->stream>>>(g->V, g->E, g->vorder, first_thin, g->n_vorder,
-                                                                     g->t01, x, y, g->key, Wb,
-                                                                     reserve ? ctr + 5 : nullptr, reserve,
+                                                                     g->t01, x, y, g->key, Wb, ctr + 5, reserve,
                                                                      ctx->gnn_grab);
             ctx->launches++;
         }
@@ -883,22 +989,28 @@ gc_status gc_priority_gnn(gc_graph *g, const gc_model *m) {
     if ((s = gc_alloc(ctx, &g->x, rows * FEAT, "gnn features")) != GC_OK) return s;
     if ((s = gc_alloc(ctx, &g->y, rows * FEAT, "gnn features")) != GC_OK) return s;
     if ((s = gc_alloc(ctx, &g->t01, rows, "gnn input table")) != GC_OK) return s;
-    if (g->n_giant && g->hub_stage_rows < g->giant_rows + 2) {
+    if (g->n_giant && g->hub_stage_rows < g->giant_rows) {
         gc_dev_free(ctx, g->hub_stage);
         g->hub_stage = nullptr;
-        if ((s = gc_alloc(ctx, &g->hub_stage, (size_t)(g->giant_rows + 2) * FEAT, "giant hub rows")) != GC_OK) return s;
-        g->hub_stage_rows = g->giant_rows + 2;
+        if ((s = gc_alloc(ctx, &g->hub_stage, (size_t)g->giant_rows * FEAT, "giant hub rows")) != GC_OK) return s;
+        g->hub_stage_rows = g->giant_rows;
     }
-    // SMs left to the giant hubs' CTAs (ctx->gnn_hub_sms: -1 one per giant hub, 0 none, n: SMs
-    // 0..n-1).  Beside the L1-bound bulk CTAs a giant hub's FP32 chain ran about twice as slow as
-    // alone; with its own SM and the bulk handed out by counters, GNN3 + JP on R-MAT 22 took
-    // 7.9-8.1 ms per job instead of 9.1 (B200, 23 giant hubs).
+    // giant hubs' feature sums (16 per hub) and completion counters (one per hub)
+    if (g->n_giant && g->giant_aux_cap < (size_t)(FEAT + 1) * g->n_giant) {
+        gc_dev_free(ctx, g->giant_aux);
+        g->giant_aux = nullptr;
+        if ((s = gc_alloc(ctx, &g->giant_aux, (size_t)(FEAT + 1) * g->n_giant, "giant hub sums")) != GC_OK) return s;
+        g->giant_aux_cap = (size_t)(FEAT + 1) * g->n_giant;
+    }
+    // SMs left to the giant hubs' chains (ctx->gnn_hub_sms: -1 one per giant hub, 0 none, n: SMs
+    // 0..n-1).  The bulk work is handed out by counters either way, so CTAs that start late (behind
+    // the hubs' CTAs) take less of it.
     uint32_t reserve = 0;
     if (ctx->gnn_hub_sms != 0 && g->n_giant) {
         reserve = ctx->gnn_hub_sms > 0 ? (uint32_t)ctx->gnn_hub_sms : g->n_giant;
         reserve = std::min<uint32_t>(reserve, (uint32_t)ctx->num_sms / 6);
     }
-    if (reserve && (s = gc_alloc(ctx, &g->gnn_ctr, 8, "gnn work counters")) != GC_OK) return s;
+    if ((s = gc_alloc(ctx, &g->gnn_ctr, 8, "gnn work counters")) != GC_OK) return s;
     if (ctx->side_stream == nullptr) {
         int lo = 0, hi = 0;
         cudaDeviceGetStreamPriorityRange(&lo, &hi);

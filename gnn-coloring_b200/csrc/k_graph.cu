@@ -164,12 +164,12 @@ gc_status gc_graph_prepare(gc_graph *g) {
         uint64_t rows = 0;
         for (uint32_t i = 0; i < n_hubs; i++) {
             const uint32_t d = hp[2 * idx[i] + 1];
-            if (d < thr || rows + d + 2 > GC_GIANT_MAX_ROWS) break;
+            if (d < thr || rows + d + 32 > GC_GIANT_MAX_ROWS) break;
             for (uint32_t r = 0; r < d; r += GC_GIANT_TASK) {
                 tasks.push_back(i);
                 tasks.push_back(r);
             }
-            rows += ((uint64_t)d + 1) & ~1ull;
+            rows += ((uint64_t)d + 31) & ~31ull;
             gw.push_back((uint32_t)rows);
             g->n_giant++;
         }

@@ -369,36 +369,385 @@ __device__ int color_one_v(const uint32_t *__restrict__ list, uint32_t cnt, cons
 // or done, so the oldest unfinished ticket always progresses.
 // Ticket records: rec[t] = (vertex, first CSR entry, predecessor count) of ticket t, so that a
 // warp needs one 16-byte load per ticket instead of the order -> V, pc chain.
+// With `rank` set, the tickets below kmax (the cluster-colored core) also record rank[u] = t.
 __global__ void k_jp_records(const uint32_t *__restrict__ order, const uint32_t *__restrict__ V,
-                             const uint32_t *__restrict__ pc, const DevState *st, uint4 *__restrict__ rec) {
+                             const uint32_t *__restrict__ pc, const DevState *st, uint4 *__restrict__ rec,
+                             uint32_t *__restrict__ rank, uint32_t kmax) {
     const uint32_t n = st->ordered;
     for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
         const uint32_t u = order[t];
         rec[t] = make_uint4(u, V[u], pc[u], 0u);
+        if (rank && t < kmax) rank[u] = t;
     }
+}
+
+// ---- the dense core: the first tickets, colored inside one thread-block cluster --------------------
+//
+// On power-law graphs the priority DAG's long chains lie almost all among the highest-priority inner
+// vertices (R-MAT 22, GNN3 keys: depth 2,683 in all, yet depth 2,000 is reached by ticket 8,422, and
+// with the first 32,768 tickets colored the rest is only 214 deep).  Through global memory every
+// link of a chain costs a store-to-poll round trip in L2 (about 1 us), so these tickets bound the
+// whole kernel.  Here one cluster colors tickets [0, K) with every color exchanged through
+// distributed shared memory instead:
+//   - each CTA holds a replica of the K core colors (16 bits each) in its shared memory;
+//   - ticket t belongs to warp (t / C) % W of CTA t % C; a warp takes its tickets in order, so it
+//     waits only on smaller tickets (held by other warps or done) and the oldest unfinished ticket
+//     always progresses;
+//   - the owner writes a color into all C replicas (lane i stores into CTA i) and to global memory;
+//     waiting warps poll their own replica;
+//   - a core vertex's predecessors are sources (color 1, known before) or inner vertices with smaller
+//     tickets (core vertices): leaves precede nothing.  A pre-pass rewrites each core ticket's
+//     predecessor list in place as ticket ranks and records whether a source is among them.
+// Waits are bounded (spin_limit polls; on expiry the error is raised and the warp publishes
+// 0xffff, which releases its successors).  A cluster barrier before exit keeps every CTA's shared
+// memory alive while others may still store into it.
+constexpr int CORE_WARPS = 16;                 // warps per CTA
+constexpr int CORE_PEND = 256;                 // per warp: uncolored predecessors remembered for polling
+constexpr uint32_t CORE_MAX = 32768;           // most core tickets (16-bit ranks, 64 KB replica)
+
+__device__ __forceinline__ unsigned int cluster_rank() {
+    unsigned int r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+__device__ __forceinline__ unsigned int cluster_size() {
+    unsigned int r;
+    asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(r));
+    return r;
+}
+__device__ __forceinline__ void cluster_sync_all() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+__device__ __forceinline__ unsigned int core_ld(const unsigned short *p) {
+    unsigned short v;
+    asm volatile("ld.relaxed.cluster.shared::cta.u16 %0, [%1];"
+                 : "=h"(v)
+                 : "r"((unsigned int)__cvta_generic_to_shared(p))
+                 : "memory");
+    return v;
+}
+// Stores v into CTA `rank`'s copy of the replica element p.
+__device__ __forceinline__ void core_st_remote(const unsigned short *p, unsigned int rank, unsigned short v) {
+    unsigned int remote;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;"
+                 : "=r"(remote)
+                 : "r"((unsigned int)__cvta_generic_to_shared(p)), "r"(rank));
+    asm volatile("st.relaxed.cluster.shared::cluster.u16 [%0], %1;" ::"r"(remote), "h"(v) : "memory");
+}
+
+// Pre-pass, one warp per core ticket t < K: the predecessor list P[first, first + count) becomes the
+// ranks of its inner predecessors (compacted in place, CSR order kept), rec[t].z their number and
+// rec[t].w = 1 when a source (color 1 from the split) is among the predecessors.
+__global__ void __launch_bounds__(256) k_jp_core_lists(uint4 *__restrict__ rec, uint32_t *__restrict__ P,
+                                                       const uint32_t *__restrict__ rank, const int *__restrict__ color,
+                                                       const DevState *st, uint32_t kmax) {
+    const uint32_t K = min(st->ordered, kmax);
+    const int lane = threadIdx.x & 31;
+    const unsigned int lt = (1u << lane) - 1u;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < K; t += nwarps) {
+        const uint4 r = rec[t];
+        uint32_t cnt = 0;
+        bool source = false;
+        for (uint32_t j0 = 0; j0 < r.z; j0 += 32) {
+            const uint32_t j = j0 + lane;
+            uint32_t rk = 0;
+            bool inner = false;
+            if (j < r.z) {
+                const uint32_t v = P[r.y + j];
+                if (color[v] == 1) source = true;
+                else inner = true, rk = rank[v];
+            }
+            const unsigned int m = __ballot_sync(0xffffffffu, inner);
+            __syncwarp();  // every lane has read its entry before any is overwritten
+            if (inner) P[r.y + cnt + __popc(m & lt)] = rk;
+            cnt += __popc(m);
+        }
+        const bool any_source = __any_sync(0xffffffffu, source);
+        if (lane == 0) rec[t] = make_uint4(r.x, r.y, cnt, any_source ? 1u : 0u);
+    }
+}
+
+// Marks color c (>= 1) in the warp's 1,024-color window bitmap.
+__device__ __forceinline__ void core_mark(uint32_t *fb, unsigned int c, uint32_t window) {
+    const uint32_t idx = c - 1u - window * WINDOW;
+    if (idx < WINDOW) atomicOr(&fb[idx >> 5], 1u << (idx & 31));
+}
+
+__global__ void __launch_bounds__(CORE_WARPS * 32, 1) k_jp_core(const uint4 *__restrict__ rec,
+                                                                const uint32_t *__restrict__ P, int *color,
+                                                                DevState *st, unsigned int spin_limit,
+                                                                uint32_t kmax) {
+    extern __shared__ __align__(16) unsigned char core_smem[];
+    unsigned short *replica = reinterpret_cast<unsigned short *>(core_smem);                   // kmax
+    uint32_t *fb_all = reinterpret_cast<uint32_t *>(core_smem + 2 * (size_t)kmax);            // W x 32
+    unsigned short *pend_all = reinterpret_cast<unsigned short *>(fb_all + CORE_WARPS * 32);  // W x CORE_PEND
+    const uint32_t K = min(ld_relaxed_u32(&st->ordered), kmax);
+    for (uint32_t i = threadIdx.x; i < K; i += blockDim.x) replica[i] = 0;
+    cluster_sync_all();  // every replica is zeroed before any remote store
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const unsigned int C = cluster_size(), me = cluster_rank();
+    uint32_t *fb = fb_all + warp * 32;
+    unsigned short *pend = pend_all + warp * CORE_PEND;
+    const uint32_t stride = C * CORE_WARPS;
+    for (uint32_t t = (uint32_t)warp * C + me; t < K; t += stride) {
+        const uint4 r = rec[t];
+        const uint32_t *list = P + r.y;
+        const uint32_t cnt = r.z;
+        int result = -1;
+        bool gave_up = false;
+        for (uint32_t window = 0; result < 0 && !gave_up; window++) {
+            fb[lane] = 0;
+            __syncwarp();
+            if (r.w && window == 0 && lane == 0) core_mark(fb, 1u, 0);
+            uint32_t npend = 0;  // warp-uniform
+            for (uint32_t j0 = 0; j0 < cnt; j0 += 32) {
+                const uint32_t j = j0 + lane;
+                const uint32_t rk = j < cnt ? __ldg(list + j) : 0xffffffffu;
+                const unsigned int c = rk != 0xffffffffu ? core_ld(replica + rk) : 0xffffffffu;
+                if (c != 0 && c != 0xffffffffu) core_mark(fb, c, window);
+                const unsigned int zero = __ballot_sync(0xffffffffu, c == 0);
+                if (zero) {
+                    const uint32_t slot = npend + __popc(zero & ((1u << lane) - 1u));
+                    if (c == 0) {
+                        if (slot < CORE_PEND) {
+                            pend[slot] = (unsigned short)rk;
+                        } else {  // list full: wait in place
+                            unsigned int spins = 0, cc;
+                            while ((cc = core_ld(replica + rk)) == 0) {
+                                if (++spins > spin_limit || ((spins & 1023u) == 0 && ld_relaxed_u32(&st->err))) {
+                                    gave_up = true;
+                                    break;
+                                }
+                            }
+                            if (!gave_up) core_mark(fb, cc, window);
+                        }
+                    }
+                    npend = min((uint32_t)CORE_PEND, npend + __popc(zero));
+                }
+            }
+            __syncwarp();
+            // poll the pending entries in the local replica
+            unsigned int spins = 0;
+            for (;;) {
+                bool left = false;
+                for (uint32_t i = lane; i < npend && !gave_up; i += 32) {
+                    const unsigned int rk = pend[i];
+                    if (rk == 0xffffu) continue;
+                    const unsigned int cc = core_ld(replica + rk);
+                    if (cc) {
+                        core_mark(fb, cc, window);
+                        pend[i] = 0xffffu;
+                    } else {
+                        left = true;
+                    }
+                }
+                if (!__any_sync(0xffffffffu, left || gave_up)) break;
+                if (++spins > spin_limit || ((spins & 1023u) == 0 && ld_relaxed_u32(&st->err))) gave_up = true;
+                if (__any_sync(0xffffffffu, gave_up)) break;
+            }
+            gave_up = __any_sync(0xffffffffu, gave_up);
+            if (gave_up) break;
+            __syncwarp();
+            const int m = window_mex(fb, lane, window);
+            __syncwarp();
+            if (m) result = m;
+        }
+        const unsigned short pub = gave_up ? (unsigned short)0xffffu : (unsigned short)result;
+        if ((unsigned int)lane < C) core_st_remote(replica + t, (unsigned int)lane, pub);
+        if (lane == 0) {
+            if (gave_up) raise_error(st, ERR_WAIT_EXPIRED, r.x);
+            st_relaxed(color + r.x, gave_up ? -1 : result);
+        }
+        __syncwarp();
+    }
+    cluster_sync_all();  // no CTA leaves while another may still store into its replica
+}
+
+// ---- after the core: a heavy and a light stream --------------------------------------------------
+//
+// Past the core the DAG is shallow and the ticket kernel is bound by how many vertices are in flight
+// (about 1.7 us from ticket to color, most of it three dependent loads).  Most of these vertices
+// have few predecessors, so they are split off: tickets with at most LIGHT_MAX predecessors form the
+// light stream, colored one vertex per lane (32 per warp), the others the heavy stream, one vertex
+// per warp as before.  Both streams keep the priority order, and each has warps of its own, so the
+// oldest unfinished vertex of either stream is always held by a running warp and all its
+// predecessors are done: the kernel always progresses.
+constexpr uint32_t LIGHT_MAX = 63;   // a light vertex's color is at most 64: one 64-bit mask
+constexpr uint32_t PART_TILE = 1024;
+
+// Heavy tickets per tile of the tickets after the core, [first, n).
+__global__ void __launch_bounds__(PART_TILE) k_jp_part_count(const uint4 *__restrict__ rec, const DevState *st,
+                                                             uint32_t core, uint32_t *__restrict__ tile_heavy) {
+    __shared__ uint32_t warp_cnt[PART_TILE / 32];
+    const uint32_t n = st->ordered, first = min(n, core);
+    const uint32_t t = first + blockIdx.x * PART_TILE + threadIdx.x;
+    const bool heavy = t < n && rec[t].z > LIGHT_MAX;
+    const unsigned int m = __ballot_sync(0xffffffffu, heavy);
+    if ((threadIdx.x & 31) == 0) warp_cnt[threadIdx.x >> 5] = __popc(m);
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        const uint32_t c = warp_cnt[threadIdx.x];
+        const uint32_t tot = __reduce_add_sync(0xffffffffu, c);
+        if (threadIdx.x == 0) tile_heavy[blockIdx.x] = tot;
+    }
+}
+
+// Exclusive prefix of the tiles' heavy counts (in place), one CTA; the stream sizes into the state.
+__global__ void __launch_bounds__(1024) k_jp_part_scan(uint32_t *__restrict__ tile_heavy, uint32_t ntiles, DevState *st,
+                                                       uint32_t core) {
+    __shared__ uint32_t warp_sum[32];
+    __shared__ uint32_t carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (uint32_t base = 0; base < ntiles; base += 1024) {
+        const uint32_t i = base + threadIdx.x;
+        const uint32_t v = i < ntiles ? tile_heavy[i] : 0u;
+        uint32_t x = v;  // inclusive warp scan
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) warp_sum[warp] = x;
+        __syncthreads();
+        if (warp == 0) {
+            uint32_t w = warp_sum[lane], wx = w;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xffffffffu, wx, o);
+                if (lane >= o) wx += y;
+            }
+            warp_sum[lane] = wx - w;  // exclusive
+        }
+        __syncthreads();
+        const uint32_t c = carry;
+        if (i < ntiles) tile_heavy[i] = c + warp_sum[warp] + x - v;
+        __syncthreads();
+        if (threadIdx.x == 1023) carry = c + warp_sum[31] + x;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const uint32_t n = st->ordered, first = min(n, core);
+        st->n_heavy = carry;
+        st->n_light = n - first - carry;
+        st->ticket_light = 0;
+    }
+}
+
+// Stable split: heavy tickets to out[0, n_heavy) in order, light tickets to out[cap - 1 - i] for the
+// i-th light ticket (the light stream is read from the top down).
+__global__ void __launch_bounds__(PART_TILE) k_jp_part_scatter(const uint4 *__restrict__ rec, const DevState *st,
+                                                               uint32_t core, const uint32_t *__restrict__ tile_heavy,
+                                                               uint4 *__restrict__ out, uint32_t cap) {
+    __shared__ uint32_t warp_off[PART_TILE / 32];
+    const uint32_t n = st->ordered, first = min(n, core);
+    const uint32_t tile0 = first + blockIdx.x * PART_TILE;
+    const uint32_t t = tile0 + threadIdx.x;
+    const bool valid = t < n;
+    const uint4 r = valid ? rec[t] : make_uint4(0u, 0u, 0u, 0u);
+    const bool heavy = valid && r.z > LIGHT_MAX;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const unsigned int m = __ballot_sync(0xffffffffu, heavy);
+    if (lane == 0) warp_off[warp] = __popc(m);
+    __syncthreads();
+    if (warp == 0) {
+        const uint32_t w = warp_off[lane];
+        uint32_t x = w;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        warp_off[lane] = x - w;
+    }
+    __syncthreads();
+    if (!valid) return;
+    const uint32_t heavy_before = tile_heavy[blockIdx.x] + warp_off[warp] + __popc(m & ((1u << lane) - 1u));
+    if (heavy) out[heavy_before] = r;
+    else out[cap - 1u - ((t - first) - heavy_before)] = r;
+}
+
+// Light stream, one vertex per lane: the predecessors' colors go into a 64-bit mask (a light vertex
+// has at most 63 predecessors, so its color is at most 64); uncolored ones are remembered by their
+// list position and re-read until colored (bounded; growing sleeps).  Returns -1 on expiry.
+__device__ __forceinline__ int color_light(const uint32_t *__restrict__ list, uint32_t cnt, const int *color,
+                                           DevState *st, unsigned int spin_limit, unsigned int nap) {
+    unsigned long long used = 0, pend = 0;  // colors 1..64 taken; list positions still uncolored
+    for (uint32_t j = 0; j < cnt; j++) {
+        const int c = ld_relaxed(color + __ldg(list + j));
+        if (c > 0 && c <= 64) used |= 1ull << (c - 1);
+        else if (c == 0) pend |= 1ull << j;  // (-1: a predecessor whose wait failed; the error is raised)
+    }
+    unsigned int spins = 0;
+    while (pend) {
+        bool progress = false;
+        unsigned long long w = pend;
+        while (w) {
+            const int j = __ffsll((long long)w) - 1;
+            w &= w - 1;
+            const int c = ld_relaxed(color + __ldg(list + j));
+            if (c) {
+                if (c > 0 && c <= 64) used |= 1ull << (c - 1);
+                pend &= ~(1ull << j);
+                progress = true;
+            }
+        }
+        if (pend && !progress) {
+            if (++spins > spin_limit || ((spins & 255u) == 0 && ld_relaxed_u32(&st->err))) return -1;
+            if (spins > 32) __nanosleep(spins > 512 ? 4 * nap : nap);
+        }
+    }
+    return __ffsll((long long)~used);  // at most 63 bits are set: a free color <= 64 exists
 }
 
 // A warp takes its next ticket only when it is free: a ticket held ahead by a warp still waiting on
 // its current vertex would stall every vertex that waits on the held one (measured several times
 // slower on R-MAT 22).
+// Without a split (split == nullptr) every warp takes tickets of rec in order.  With a split, the
+// CTA's first COLOR_WARPS_PER_CTA - light_warps warps take the heavy stream split[0, n_heavy) one
+// vertex each (ticket counter st->ticket, from 0), the others the light stream -- split[cap - 1 - i],
+// i < n_light -- 32 vertices at a time, one per lane (counter st->ticket_light).
 __global__ void __launch_bounds__(COLOR_WARPS_PER_CTA * 32, 2) k_jp_color(const uint4 *__restrict__ rec,
                                                                        const uint32_t *__restrict__ P,
                                                                        const uint32_t *__restrict__ pc, int *color,
                                                                        DevState *st, unsigned int spin_limit,
                                                                        unsigned int tight, unsigned int nap,
                                                                        unsigned long long *fmask,
-                                                                       const unsigned long long *epoch_word) {
+                                                                       const unsigned long long *epoch_word,
+                                                                       const uint4 *__restrict__ split, uint32_t cap,
+                                                                       int light_warps) {
     __shared__ uint32_t forbid[COLOR_WARPS_PER_CTA][32];
     __shared__ uint32_t pending[COLOR_WARPS_PER_CTA][PENDING];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const uint32_t n = ld_relaxed_u32(&st->ordered);
     const uint32_t epoch = fmask ? (uint32_t)*epoch_word : 0u;
+    if (split && warp >= COLOR_WARPS_PER_CTA - light_warps) {
+        const uint32_t nl = ld_relaxed_u32(&st->n_light);
+        for (;;) {
+            uint32_t t0 = 0;
+            if (lane == 0) t0 = atomicAdd(&st->ticket_light, 32u);
+            t0 = __shfl_sync(0xffffffffu, t0, 0);
+            if (t0 >= nl) break;
+            const uint32_t i = t0 + lane;
+            if (i < nl) {
+                const uint4 r = split[cap - 1u - i];
+                const int c = color_light(P + r.y, r.z, color, st, spin_limit, nap);
+                if (c < 0) raise_error(st, ERR_WAIT_EXPIRED, r.x);
+                st_relaxed(color + r.x, c);  // -1 on error is non-zero: successors stop waiting
+            }
+            __syncwarp();
+        }
+        return;
+    }
+    const uint4 *src = split ? split : rec;
+    const uint32_t n = split ? ld_relaxed_u32(&st->n_heavy) : ld_relaxed_u32(&st->ordered);
     for (;;) {
         uint32_t t = 0;
         if (lane == 0) t = atomicAdd(&st->ticket, 1u);
         t = __shfl_sync(0xffffffffu, t, 0);
         if (t >= n) break;
-        const uint4 r = rec[t];
+        const uint4 r = src[t];
         const uint32_t u = r.x;
         const int c = color_one_v(P + r.y, r.z, color, forbid[warp], pending[warp], lane, st, spin_limit, tight, nap,
                                   pc, fmask, epoch, u);
@@ -600,13 +949,79 @@ __global__ void k_keys_from_colors(const int *__restrict__ color, uint32_t N, ui
 }
 
 // Also advances the epoch of the published forbidden colors (never 0: the buffer starts zeroed).
-__global__ void k_reset_ticket(DevState *st, unsigned long long *epoch_word) {
-    st->ticket = 0;
+// The ordered kernel's first ticket: past the core tickets the cluster colored (first_cap of them
+// at most), else 0.
+__global__ void k_reset_ticket(DevState *st, unsigned long long *epoch_word, uint32_t first_cap = 0) {
+    st->ticket = min(st->ordered, first_cap);
     st->big_leaves = 0;
     if (epoch_word) {
         const unsigned long long e = (*epoch_word + 1) & 0xffffffffull;
         *epoch_word = e ? e : 1;
     }
+}
+
+size_t core_smem_bytes(uint32_t kmax) {
+    return 2 * (size_t)kmax + sizeof(uint32_t) * CORE_WARPS * 32 + sizeof(unsigned short) * CORE_WARPS * CORE_PEND;
+}
+
+// Once per context: the core kernel's cluster size -- 16 CTAs (a non-portable size) when the device
+// can place such a cluster with this kernel's shared memory, else 8, else 0 (no core phase).
+gc_status core_cluster_config(gc_ctx *ctx) {
+    if (ctx->jp_core_cluster >= 0) return GC_OK;
+    ctx->jp_core_cluster = 0;
+    const size_t smem = core_smem_bytes(CORE_MAX);
+    gc_status s = gc_check_cuda(ctx, cudaFuncSetAttribute(k_jp_core, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                                "core smem");
+    if (s != GC_OK) return s;
+    if (cudaFuncSetAttribute(k_jp_core, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)
+        cudaGetLastError();
+    for (int C : {16, 8}) {
+        cudaLaunchConfig_t cfg = {};
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = C;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.gridDim = dim3(C);
+        cfg.blockDim = dim3(CORE_WARPS * 32);
+        cfg.dynamicSmemBytes = smem;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        int n = 0;
+        if (cudaOccupancyMaxActiveClusters(&n, k_jp_core, &cfg) != cudaSuccess) {
+            cudaGetLastError();
+            continue;
+        }
+        if (n >= 1) {
+            ctx->jp_core_cluster = C;
+            break;
+        }
+    }
+    return GC_OK;
+}
+
+gc_status launch_core(gc_ctx *ctx, gc_graph *g, uint32_t kmax) {
+    const int C = ctx->jp_core_cluster;
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = C;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3(C);
+    cfg.blockDim = dim3(CORE_WARPS * 32);
+    cfg.dynamicSmemBytes = core_smem_bytes(kmax);
+    cfg.stream = ctx->stream;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    const uint4 *rec = g->jprec;
+    const uint32_t *P = g->P;
+    int *color = g->color;
+    DevState *st = ctx->dstate;
+    const unsigned int spin = ctx->spin_limit;
+    gc_status s = gc_check_cuda(ctx, cudaLaunchKernelEx(&cfg, k_jp_core, rec, P, color, st, spin, kmax), "jp core");
+    ctx->launches++;
+    return s;
 }
 
 int bit_length(uint64_t x) {
@@ -730,8 +1145,20 @@ gc_status gc_jp_color(gc_graph *g) {
     }
 
     if ((s = gc_alloc(ctx, &g->jprec, g->cap_N, "ticket records")) != GC_OK) return s;
-    k_jp_records<<<ctx->num_sms * 4, 256, 0, ctx->stream>>>(g->order, g->V, g->pc, ctx->dstate, g->jprec);
+    uint32_t core = 0;  // core tickets colored in one cluster (at most)
+    if (ctx->jp_core_max && (s = core_cluster_config(ctx)) == GC_OK && ctx->jp_core_cluster > 0) core = ctx->jp_core_max;
+    if (s != GC_OK) return s;
+    if (core && (s = gc_alloc(ctx, &g->rank, g->cap_N, "core ranks")) != GC_OK) return s;
+    k_jp_records<<<ctx->num_sms * 4, 256, 0, ctx->stream>>>(g->order, g->V, g->pc, ctx->dstate, g->jprec,
+                                                            core ? g->rank : nullptr, core);
     ctx->launches++;
+    if (core) {
+        ProfScope ps(ctx, "jp_core", ctx->stream);
+        k_jp_core_lists<<<ctx->num_sms * 8, 256, 0, ctx->stream>>>(g->jprec, g->P, g->rank, g->color, ctx->dstate,
+                                                                   core);
+        ctx->launches++;
+        if ((s = launch_core(ctx, g, core)) != GC_OK) return s;
+    }
 
     // 3. ordered coloring
     int &occupancy = ctx->color_blocks_per_sm;
@@ -746,12 +1173,29 @@ gc_status gc_jp_color(gc_graph *g) {
     const int blocks = (want > 0 && want < occupancy) ? want : occupancy;
     const unsigned int tight = g->jp_ctas > 0 ? g->jp_tight : ctx->jp_tight;
     const unsigned int nap = g->jp_ctas > 0 ? g->jp_nap : ctx->jp_nap;
-    k_reset_ticket<<<1, 1, 0, ctx->stream>>>(ctx->dstate, epoch_word);
+    // the tickets after the core as a heavy and a light stream (light_warps warps per CTA take the light one)
+    const int light_warps = ctx->jp_light_warps;
+    uint4 *split = nullptr;
+    if (light_warps > 0 && light_warps < COLOR_WARPS_PER_CTA) {
+        const uint32_t ntiles = (N + PART_TILE - 1) / PART_TILE;
+        if ((s = gc_alloc(ctx, &g->jpsplit, g->cap_N, "ticket streams")) != GC_OK) return s;
+        if ((s = gc_alloc(ctx, &g->part_tiles, (g->cap_N + PART_TILE - 1) / PART_TILE, "ticket stream tiles")) != GC_OK)
+            return s;
+        ProfScope ps(ctx, "jp_streams", ctx->stream);
+        k_jp_part_count<<<ntiles, PART_TILE, 0, ctx->stream>>>(g->jprec, ctx->dstate, core, g->part_tiles);
+        k_jp_part_scan<<<1, 1024, 0, ctx->stream>>>(g->part_tiles, ntiles, ctx->dstate, core);
+        k_jp_part_scatter<<<ntiles, PART_TILE, 0, ctx->stream>>>(g->jprec, ctx->dstate, core, g->part_tiles, g->jpsplit,
+                                                                 g->cap_N);
+        ctx->launches += 3;
+        split = g->jpsplit;
+    }
+    k_reset_ticket<<<1, 1, 0, ctx->stream>>>(ctx->dstate, epoch_word, split ? 0u : core);
     ctx->launches++;
     {
         ProfScope ps(ctx, "jp_color", ctx->stream);
         k_jp_color<<<ctx->num_sms * blocks, COLOR_WARPS_PER_CTA * 32, 0, ctx->stream>>>(
-            g->jprec, g->P, g->pc, g->color, ctx->dstate, ctx->spin_limit, tight, nap, fmask, epoch_word);
+            g->jprec, g->P, g->pc, g->color, ctx->dstate, ctx->spin_limit, tight, nap, fmask, epoch_word, split,
+            g->cap_N, light_warps);
         ctx->launches++;
     }
     // 4. leaves

@@ -16,6 +16,9 @@
 //             fits in what the budget has left.  Such jobs start in arrival order (one blocked by
 //             the budget holds back the later ones, so none starves); small jobs never wait on
 //             the budget.  A job that could never fit is refused at submission (GC_ERR_BUDGET).
+//             With two or more lanes, at most lanes - 1 of them run such jobs at a time: one lane
+//             always stays for small jobs, whose latency would otherwise queue behind seconds of
+//             large-graph work.
 //   batching  continuous: an idle lane takes the oldest pending job; if it is small, the lane also
 //             takes every other pending small job of the same class (heuristic, layers, recolor)
 //             that still fits its slot, and colors them all in one gc_batch_color_once pass.  Jobs
@@ -114,6 +117,7 @@ struct gc_server {
     uint64_t next_id = 1;
     uint64_t reserved = 0, peak_reserved = 0;
     bool large_blocked = false;  // set during a pick when the oldest large job did not fit
+    uint32_t large_running = 0;  // lanes running a job alone
     bool stop = false;
     bool started = false;        // first submission seen (models are fixed from then on)
     uint32_t inflight = 0;       // jobs taken by lanes and not yet complete
@@ -156,6 +160,7 @@ Work pick_work(gc_server *s) {
                 continue;
             }
             if (large_seen_blocked) continue;  // later large jobs wait behind the blocked one
+            if (c.lanes > 1 && s->large_running >= c.lanes - 1) continue;  // a lane stays for small jobs
             if (s->reserved + j->bytes <= c.hbm_budget) {
                 w.jobs.push_back(j);
                 break;
@@ -186,6 +191,7 @@ Work pick_work(gc_server *s) {
         if (!w.batch) {
             s->reserved += w.jobs[0]->bytes;
             s->peak_reserved = std::max(s->peak_reserved, s->reserved);
+            s->large_running++;
         }
     }
     return w;
@@ -391,7 +397,10 @@ void lane_loop(gc_server *s, Lane *L) {
         lk.lock();
         const uint32_t n = (uint32_t)w.jobs.size();
         for (size_t i = 0; i < w.jobs.size(); i++) complete(s, w.jobs[i], status[i], colors[i], n, errors[i]);
-        if (!w.batch) s->reserved -= w.jobs[0]->bytes;
+        if (!w.batch) {
+            s->reserved -= w.jobs[0]->bytes;
+            s->large_running--;
+        }
         s->inflight -= n;
         s->cv_done.notify_all();
         s->cv_work.notify_all();  // budget freed, or more work may be pending

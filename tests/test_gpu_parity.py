@@ -112,6 +112,96 @@ def test_mesh_graphs_culberson(gpu_ctx, golden, models):
         assert np.array_equal(g.colors(), O.culberson(N, V, E, co, 9))
 
 
+def _star(n):
+    """Vertex 0 joined to all others: one hub of n - 1 neighbours whose layer-0 id features
+    (v / n, dyadic for n a power of two) make exact rounding ties in its FP32 sum."""
+    V = np.concatenate([[0, n - 1], np.arange(n, 2 * n - 1)]).astype(np.uint32)
+    E = np.concatenate([np.arange(1, n), np.zeros(n - 1)]).astype(np.uint32)
+    return n, V, E
+
+
+def _one_graph_batch_priorities(ctx, graph, model, hub_degree):
+    t = gcn.default_tuning()
+    t.hub_degree = hub_degree
+    t.warp_degree = min(t.warp_degree, hub_degree)
+    b = gcn.Batch(ctx, graphs=[graph])
+    b.tuning = t
+    b.color("GNN", model)
+    p, c = b.priorities(), b.colors()
+    b.close()
+    return p, c
+
+
+@pytest.mark.parametrize("L", [2, 3, 4])
+def test_giant_hub_path_matches_oracle(gpu_ctx, golden, models, L):
+    """Hubs with at least max(2 x hub degree, largest degree / 3) neighbours are summed by the
+    exact binade-step evaluation of the FP32 chain.  Lowering the hub degree sends many vertices
+    of small graphs there; every priority must still equal the oracle's bit for bit."""
+    params, md = golden.model(L)
+    graphs = [gcn.gen_rmat(1 << 15, 16, 9), _star(1 << 17), _star(100000), gcn.gen_er(20000, 400000, 4)]
+    for graph in graphs:
+        N, V, E = graph
+        p_ref = O.ordering("GNN", N, V, E, params, md)
+        c_ref, _ = O.greedy_color(N, V, E, p_ref)
+        for hub in (64, 1024):
+            p, c = _one_graph_batch_priorities(gpu_ctx, graph, models[L], hub)
+            assert np.array_equal(p, p_ref), (N, hub, "priorities")
+            assert np.array_equal(c, c_ref), (N, hub, "colors")
+
+
+def test_giant_threshold_setting(golden):
+    """GC_GNN_GIANT_DEGREE moves hubs between the CTA path and the exact column path; R-MAT 18's
+    hubs (up to 25,119 neighbours) through either give the oracle's priorities."""
+    N, V, E = gcn.gen_rmat(1 << 18, 16, 2)
+    params, md = golden.model(3)
+    p_ref = O.ordering("GNN", N, V, E, params, md)
+    for giant in ("17000", "1000000"):
+        ctx = _ctx_with({"GC_GNN_GIANT_DEGREE": giant})
+        m = gcn.Model(ctx, params, md)
+        g = gcn.Graph(ctx, N, V, E)
+        g.priority("GNN", m)
+        assert np.array_equal(g.priorities(), p_ref), giant
+        g.close()
+        m.close()
+        ctx.close()
+
+
+def _ctx_with(env: dict):
+    old = {k: os.environ.get(k) for k in env}
+    os.environ.update(env)
+    try:
+        return gcn.Context(int(os.environ.get("GC_DEVICE", "0")))
+    finally:
+        for k, v in old.items():
+            if v is None:
+                del os.environ[k]
+            else:
+                os.environ[k] = v
+
+
+@pytest.mark.parametrize("core", ["0", "64", "5000", "32768"])
+def test_jp_core_sizes_give_the_oracle_colors(golden, core):
+    """The first GC_JP_CORE tickets are colored inside one thread-block cluster (colors exchanged
+    through distributed shared memory), the rest by the ticket kernel: any split gives the greedy
+    coloring of the priorities, for float (GNN) and integer (LF) keys and after Culberson rounds."""
+    ctx = _ctx_with({"GC_JP_CORE": core})
+    params, md = golden.model(3)
+    m = gcn.Model(ctx, params, md)
+    for N, V, E in (gcn.gen_rmat(1 << 17, 16, 2), gcn.gen_er(30000, 300000, 8)):
+        g = gcn.Graph(ctx, N, V, E)
+        for heur in ("GNN", "LF"):
+            g.priority(heur, m if heur == "GNN" else None)
+            g.color()
+            p = g.priorities()
+            c_ref, _ = O.greedy_color(N, V, E, p)
+            assert np.array_equal(g.colors(), c_ref), (core, N, heur)
+        g.recolor(2)
+        assert np.array_equal(g.colors(), O.culberson(N, V, E, c_ref, 2)), (core, N)
+        g.close()
+    m.close()
+    ctx.close()
+
+
 def test_user_priorities(gpu_ctx):
     N, V, E = gcn.gen_rmat(1 << 12, 8, 21)
     rng = np.random.default_rng(0)
