@@ -479,8 +479,8 @@ __global__ void __launch_bounds__(CORE_WARPS * 32, 1) k_jp_core(const uint4 *__r
                                                                 DevState *st, unsigned int spin_limit,
                                                                 uint32_t kmax) {
     extern __shared__ __align__(16) unsigned char core_smem[];
-    unsigned short *replica = reinterpret_cast<unsigned short *>(core_smem);                   // kmax
-    uint32_t *fb_all = reinterpret_cast<uint32_t *>(core_smem + 2 * (size_t)kmax);            // W x 32
+    unsigned short *replica = reinterpret_cast<unsigned short *>(core_smem);  // kmax, rounded up to 8
+    uint32_t *fb_all = reinterpret_cast<uint32_t *>(core_smem + 2 * (size_t)((kmax + 7u) & ~7u));  // W x 32
     unsigned short *pend_all = reinterpret_cast<unsigned short *>(fb_all + CORE_WARPS * 32);  // W x CORE_PEND
     const uint32_t K = min(ld_relaxed_u32(&st->ordered), kmax);
     for (uint32_t i = threadIdx.x; i < K; i += blockDim.x) replica[i] = 0;
@@ -675,10 +675,19 @@ __global__ void __launch_bounds__(PART_TILE) k_jp_part_scatter(const uint4 *__re
 __device__ __forceinline__ int color_light(const uint32_t *__restrict__ list, uint32_t cnt, const int *color,
                                            DevState *st, unsigned int spin_limit, unsigned int nap) {
     unsigned long long used = 0, pend = 0;  // colors 1..64 taken; list positions still uncolored
-    for (uint32_t j = 0; j < cnt; j++) {
-        const int c = ld_relaxed(color + __ldg(list + j));
-        if (c > 0 && c <= 64) used |= 1ull << (c - 1);
-        else if (c == 0) pend |= 1ull << j;  // (-1: a predecessor whose wait failed; the error is raised)
+    constexpr int GROUP = 8;                // ids, then colors, GROUP at a time in flight
+    for (uint32_t j0 = 0; j0 < cnt; j0 += GROUP) {
+        uint32_t v[GROUP];
+        int c[GROUP];
+#pragma unroll
+        for (int k = 0; k < GROUP; k++) v[k] = j0 + k < cnt ? __ldg(list + j0 + k) : 0xffffffffu;
+#pragma unroll
+        for (int k = 0; k < GROUP; k++) c[k] = v[k] != 0xffffffffu ? ld_relaxed(color + v[k]) : -2;
+#pragma unroll
+        for (int k = 0; k < GROUP; k++) {
+            if (c[k] > 0 && c[k] <= 64) used |= 1ull << (c[k] - 1);
+            else if (c[k] == 0) pend |= 1ull << (j0 + k);  // (-1: a predecessor whose wait failed; raised)
+        }
     }
     unsigned int spins = 0;
     while (pend) {
@@ -961,7 +970,8 @@ __global__ void k_reset_ticket(DevState *st, unsigned long long *epoch_word, uin
 }
 
 size_t core_smem_bytes(uint32_t kmax) {
-    return 2 * (size_t)kmax + sizeof(uint32_t) * CORE_WARPS * 32 + sizeof(unsigned short) * CORE_WARPS * CORE_PEND;
+    return 2 * (size_t)((kmax + 7u) & ~7u) + sizeof(uint32_t) * CORE_WARPS * 32 +
+           sizeof(unsigned short) * CORE_WARPS * CORE_PEND;
 }
 
 // Once per context: the core kernel's cluster size -- 16 CTAs (a non-portable size) when the device

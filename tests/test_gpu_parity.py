@@ -58,6 +58,31 @@ def test_reference_models(gpu_ctx, golden, golden_ref):
             assert np.array_equal(g.colors(), golden_ref[f"{name}/GNN{L}/color"]), (name, L)
 
 
+def test_rmat22_gnn3_reference_model_matches_the_reference(gpu_ctx):
+    """The headline configuration at full size: R-MAT scale 22 (4.2 M vertices, 128 M directed
+    edges, hubs of up to 162,886 neighbours -- the giant-hub path, the cluster core and both ticket
+    streams all run), the reference's own models/m3.gnn.  Priorities (bit patterns) and colors
+    must equal the reference's gnn_internal_par on the same graph, run here on the host cores."""
+    if not (R.available() and R.has_models()):
+        pytest.skip("the compiled reference and its model files are not present (oracle/_ref)")
+    N, V, E = gcn.gen_rmat(1 << 22, 16, 2)
+    m = gcn.Model.load(gpu_ctx, os.path.join(R.MODELS, "m3.gnn"))
+    g = gcn.Graph(gpu_ctx, N, V, E)
+    g.priority("GNN", m)
+    count = g.color()
+    p, c = g.priorities(), g.colors()
+    g.close()
+    m.close()
+    R.set_threads(os.cpu_count() or 1)
+    job = R.GnnJob(N, V, E, 3)
+    c_ref = job.run()[:N].copy()
+    p_ref = job.p[:N].copy()
+    job.close()
+    assert np.array_equal(p.view(np.uint64), p_ref.view(np.uint64)), "GNN3 priorities differ from the reference"
+    assert np.array_equal(c, c_ref), "colors differ from the reference"
+    assert count == int(c_ref.max())
+
+
 def er65k():
     # the plain CPU-runnable configuration: ER n=65,536, 524,288 undirected edges, seed 1
     return gcn.gen_er(65536, 524288, 1)
@@ -179,12 +204,14 @@ def _ctx_with(env: dict):
                 os.environ[k] = v
 
 
-@pytest.mark.parametrize("core", ["0", "64", "5000", "32768"])
-def test_jp_core_sizes_give_the_oracle_colors(golden, core):
+@pytest.mark.parametrize("core,light", [("0", "0"), ("0", "2"), ("64", "2"), ("5000", "6"), ("32768", "0"),
+                                        ("32768", "2"), ("4097", "2")])
+def test_jp_core_sizes_give_the_oracle_colors(golden, core, light):
     """The first GC_JP_CORE tickets are colored inside one thread-block cluster (colors exchanged
-    through distributed shared memory), the rest by the ticket kernel: any split gives the greedy
-    coloring of the priorities, for float (GNN) and integer (LF) keys and after Culberson rounds."""
-    ctx = _ctx_with({"GC_JP_CORE": core})
+    through distributed shared memory), the rest by the ticket kernel, split into a heavy and a
+    light stream when GC_JP_LIGHT_WARPS > 0: any combination gives the greedy coloring of the
+    priorities, for float (GNN) and integer (LF) keys and after Culberson rounds."""
+    ctx = _ctx_with({"GC_JP_CORE": core, "GC_JP_LIGHT_WARPS": light})
     params, md = golden.model(3)
     m = gcn.Model(ctx, params, md)
     for N, V, E in (gcn.gen_rmat(1 << 17, 16, 2), gcn.gen_er(30000, 300000, 8)):
@@ -194,9 +221,9 @@ def test_jp_core_sizes_give_the_oracle_colors(golden, core):
             g.color()
             p = g.priorities()
             c_ref, _ = O.greedy_color(N, V, E, p)
-            assert np.array_equal(g.colors(), c_ref), (core, N, heur)
+            assert np.array_equal(g.colors(), c_ref), (core, light, N, heur)
         g.recolor(2)
-        assert np.array_equal(g.colors(), O.culberson(N, V, E, c_ref, 2)), (core, N)
+        assert np.array_equal(g.colors(), O.culberson(N, V, E, c_ref, 2)), (core, light, N)
         g.close()
     m.close()
     ctx.close()
