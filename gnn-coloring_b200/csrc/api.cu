@@ -119,8 +119,8 @@ void gc_graph_free_buffers(gc_graph *g) {
     void *bufs[] = {g->key,       g->color,  g->P,        g->pc,       g->order,    g->sort_buf, g->sort_hist,
                     g->big,       g->hubs,   g->x,        g->y,        g->t01,      g->deg_rem,  g->frontier,
                     g->frontier2, g->removed, g->leaf_list, g->vorder, g->rank,     g->p64,      g->seg_voff,
-                    g->seg_stat,  g->fmask,    g->giant,    g->hub_stage, g->jprec, g->class_first,
-                    g->gnn_ctr,   g->giant_aux, g->jpsplit, g->part_tiles};
+                    g->seg_stat,  g->fmask,    g->jprec, g->class_first,
+                    g->gnn_ctr,   g->hub_aux, g->jpsplit, g->part_tiles};
     for (void *p : bufs) gc_dev_free(ctx, p);
 }
 
@@ -284,16 +284,17 @@ gc_status gc_ctx_create(int device, gc_ctx **out) {
     if (const char *e = getenv("GC_JP_CLASSES")) ctx->jp_classes = atoi(e) != 0;
     if (const char *e = getenv("GC_JP_DECIDE")) ctx->jp_decide = atoi(e) != 0;
     if (const char *e = getenv("GC_JP_LIGHT_WARPS")) ctx->jp_light_warps = atoi(e);
+    if (const char *e = getenv("GC_GNN_HUB_SIDE")) ctx->gnn_hub_side = atoi(e) != 0;
+    if (const char *e = getenv("GC_GNN_HUB_CTAS")) ctx->gnn_hub_ctas_per_sm = std::max<uint32_t>(1u, (uint32_t)strtoul(e, nullptr, 10));
+    if (const char *e = getenv("GC_JP_CORE_BLOCK")) ctx->jp_core_block = std::max<uint32_t>(1u, (uint32_t)strtoul(e, nullptr, 10));
+    if (const char *e = getenv("GC_JP_CORE_NAP")) ctx->jp_core_nap = (unsigned int)strtoul(e, nullptr, 10);
     if (const char *e = getenv("GC_JP_CORE"))
         ctx->jp_core_max = std::min<uint32_t>((uint32_t)strtoul(e, nullptr, 10), 32768u);
     if (const char *e = getenv("GC_JP_NAP")) ctx->jp_nap = (unsigned int)strtoul(e, nullptr, 10);
     if (const char *e = getenv("GC_GNN_WARP_DEGREE")) ctx->gnn_warp_deg = (uint32_t)strtoul(e, nullptr, 10);
-    if (const char *e = getenv("GC_GNN_HUB_SMS")) ctx->gnn_hub_sms = atoi(e);
     if (const char *e = getenv("GC_GNN_GRAB")) ctx->gnn_grab = std::max<uint32_t>(1u, (uint32_t)strtoul(e, nullptr, 10));
     if (const char *e = getenv("GC_GNN_HEAVY")) ctx->gnn_heavy = (uint32_t)strtoul(e, nullptr, 10);
-    if (const char *e = getenv("GC_GNN_GIANT_DEGREE")) ctx->gnn_giant_deg = (uint32_t)strtoul(e, nullptr, 10);
     if (const char *e = getenv("GC_GNN_THIN_DEGREE")) ctx->gnn_thin_deg = (uint32_t)strtoul(e, nullptr, 10);
-    if (const char *e = getenv("GC_GNN_SERIAL")) ctx->gnn_serial = atoi(e) != 0;  // 1: hubs first, then the bulk
     if (s != GC_OK) {
         gc_ctx_destroy(ctx);
         return s;
@@ -317,10 +318,6 @@ static void ctx_release(gc_ctx *ctx) {
     if (--ctx->refs > 0) return;
     DeviceGuard dg(ctx);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
-    if (ctx->side_stream) {
-        cudaStreamSynchronize(ctx->side_stream);
-        cudaStreamDestroy(ctx->side_stream);
-    }
     for (auto &r : ctx->prof_recs) {
         cudaEventDestroy(r.a);
         cudaEventDestroy(r.b);
@@ -330,10 +327,14 @@ static void ctx_release(gc_ctx *ctx) {
         cudaStreamSynchronize(ctx->copy_stream);
         cudaStreamDestroy(ctx->copy_stream);
     }
-    if (ctx->ev_copy_fence) cudaEventDestroy(ctx->ev_copy_fence);
-    if (ctx->ev_copy_done) cudaEventDestroy(ctx->ev_copy_done);
+    if (ctx->hub_stream) {
+        cudaStreamSynchronize(ctx->hub_stream);
+        cudaStreamDestroy(ctx->hub_stream);
+    }
     if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
     if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
+    if (ctx->ev_copy_fence) cudaEventDestroy(ctx->ev_copy_fence);
+    if (ctx->ev_copy_done) cudaEventDestroy(ctx->ev_copy_done);
     if (ctx->dstate) cudaFree(ctx->dstate);
     if (ctx->hstate) cudaFreeHost(ctx->hstate);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -357,7 +358,7 @@ int gc_prof_read(gc_ctx *ctx, const char **names, double *total_ms, uint64_t *la
     if (!ctx) return 0;
     DeviceGuard dg(ctx);
     cudaStreamSynchronize(ctx->stream);
-    if (ctx->side_stream) cudaStreamSynchronize(ctx->side_stream);
+    if (ctx->hub_stream) cudaStreamSynchronize(ctx->hub_stream);
     std::vector<const char *> nm;
     std::vector<double> ms;
     std::vector<uint64_t> cnt;

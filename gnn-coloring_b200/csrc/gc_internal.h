@@ -17,8 +17,9 @@ struct gc_prof_rec {
     cudaEvent_t a, b;
 };
 
-// GNN layer tiers by neighbour count: a whole CTA above GC_GNN_HUB_DEGREE, one warp above
-// GC_GNN_WARP_DEGREE, four lanes otherwise.
+// Degree tiers: above GC_GNN_HUB_DEGREE a vertex is a hub (JP split tasks; in the GNN its neighbour
+// sums are evaluated exactly by whole warps before each layer); above GC_GNN_WARP_DEGREE the split
+// gives it a warp.
 constexpr uint32_t GC_GNN_HUB_DEGREE = 16384;
 constexpr uint32_t GC_GNN_WARP_DEGREE = 256;
 // The GNN layers' own warp tier (degree schedule): a warp stages 32 rows through shared memory, which
@@ -30,8 +31,11 @@ struct gc_ctx {
     int device = 0;
     int num_sms = 0;
     cudaStream_t stream = nullptr;
-    cudaStream_t side_stream = nullptr;  // GNN hub CTAs run here, overlapping the bulk of a layer
+    cudaStream_t hub_stream = nullptr;   // GNN: the hubs' kernel beside the layer kernel (high priority)
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    bool gnn_hub_side = false;           // GNN: hubs beside the layer kernel (GC_GNN_HUB_SIDE=1), else before it
+    uint32_t gnn_hub_ctas_per_sm = 2;    // GNN: persistent hub CTAs per SM (GC_GNN_HUB_CTAS)
+    bool hub_smem_set[3] = {false, false, false};  // hub kernels' shared-memory limit raised
     cudaStream_t copy_stream = nullptr;  // host copies that overlap work on `stream` (created on first use)
     cudaEvent_t ev_copy_fence = nullptr, ev_copy_done = nullptr;
     int color_blocks_per_sm = 0;         // resident CTAs of the coloring kernel (occupancy query)
@@ -42,16 +46,14 @@ struct gc_ctx {
     bool jp_classes = true;              // Culberson rounds: class by class instead of tickets
     uint32_t jp_core_max = 32768;        // coloring: first tickets colored inside one cluster (0: off; GC_JP_CORE)
     int jp_core_cluster = -1;            // CTAs of that cluster (16 or 8; 0: unavailable; -1: not yet queried)
+    uint32_t jp_core_block = 16;         // consecutive core tickets per CTA (GC_JP_CORE_BLOCK)
+    unsigned int jp_core_nap = 0;        // core kernel: sleep between polling rounds, ns (GC_JP_CORE_NAP)
     int jp_light_warps = 2;              // coloring: warps per CTA on the light stream (0: no split; GC_JP_LIGHT_WARPS)
     int gnn_blocks_per_sm[3] = {0, 0, 0};  // resident CTAs of each GNN layer kernel
     uint32_t gnn_warp_deg = GC_GNN_WIDE_DEGREE;  // GNN: above this many neighbours a vertex gets a warp
-    uint32_t gnn_giant_deg = 0;          // GNN: hubs with at least this many neighbours are staged (0: automatic)
     uint32_t gnn_thin_deg = 16;          // GNN: vertices with at most this many neighbours get one lane each
     uint32_t gnn_grab = 2;               // GNN counter hand-out: items per grab (GC_GNN_GRAB; 1-2 best, 8 +4 %, 16 +17 %)
     uint32_t gnn_heavy = 16384;          // GNN counter hand-out: leading four-lane items taken singly (GC_GNN_HEAVY)
-    int gnn_hub_sms = -1;                // GNN: SMs left to giant-hub CTAs (-1: one per giant hub, 0: none; GC_GNN_HUB_SMS)
-    bool gnn_serial = false;             // hub CTAs beside the bulk on a high-priority stream (GC_GNN_SERIAL=1: before it)
-    bool hub_smem_set[3] = {false, false, false};  // hub kernels' shared-memory limit raised
     cudaMemPool_t pool = nullptr;        // when set, graph buffers are stream-ordered allocations from this pool
     gc::DevState *dstate = nullptr;      // device status block
     gc::DevState *hstate = nullptr;      // pinned host mirror for read-back
@@ -79,13 +81,6 @@ struct ProfScope {
 // pass, this many edges per warp task.
 constexpr uint32_t GC_SPLIT_CHUNK = 1024;  // edges per warp task (shared-memory buffer per warp)
 constexpr int GC_JP_MASK_WORDS = 8;        // published forbidden colors: 8 x 32 = colors 1..256
-// Giant hubs: hubs with at least max(2 * hub degree, largest hub degree / 3) neighbours.  Before each
-// GNN layer all SMs copy these hubs' neighbour rows, in CSR order, into a staging buffer with one
-// column per feature (each hub's columns padded to a multiple of 32 rows); one warp per hub and
-// feature then evaluates the column's FP32 chain exactly, 1,024 values per step.  GC_GIANT_TASK rows
-// per gather task; at most GC_GIANT_MAX_ROWS rows.
-constexpr uint32_t GC_GIANT_TASK = 2048;
-constexpr uint64_t GC_GIANT_MAX_ROWS = 1ull << 25;
 
 struct gc_graph {
     gc_ctx *ctx = nullptr;
@@ -125,17 +120,8 @@ struct gc_graph {
     size_t big_cap = 0;              // words allocated for `big`
     uint32_t *hubs = nullptr;        // vertices with deg > GC_GNN_HUB_DEGREE, by descending degree
     uint32_t n_hubs = 0;
-    // the leading n_giant hubs are giant: giant[0..n_giant] their staging row offsets (multiples of
-    // 32: hub h's 16 columns start at 16 * giant[h] floats and are giant[h + 1] - giant[h] rows
-    // long), then n_giant_tasks (hub slot, first row) gather tasks
-    uint32_t n_giant = 0, n_giant_tasks = 0;
-    uint32_t *giant = nullptr;
-    size_t giant_cap = 0;            // words allocated for `giant`
-    uint64_t giant_rows = 0;         // staging rows
-    float *hub_stage = nullptr;      // GNN: giant_rows x 16 floats, feature columns (allocated on first use)
-    uint64_t hub_stage_rows = 0;
-    uint32_t *giant_aux = nullptr;   // GNN: per giant hub 16 feature sums, then one completion counter each
-    size_t giant_aux_cap = 0;
+    uint32_t *hub_aux = nullptr;     // GNN: per hub 16 feature sums, then one completion counter each
+    size_t hub_aux_cap = 0;
     uint32_t *gnn_ctr = nullptr;     // GNN: 8 work counters (bulk hand-out)
     uint32_t *vorder = nullptr;      // the other vertices by descending degree (GNN schedule)
     uint32_t n_vorder = 0;

@@ -18,15 +18,13 @@
 //   - quad tier: four lanes per vertex, a float4 of the row each, eight vertices per warp;
 //   - warp tier (more than GC_GNN_WIDE_DEGREE neighbours): a warp per vertex, rows staged in
 //     shared memory;
-//   - hubs (more than GC_GNN_HUB_DEGREE): a CTA per hub that streams neighbour rows into shared
-//     memory with cp.async while one thread per feature runs the sequential FP32 chain; the
-//     largest hubs read rows that k_gnn_hub_gather first copies into a contiguous buffer.  Hub
-//     CTAs run on a second stream, so the long chains overlap the bulk of the layer, and each
-//     giant hub's CTA gets an SM of its own (the bulk CTAs leave the first SMs to them).
+//   - hubs (more than GC_GNN_HUB_DEGREE): before the layer kernel, one CTA per (hub, group of four
+//     features) gathers the neighbour rows in steps of 1,024 into shared memory, and one warp per
+//     feature evaluates the reference's sequential FP32 chain exactly, a step at a time
+//     (exact_step below); the hub's last CTA runs its dense part.
 // Neighbour rows are read with __ldg: a layer never writes the features it reads.  In an A/B on
 // R-MAT 22 (GNN3) the explicit read-only load made the bulk hidden and output layers about 6 %
-// faster than the plain loads the compiler emits here; the step time did not change, since the
-// hub chains bound each layer.
+// faster than the plain loads the compiler emits here.
 //
 // Compiled without fast-math; every add, divide and FMA is an explicit round-to-nearest
 // intrinsic so the compiler cannot contract or reassociate them.
@@ -60,15 +58,8 @@ __global__ void k_gnn_table0(const uint32_t *__restrict__ V, uint32_t N, float f
 
 constexpr unsigned int FULL = 0xffffffffu;
 
-__device__ __forceinline__ uint32_t sm_id() {
-    uint32_t r;
-    asm volatile("mov.u32 %0, %%smid;" : "=r"(r));
-    return r;
-}
-
-// Bulk work handed out by an atomic counter, n items per warp at a time (used when some SMs are
-// left to the giant-hub CTAs, so that the CTAs that do start cover all the work; the sizes are the
-// context's gnn_grab and gnn_heavy).
+// Bulk work handed out by an atomic counter, n items per warp at a time (the sizes are the context's
+// gnn_grab and gnn_heavy), so that the warps that start late take less of it.
 __device__ __forceinline__ uint32_t grab_work(uint32_t *ctr, uint32_t n, int lane) {
     uint32_t b = 0;
     if (lane == 0) b = atomicAdd(ctr, n);
@@ -207,20 +198,16 @@ __device__ __forceinline__ void warp_vertex(uint32_t u, const uint32_t *__restri
     }
 }
 
-// Degree order split in two tiers: the first n_wide vertices (more than GC_GNN_WARP_DEGREE
-// neighbours) one per warp, the rest eight per warp (four lanes each).  Work items are handed out
-// by warp index, heaviest first.
+// Work items, heaviest first: the degree order in two tiers, its first n_wide vertices (more than the
+// GNN warp degree) one per warp, the rest eight per warp (four lanes each).  Handed out by counters
+// (work_ctr).
 template <int MODE>
 __global__ void __launch_bounds__(GNN_THREADS, 4) k_gnn_layer(const uint32_t *__restrict__ V, const uint32_t *__restrict__ E,
                                                               const uint32_t *__restrict__ vorder, uint32_t n_wide,
                                                               uint32_t n_vorder, const float2 *__restrict__ t01,
                                                               const float *__restrict__ x, float *__restrict__ y,
                                                               uint32_t *__restrict__ key, const float *__restrict__ Wb,
-                                                              uint32_t *work_ctr, uint32_t reserve, uint32_t grab,
-                                                              uint32_t heavy) {
-    // an SM left to the giant-hub CTAs: the whole CTA leaves, except the grid's last CTA, which
-    // stays wherever it runs, so the counter's work is done whatever the placement
-    if (reserve && sm_id() < reserve && blockIdx.x != gridDim.x - 1) return;
+                                                              uint32_t *work_ctr, uint32_t grab, uint32_t heavy) {
     __shared__ __align__(16) float sW[LAYER_PARAMS];
     __shared__ __align__(16) float slabs[GNN_THREADS / 32][32 * FEAT];
     for (int i = threadIdx.x; i < LAYER_PARAMS; i += blockDim.x) sW[i] = Wb[i];
@@ -304,10 +291,11 @@ __global__ void __launch_bounds__(GNN_THREADS, 4) k_gnn_layer(const uint32_t *__
         }
     };
     // Dynamic hand-out (work_ctr): items are sorted heaviest first, so the warp-tier vertices
-    // (work_ctr[0]) and the leading `heavy` four-lane items (work_ctr[1]) go one at a time and
-    // spread over the warps; the rest go `grab` at a time (work_ctr[2]).  Otherwise a fixed
+    // (work_ctr[0]) and the leading `heavy` four-lane items (work_ctr[1]) go one at a time
+    // and spread over the warps; the rest go `grab` at a time (work_ctr[2]).  Otherwise a fixed
     // stride.  One call site, so the item body is inlined once.
-    const uint32_t heavy_end = min(n_items, n_wide + heavy);
+    const uint32_t n_first = n_wide;
+    const uint32_t heavy_end = min(n_items, n_first + heavy);
     uint32_t phase = 0, cur = 0, end = 0, sit = warp;
     for (;;) {
         uint32_t it;
@@ -315,10 +303,10 @@ __global__ void __launch_bounds__(GNN_THREADS, 4) k_gnn_layer(const uint32_t *__
             while (cur == end && phase < 3) {
                 if (phase == 0) {
                     const uint32_t x = grab_work(work_ctr, 1u, lane);
-                    if (x < n_wide) cur = x, end = x + 1;
+                    if (x < n_first) cur = x, end = x + 1;
                     else phase = 1;
                 } else if (phase == 1) {
-                    const uint32_t x = n_wide + grab_work(work_ctr + 1, 1u, lane);
+                    const uint32_t x = n_first + grab_work(work_ctr + 1, 1u, lane);
                     if (x < heavy_end) cur = x, end = x + 1;
                     else phase = 2;
                 } else {
@@ -353,10 +341,7 @@ __global__ void __launch_bounds__(THIN_THREADS, 3) k_gnn_thin(const uint32_t *__
                                                               uint32_t n_vorder, const float2 *__restrict__ t01,
                                                               const float *__restrict__ x, float *__restrict__ y,
                                                               uint32_t *__restrict__ key, const float *__restrict__ Wb,
-                                                              uint32_t *work_ctr, uint32_t reserve, uint32_t grab) {
-    // an SM left to the giant-hub CTAs: the whole CTA leaves, except the grid's last CTA, which
-    // stays wherever it runs, so the counter's work is done whatever the placement
-    if (reserve && sm_id() < reserve && blockIdx.x != gridDim.x - 1) return;
+                                                              uint32_t *work_ctr, uint32_t grab) {
     __shared__ __align__(16) float sW[LAYER_PARAMS];
     for (int i = threadIdx.x; i < LAYER_PARAMS; i += blockDim.x) sW[i] = Wb[i];
     __syncthreads();
@@ -497,35 +482,183 @@ __global__ void __launch_bounds__(THIN_THREADS, 3) k_gnn_thin(const uint32_t *__
     }
 }
 
-// ---- hub vertices: one CTA each --------------------------------------------------------------
+// ---- hubs: exact neighbour sums by whole warps ----------------------------------------------------
+//
+// A hub's FP32 neighbour sum s = (((+0 + a_0) + a_1) + ...) + a_{d-1} is a serial chain of d adds in
+// the reference (fast_gnn.c:13-47), 4 cycles each on the GPU: 0.65 ms for the largest R-MAT 22 hub
+// per layer.  Here a warp evaluates it exactly, 1,024 values per step, from these facts (all values
+// are >= +0: ReLU outputs, deg/md, id/N):
+//   - While s lies in the binade [2^e, 2^(e+1)), s = m * u with u = 2^(e-23) and an integer m in
+//     [2^23, 2^24).  Adding a >= 0 rounds m + a/u to an integer: with a/u = q + r (q integer,
+//     0 <= r < 1) the result is m + q for r < 1/2 and m + q + 1 for r > 1/2, whatever m is; an exact
+//     tie (r = 1/2) goes to the even result, so it adds q + ((m + q) & 1) and leaves m even.
+//   - So while the sum stays in its binade, a run of values adds an integer total that depends only
+//     on the parity of m at the run's start: a 2-state transducer (parity in -> total, parity out),
+//     and transducers compose associatively.
+// Lane l holds values 32l .. 32l+31 of the step and builds its transducer over them for both start
+// parities; a 5-round warp scan composes the lanes in order.  The first lane whose run would carry s
+// out of the binade, or that holds a value with a/u >= 2^24 (or Inf/NaN), is added with plain FP32
+// adds in order (shuffles broadcast its values; every lane adds them, so s stays warp-uniform), and
+// the step resumes after it in the new binade.  +0 plus zeros stays +0, and a sum below 2^-103 (grid
+// or its inverse not a normal float) is also added lane by lane with FP32 adds.
+constexpr uint32_t EXACT_TOP = 1u << 24;
+constexpr uint32_t EXACT_SAT = 1u << 25;  // transducer totals are clamped here: >= 2^24 means "leaves"
+constexpr uint32_t HX_TILE = 1024;        // values per step
 
-// Hub CTAs: a producer warp streams the hub's neighbour rows into a shared-memory ring with
-// cp.async, each stage completing on its own mbarrier; a consumer quad adds the rows in CSR
-// order, four features per lane.  No CTA-wide barrier: the producer runs up to HUB_STAGES stages
-// ahead and refills a stage as soon as the consumer releases it.  Every mbarrier wait is bounded:
-// on expiry the kernel raises ERR_WAIT_EXPIRED and returns.
-constexpr int HUB_THREADS = 64;    // warp 0 adds, warp 1 loads
-constexpr int HUB_ROWS = 128;      // rows per stage: 4 per producer lane
-#ifndef GC_HUB_STAGES
-#define GC_HUB_STAGES 12
-#endif
-constexpr int HUB_STAGES = GC_HUB_STAGES;
-#ifndef GC_HUB_ID_AHEAD
-#define GC_HUB_ID_AHEAD 4
-#endif
-constexpr int HUB_ID_AHEAD = GC_HUB_ID_AHEAD;  // the producer reads neighbour ids this many stages early
-constexpr int HUB_BATCH = 16;      // staged values the consumer loads ahead of its add chain
-constexpr unsigned int HUB_WAIT_LIMIT = 1u << 20;  // each try_wait may also suspend briefly
+struct Xd {
+    uint32_t t0, t1;  // total added for start parity 0 / 1
+    uint32_t p0, p1;  // end parity for start parity 0 / 1
+};
+__device__ __forceinline__ Xd xd_after(const Xd &f, const Xd &g) {  // f, then g
+    Xd h;
+    h.t0 = min(f.t0 + (f.p0 ? g.t1 : g.t0), EXACT_SAT);
+    h.t1 = min(f.t1 + (f.p1 ? g.t1 : g.t0), EXACT_SAT);
+    h.p0 = f.p0 ? g.p1 : g.p0;
+    h.p1 = f.p1 ? g.p1 : g.p0;
+    return h;
+}
 
+__device__ __forceinline__ uint32_t hx_pos(uint32_t r) { return (r & ~31u) | ((r ^ (r >> 5)) & 31u); }
+
+// The 32 values of lane c added to s with FP32 adds, in order (every lane reads them: broadcasts).
+__device__ __forceinline__ void serial_lane(float &s, const float *col, uint32_t c) {
+    const float *cp = col + 32u * c;
+#pragma unroll 8
+    for (uint32_t k = 0; k < 32; k++) s = __fadd_rn(s, cp[k ^ c]);
+}
+
+// Parity (0/1) of the increments at the positions of mask m.
+__device__ __forceinline__ uint32_t par(uint32_t pm, uint32_t m) { return (uint32_t)__popc(pm & m) & 1u; }
+
+// Adds one step of 1,024 values to s, bit-identical to the serial chain.  col is the step's column
+// in shared memory, value r at col[hx_pos(r)], +0 past the column's end; lane l takes values
+// 32l .. 32l+31 (slot k ^ l of its 32-word block: 32 distinct banks per load).
+//
+// A lane's transducer from its increments nt_k (rounded to nearest, ties counted as q) and two bit
+// masks, pm (nt_k odd) and tm (value k is a tie): with ties at k_1 < ... < k_n, the first tie adds one
+// more when P + (increments up to and including k_1) is odd (P = the start parity), each later tie k_j
+// adds one when the increments in (k_{j-1}, k_j] have odd sum, and after a tie the parity is that of
+// the increments after the last one.
+__device__ __forceinline__ void exact_step(float &s, const float *col, int lane) {
+    uint32_t start = 0;  // lanes [0, start) are in s (warp-uniform)
+    const float *colp = col + 32u * (uint32_t)lane;
+    while (start < 32) {
+        const bool act = (uint32_t)lane >= start;
+        if (s == 0.0f) {
+            bool nz = false;
+#pragma unroll 8
+            for (uint32_t k = 0; k < 32; k++) nz |= colp[k ^ (uint32_t)lane] != 0.0f;
+            const unsigned int nzm = __ballot_sync(FULL, act && nz);
+            if (!nzm) return;
+            const uint32_t c = (uint32_t)(__ffs(nzm) - 1);
+            serial_lane(s, col, c);
+            start = c + 1u;
+            continue;
+        }
+        const uint32_t be = (__float_as_uint(s) >> 23) & 0xffu;
+        if (be < 24u || be == 255u) {
+            serial_lane(s, col, start);
+            start++;
+            continue;
+        }
+        const float scale = __uint_as_float((277u - be) << 23);  // 1/u = 2^(23-e), e = be - 127
+        const uint32_t m = __float2uint_rz(__fmul_rn(s, scale));
+        Xd x = {0u, 0u, 0u, 1u};
+        bool bad = false;
+        if (act) {
+            uint32_t ta = 0, tb = 0, pm = 0, tm = 0;  // two partial sums in flight
+#pragma unroll
+            for (uint32_t k = 0; k < 32; k++) {
+                const float xv = __fmul_rn(colp[k ^ (uint32_t)lane], scale);
+                bad |= !(xv < 16777216.0f);  // also Inf and NaN
+                const float xs = fminf(xv, 16777216.0f);
+                const float qf = floorf(xs);
+                const float r = __fsub_rn(xs, qf);
+                const uint32_t nt = __float2uint_rz(qf) + (r > 0.5f ? 1u : 0u);
+                if (k & 1) tb += nt;
+                else ta += nt;
+                pm |= (nt & 1u) << k;
+                tm |= (r == 0.5f ? 1u : 0u) << k;
+            }
+            const uint32_t t = min(ta + tb, EXACT_SAT);  // at most 32 (2^24 + 1)
+            if (!tm) {
+                x.t0 = x.t1 = t;
+                x.p0 = par(pm, 0xffffffffu);
+                x.p1 = x.p0 ^ 1u;
+            } else {
+                const int k1 = __ffs(tm) - 1;
+                const uint32_t first = par(pm, 0xffffffffu >> (31 - k1));  // increments 0 .. k1
+                uint32_t extra = 0, rest = tm & (tm - 1u), prev = (uint32_t)k1;
+                while (rest) {  // later ties: one more when (prev, k] has odd sum
+                    const uint32_t k = (uint32_t)(__ffs(rest) - 1);
+                    extra += par(pm, (0xffffffffu >> (31 - k)) & ~(0xffffffffu >> (31 - prev)));
+                    prev = k;
+                    rest &= rest - 1u;
+                }
+                x.t0 = min(t + extra + first, EXACT_SAT);          // P = 0: the first tie adds one when odd
+                x.t1 = min(t + extra + (first ^ 1u), EXACT_SAT);   // P = 1
+                x.p0 = x.p1 = prev == 31u ? 0u : par(pm, 0xffffffffu << (prev + 1u));
+            }
+        }
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {  // inclusive composition over the lanes, in order
+            Xd f;
+            f.t0 = __shfl_up_sync(FULL, x.t0, o);
+            f.t1 = __shfl_up_sync(FULL, x.t1, o);
+            f.p0 = __shfl_up_sync(FULL, x.p0, o);
+            f.p1 = __shfl_up_sync(FULL, x.p1, o);
+            if (lane >= o) x = xd_after(f, x);
+        }
+        const uint32_t I = (m & 1u) ? x.t1 : x.t0;  // added through this lane
+        const unsigned int cm = __ballot_sync(FULL, act && (bad || m + I >= EXACT_TOP));
+        const float unscale = __uint_as_float((be - 23u) << 23);
+        if (!cm) {
+            s = __fmul_rn(__uint2float_rn(m + __shfl_sync(FULL, I, 31)), unscale);
+            return;
+        }
+        const uint32_t c = (uint32_t)(__ffs(cm) - 1);
+        const uint32_t before = __shfl_sync(FULL, I, c > 0 ? (int)c - 1 : 0);
+        if (c > start) s = __fmul_rn(__uint2float_rn(m + before), unscale);
+        serial_lane(s, col, c);
+        start = c + 1u;
+    }
+}
+
+// Hubs (more than the hub degree), beside each layer kernel on a high-priority stream: persistent
+// CTAs, one per SM, take (hub, group of 4 features) items from a counter, heaviest hub first -- one
+// group of the two layer-0 inputs in the input layer -- with one warp per feature.  Per step
+// the CTA gathers 1,024 neighbour rows (its group's float4, or the float2 of layer-0 inputs; each warp
+// a quarter or half) into a feature-major tile in shared memory, XOR-swizzled so that both the
+// gather's stores (32 consecutive rows) and each warp's read of its contiguous per-lane runs hit 32
+// distinct banks; the rows of the next step are in flight while the current one is summed.  The
+// hub's last CTA to finish (a counter per hub, zeroed before the layer) runs the dense part: mean,
+// 32 x 16 FMA chain in order, ReLU, and in the output layer the reference's fixed-tree sum.
+
+constexpr int HX_STAGE = 3;  // staging ring: steps of rows in flight (cp.async)
+constexpr int HX_TILES = 3;  // column tiles ready or being summed: how far the feature warps may drift
+constexpr unsigned int HX_WAIT_LIMIT = 1u << 22;  // polls of one mbarrier phase
+
+__device__ __forceinline__ void cp_async_16(void *smem, const void *gmem) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((unsigned int)__cvta_generic_to_shared(smem)),
+                 "l"(gmem)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_8(void *smem, const void *gmem) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((unsigned int)__cvta_generic_to_shared(smem)),
+                 "l"(gmem)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
 __device__ __forceinline__ unsigned int smem_u32(const void *p) { return (unsigned int)__cvta_generic_to_shared(p); }
 __device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned int count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
 }
 __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
     asm volatile("{\n .reg .b64 st;\n mbarrier.arrive.shared::cta.b64 st, [%0];\n}" ::"r"(smem_u32(bar)) : "memory");
-}
-__device__ __forceinline__ void mbar_arrive_on_copies(uint64_t *bar) {
-    asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned int parity) {
     unsigned int ok;
@@ -536,178 +669,126 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned int parity
         : "memory");
     return ok != 0;
 }
-// Waits for the phase of `parity` to complete; false if the wait gave up (error raised).
+// Waits for the phase of `parity`; false (error raised) when it does not complete in time or another
+// wait already gave up.
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned int parity, DevState *st) {
-    for (unsigned int i = 0; i < HUB_WAIT_LIMIT; i++) {
+    for (unsigned int i = 0; i < HX_WAIT_LIMIT; i++) {
         if (mbar_try_wait(bar, parity)) return true;
         if ((i & 1023u) == 1023u && ld_relaxed_u32(&st->err)) return false;
     }
     raise_error(st, ERR_WAIT_EXPIRED, 0xffffffffu);
     return false;
 }
-__device__ __forceinline__ void cp_async_8(void *smem, const void *gmem) {
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(smem)), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_16(void *smem, const void *gmem) {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(smem)), "l"(gmem) : "memory");
-}
 
-// Giant hubs' neighbour rows, in CSR order, into the staging buffer, one column per feature: hub
-// slot h owns the block of 16 columns starting at 16 * giant[h], each giant[h + 1] - giant[h] floats
-// long (its degree rounded up to 32), so that one warp later streams one feature's column with
-// coalesced loads.  All SMs, one warp per task of GC_GIANT_TASK rows.  Hidden and output layers:
-// four lanes per 64-byte row (one float4 each), eight rows per instruction; input layer: a lane per
-// row and two columns (deg/md, id/N).
-template <int MODE>
-__global__ void __launch_bounds__(256) k_gnn_hub_gather(const uint32_t *__restrict__ V, const uint32_t *__restrict__ E,
-                                                        const uint32_t *__restrict__ hubs,
-                                                        const uint32_t *__restrict__ giant, uint32_t n_giant,
-                                                        uint32_t n_tasks, const float2 *__restrict__ t01,
-                                                        const float *__restrict__ x, float *__restrict__ stage) {
-    const uint32_t *tasks = giant + n_giant + 1;
-    const int lane = threadIdx.x & 31, q = lane & 3;
-    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-    for (uint32_t t = warp; t < n_tasks; t += nwarps) {
-        const uint32_t slot = tasks[2 * t], r0 = tasks[2 * t + 1];
-        const uint32_t u = hubs[slot], base = V[u], d = V[u + 1] - base;
-        const uint32_t rend = min(d, r0 + GC_GIANT_TASK);
-        const size_t dp = giant[slot + 1] - giant[slot];
-        float *cols = stage + (size_t)FEAT * giant[slot];
-        if (MODE == MODE_INPUT) {
-            for (uint32_t r = r0 + lane; r < rend; r += 32) {
-                const float2 tv = __ldg(t01 + ld_stream(E + base + r));
-                cols[r] = tv.x;
-                cols[dp + r] = tv.y;
+// One (hub, feature group) item, warp-specialized.  The producer (the CTA's last warp) copies each
+// step's rows -- their group piece -- by cp.async into a staging ring of HX_STAGE steps (ids read a
+// step ahead), waits for its own copies, writes them as swizzled feature columns into the tile ring
+// slot released by the feature warps (mbarrier `empty`, one arrival per feature warp), and marks it
+// full (mbarrier `full`).  Each feature warp sums its column step by step on its own, so a slow
+// feature (a tie, a change of binade) does not hold the others back by more than the ring's depth.
+// T counts the CTA's steps over all its items, so the barriers' phases continue from item to item.
+template <int MODE, int NG, int NW>
+__device__ __forceinline__ bool hubx_item(uint32_t h, uint32_t g, uint32_t &T, const uint32_t *__restrict__ V,
+                                          const uint32_t *__restrict__ E, const uint32_t *__restrict__ hubs,
+                                          const float2 *__restrict__ t01, const float *__restrict__ x,
+                                          float *__restrict__ sums, unsigned char *smem, uint64_t *full,
+                                          uint64_t *empty, DevState *st) {
+    constexpr int PER = (int)HX_TILE / 32;                // rows per producer lane per step
+    constexpr int PIECE = (MODE == MODE_INPUT) ? 8 : 16;  // bytes of a row's group piece
+    float *tiles = reinterpret_cast<float *>(smem);                                     // HX_TILES x NW x HX_TILE
+    unsigned char *ring = smem + sizeof(float) * HX_TILES * NW * HX_TILE;               // HX_STAGE x HX_TILE pieces
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const uint32_t u = hubs[h], beg = V[u], d = V[u + 1] - beg;
+    const uint32_t nsteps = (d + HX_TILE - 1) / HX_TILE;
+    bool ok = true;
+    if (w == NW) {  // producer
+        uint32_t ids[PER];
+        auto load_ids = [&](uint32_t t) {
+#pragma unroll
+            for (int i = 0; i < PER; i++) {
+                const uint32_t r = t * HX_TILE + 32u * i + lane;
+                ids[i] = r < d ? ld_stream(E + beg + r) : 0xffffffffu;
             }
-        } else {
-            const float4 *X4 = reinterpret_cast<const float4 *>(x);
-            float *c0 = cols + (size_t)(4 * q) * dp;
-            for (uint32_t r = r0 + (lane >> 2); r < rend; r += 32) {
-                uint32_t v[4];
-                float4 val[4];
+        };
+        auto issue = [&](uint32_t t) {  // step t's copies: one commit group, possibly empty
+            if (t < nsteps) {
+                unsigned char *slot = ring + (size_t)(t % HX_STAGE) * HX_TILE * PIECE;
 #pragma unroll
-                for (int k = 0; k < 4; k++) v[k] = r + 8 * k < rend ? E[base + r + 8 * k] : 0u;
-#pragma unroll
-                for (int k = 0; k < 4; k++)
-                    if (r + 8 * k < rend) val[k] = __ldg(X4 + (size_t)v[k] * 4 + q);
-#pragma unroll
-                for (int k = 0; k < 4; k++)
-                    if (r + 8 * k < rend) {
-                        const uint32_t rr = r + 8 * k;
-                        c0[rr] = val[k].x;
-                        c0[dp + rr] = val[k].y;
-                        c0[2 * dp + rr] = val[k].z;
-                        c0[3 * dp + rr] = val[k].w;
+                for (int i = 0; i < PER; i++) {
+                    const uint32_t r = 32u * i + lane;
+                    if (ids[i] != 0xffffffffu) {
+                        if (MODE == MODE_INPUT) cp_async_8(slot + (size_t)r * PIECE, t01 + ids[i]);
+                        else cp_async_16(slot + (size_t)r * PIECE, x + (size_t)ids[i] * FEAT + 4u * g);
                     }
-            }
-        }
-    }
-}
-
-// The reference's neighbour sum s = (((+0 + a_0) + a_1) + ...) + a_{n-1} in FP32, round to nearest
-// even, for a column of n values a_i >= +0 (ReLU outputs, deg/md, id/N: never negative), with the
-// whole warp, 1,024 values per step.  Bit-identical to the serial chain, by this argument:
-//   While s lies in the binade [2^e, 2^(e+1)), s = m * u with u = 2^(e-23) and an integer m in
-//   [2^23, 2^24).  Adding a >= 0 rounds m + a/u to an integer: with a/u = q + r (q integer,
-//   0 <= r < 1) the result is m + q for r < 1/2 and m + q + 1 for r > 1/2, whatever m is; only an
-//   exact tie (r = 1/2) depends on m (to even).  So as long as every partial sum stays below
-//   2^(e+1), i.e. m plus all increments stays below 2^24, the step's result is m + (the integer
-//   sum of the increments), and integer addition is associative.  The increments are exact: a/u is
-//   a scaling by a power of two.
-// A step falls back to the serial chain (shuffles broadcast the values; every lane adds them in
-// order, so s stays warp-uniform) when that does not hold: s below 2^-103 (grid or its inverse not
-// a normal float, e.g. the first step from +0) or infinite, a value with a/u >= 2^24 (or Inf/NaN), an exact tie
-// anywhere in the step, or a step that would carry s into the next binade.  Partial sums are
-// clamped at 2^24, which already means "fall back".  Each lane loads its next step's values while
-// the current ones are summed.
-__device__ __forceinline__ float exact_column_sum(const float *__restrict__ col, uint32_t n, int lane) {
-    constexpr uint32_t STEP = 1024, TOP = 1u << 24;
-    float s = 0.0f;
-    float nx[32];
-#pragma unroll
-    for (int j = 0; j < 32; j++) {
-        const uint32_t i = 32 * j + lane;
-        nx[j] = i < n ? __ldcg(col + i) : 0.0f;
-    }
-    for (uint32_t c0 = 0; c0 < n; c0 += STEP) {
-        const uint32_t cn = min(STEP, n - c0);
-        float a[32];
-#pragma unroll
-        for (int j = 0; j < 32; j++) a[j] = nx[j];
-        if (c0 + STEP < n) {
-#pragma unroll
-            for (int j = 0; j < 32; j++) {
-                const uint32_t i = c0 + STEP + 32 * j + lane;
-                nx[j] = i < n ? __ldcg(col + i) : 0.0f;
-            }
-        }
-        const uint32_t be = (__float_as_uint(s) >> 23) & 0xffu;  // biased exponent of s
-        if (be >= 24u && be < 255u) {
-            const float scale = __uint_as_float((277u - be) << 23);  // 1/u = 2^(23-e), e = be - 127
-            const float unscale = __uint_as_float((be - 23u) << 23);  // u = 2^(e-23)
-            const uint32_t m = __float2uint_rz(__fmul_rn(s, scale));
-            uint32_t acc = 0;
-            bool bad = false;
-#pragma unroll
-            for (int j = 0; j < 32; j++) {
-                const float xv = __fmul_rn(a[j], scale);
-                const bool ok = xv < 16777216.0f;  // false for >= 2^24, Inf and NaN
-                const float xs = ok ? xv : 0.0f;
-                const float qf = floorf(xs);
-                const float r = __fsub_rn(xs, qf);  // exact: xs < 2^24
-                bad |= !ok || r == 0.5f;
-                acc += __float2uint_rz(qf) + (r > 0.5f ? 1u : 0u);  // at most 32 * 2^24
-            }
-            if (!__any_sync(FULL, bad)) {
-                const uint32_t tot = __reduce_add_sync(FULL, min(acc, TOP));
-                const uint32_t mend = m + tot;
-                if (mend < TOP) {
-                    s = __fmul_rn(__uint2float_rn(mend), unscale);
-                    continue;
                 }
             }
+            cp_async_commit();
+        };
+        for (uint32_t t = 0; t + 1 < HX_STAGE; t++) {
+            if (t < nsteps) load_ids(t);
+            issue(t);
         }
-#pragma unroll
-        for (int j = 0; j < 32; j++) {
-            if (32u * j >= cn) break;
-#pragma unroll 8
-            for (int k = 0; k < 32; k++) {
-                const float t = __shfl_sync(FULL, a[j], k);
-                if (32u * j + k < cn) s = __fadd_rn(s, t);
+        if (HX_STAGE - 1 < nsteps) load_ids(HX_STAGE - 1);
+        for (uint32_t t = 0; t < nsteps; t++, T++) {
+            cp_async_wait<HX_STAGE - 2>();  // step t's copies (this warp's only) have landed
+            __syncwarp();
+            const uint32_t slot_t = T % HX_TILES;
+            if (T >= HX_TILES && !mbar_wait(&empty[slot_t], ((T / HX_TILES) - 1u) & 1u, st)) {
+                ok = false;
+                break;
             }
+            const unsigned char *stg = ring + (size_t)(t % HX_STAGE) * HX_TILE * PIECE;
+            float *tile = tiles + (size_t)slot_t * NW * HX_TILE;
+#pragma unroll 4
+            for (int i = 0; i < PER; i++) {  // staged rows -> swizzled columns (rows past the end: +0)
+                const uint32_t r = 32u * i + lane;
+                const bool in = t * HX_TILE + r < d;
+                const uint32_t p = hx_pos(r);
+                if (MODE == MODE_INPUT) {
+                    const float2 v = in ? *reinterpret_cast<const float2 *>(stg + (size_t)r * PIECE) : make_float2(0.0f, 0.0f);
+                    tile[p] = v.x;
+                    tile[HX_TILE + p] = v.y;
+                } else {
+                    const float4 v = in ? *reinterpret_cast<const float4 *>(stg + (size_t)r * PIECE)
+                                        : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                    tile[p] = v.x;
+                    tile[HX_TILE + p] = v.y;
+                    tile[(NW > 2 ? 2 : 0) * HX_TILE + p] = v.z;
+                    tile[(NW > 3 ? 3 : 0) * HX_TILE + p] = v.w;
+                }
+            }
+            __syncwarp();  // the staging slot is read and the tile written by every lane
+            if (lane == 0) mbar_arrive(&full[slot_t]);
+            const uint32_t tn = t + HX_STAGE - 1;
+            issue(tn);
+            if (tn + 1 < nsteps) load_ids(tn + 1);
         }
+        cp_async_wait<0>();  // no copy of ours in flight, whatever happened
+        __syncwarp();
+    } else {  // feature warp w
+        float s = 0.0f;
+        for (uint32_t t = 0; t < nsteps; t++, T++) {
+            const uint32_t slot_t = T % HX_TILES;
+            if (!mbar_wait(&full[slot_t], (T / HX_TILES) & 1u, st)) {
+                ok = false;
+                break;
+            }
+            exact_step(s, tiles + ((size_t)slot_t * NW + w) * HX_TILE, lane);
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&empty[slot_t]);
+        }
+        if (ok && lane == 0) sums[h * FEAT + g * NW + (uint32_t)w] = s;
     }
-    return s;
+    return ok;
 }
 
-// Giant hubs' layer: one warp per (hub, feature) -- two features in the input layer -- sums the
-// hub's staged column with exact_column_sum; the hub's last warp to finish (a counter per hub,
-// zeroed before the layer) runs the dense part: mean, 32 x 16 FMA chain in order, ReLU, and in the
-// output layer the reference's fixed-tree sum into the key.
+// The dense part of hub h from its 16 feature sums (input layer: the two layer-0 sums), by one warp.
 template <int MODE>
-__global__ void __launch_bounds__(128) k_gnn_giant_chain(const uint32_t *__restrict__ V, const uint32_t *__restrict__ hubs,
-                                                         const uint32_t *__restrict__ giant, uint32_t n_giant,
-                                                         const float *__restrict__ stage, const float2 *__restrict__ t01,
-                                                         const float *__restrict__ x, float *__restrict__ y,
-                                                         uint32_t *__restrict__ key, const float *__restrict__ Wb,
-                                                         float *__restrict__ sums, uint32_t *__restrict__ done) {
-    constexpr int NF = (MODE == MODE_INPUT) ? 2 : FEAT;
-    const int lane = threadIdx.x & 31;
-    const uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    if (w >= n_giant * NF) return;
-    const uint32_t h = w / NF, f = w % NF;
+__device__ __forceinline__ void hub_dense(uint32_t h, const uint32_t *__restrict__ V, const uint32_t *__restrict__ hubs,
+                                          const float2 *__restrict__ t01, const float *__restrict__ x,
+                                          float *__restrict__ y, uint32_t *__restrict__ key,
+                                          const float *__restrict__ Wb, const float *__restrict__ sums, int lane) {
     const uint32_t u = hubs[h], d = V[u + 1] - V[u];
-    const size_t dp = giant[h + 1] - giant[h];
-    const float sum = exact_column_sum(stage + (size_t)FEAT * giant[h] + f * dp, d, lane);
-    uint32_t last = 0;
-    if (lane == 0) {
-        sums[h * FEAT + f] = sum;
-        __threadfence();
-        last = atomicAdd(done + h, 1u) == NF - 1;
-    }
-    if (!__shfl_sync(FULL, last, 0)) return;
-    __threadfence();
     const float fd = __uint2float_rn(d);
     const int j = lane & 15;
     float c = __ldg(Wb + 2 * FEAT * FEAT + j);
@@ -748,201 +829,95 @@ __global__ void __launch_bounds__(128) k_gnn_giant_chain(const uint32_t *__restr
     }
 }
 
-// The other hubs (slots n_giant .. n_hubs - 1): one CTA each gathers the rows with cp.async.
+// Hubs (more than the hub degree), before each layer kernel: persistent CTAs take (hub, group of 4
+// features) items from a counter, heaviest hub first (the input layer: one item per hub, its two
+// layer-0 inputs); NW feature warps and one producer warp each (hubx_item).  The hub's last item to
+// finish (a counter per hub, zeroed before the layer) runs the dense part: mean, 32 x 16 FMA chain
+// in order, ReLU, and in the output layer the reference's fixed-tree sum into the key.
 template <int MODE>
-__global__ void __launch_bounds__(HUB_THREADS) k_gnn_hub(const uint32_t *__restrict__ V, const uint32_t *__restrict__ E,
-                                                         const uint32_t *__restrict__ hubs,
-                                                         const float2 *__restrict__ t01, const float *__restrict__ x,
-                                                         float *__restrict__ y, uint32_t *__restrict__ key,
-                                                         const float *__restrict__ Wb, DevState *st, uint32_t first) {
-    constexpr int ROW = (MODE == MODE_INPUT) ? 2 : FEAT;  // floats per staged row
-    extern __shared__ __align__(16) float stage[];         // HUB_STAGES * HUB_ROWS * ROW floats
-    __shared__ __align__(16) float sW[LAYER_PARAMS];
-    __shared__ __align__(8) uint64_t full[HUB_STAGES], empty[HUB_STAGES];
-    for (int i = threadIdx.x; i < LAYER_PARAMS; i += blockDim.x) sW[i] = Wb[i];
+__global__ void __launch_bounds__(160) k_gnn_hubx(const uint32_t *__restrict__ V, const uint32_t *__restrict__ E,
+                                                  const uint32_t *__restrict__ hubs, const float2 *__restrict__ t01,
+                                                  const float *__restrict__ x, float *__restrict__ y,
+                                                  uint32_t *__restrict__ key, const float *__restrict__ Wb,
+                                                  float *__restrict__ sums, uint32_t *__restrict__ done,
+                                                  uint32_t *__restrict__ items, uint32_t n_hubs, DevState *st) {
+    constexpr int NG = (MODE == MODE_INPUT) ? 1 : 4;  // items (feature groups) per hub
+    constexpr int NW = (MODE == MODE_INPUT) ? 2 : 4;  // feature warps per CTA
+    extern __shared__ __align__(16) unsigned char hx_smem[];
+    __shared__ __align__(8) uint64_t full[HX_TILES], empty[HX_TILES];
+    __shared__ uint32_t item_s, last_s;
     if (threadIdx.x == 0) {
-        for (int i = 0; i < HUB_STAGES; i++) {
-            mbar_init(&full[i], 32);  // one copy-completion arrival per producer lane
-            mbar_init(&empty[i], 1);  // the consumer's release
+        for (int i = 0; i < HX_TILES; i++) {
+            mbar_init(&full[i], 1);
+            mbar_init(&empty[i], NW);
         }
     }
     __syncthreads();
-    const uint32_t u = hubs[first + blockIdx.x];
-    const uint32_t beg = V[u], end = V[u + 1], d = end - beg;
-    const uint32_t nchunks = (d + HUB_ROWS - 1) / HUB_ROWS;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-
-    if (warp == 1) {
-        // producer: ids HUB_ID_AHEAD stages ahead in registers, rows via cp.async
-        uint32_t ids[HUB_ID_AHEAD][4];
-        auto load_ids = [&](uint32_t c, uint32_t (&out)[4]) {
-#pragma unroll
-            for (int k = 0; k < 4; k++) {
-                const uint32_t i = beg + c * HUB_ROWS + k * 32 + lane;
-                out[k] = (c < nchunks && i < end) ? ld_stream(E + i) : 0xffffffffu;
-            }
-        };
-#pragma unroll
-        for (int a = 0; a < HUB_ID_AHEAD; a++) load_ids(a, ids[a]);
-        for (uint32_t c = 0; c < nchunks; c++) {
-            const uint32_t s = c % HUB_STAGES;
-            if (c >= HUB_STAGES && !mbar_wait(&empty[s], ((c / HUB_STAGES) - 1) & 1u, st)) {
-                asm volatile("cp.async.wait_all;" ::: "memory");
-                return;
-            }
-            float *buf = stage + (size_t)s * HUB_ROWS * ROW;
-            if (MODE == MODE_INPUT) {
-#pragma unroll
-                for (int k = 0; k < 4; k++) {
-                    const uint32_t v = ids[0][k];
-                    if (v != 0xffffffffu) cp_async_8(buf + (size_t)(k * 32 + lane) * ROW, t01 + v);
-                }
-            } else {
-                // four adjacent lanes copy the four 16-byte pieces of one row: each instruction
-                // moves eight whole 64-byte rows (two sectors each) rather than 32 scattered pieces
-                const int piece = lane & 3;
-#pragma unroll
-                for (int k = 0; k < 4; k++) {
-#pragma unroll
-                    for (int j = 0; j < 4; j++) {
-                        const int r = j * 8 + (lane >> 2);  // row k * 32 + r of the stage
-                        const uint32_t v = __shfl_sync(0xffffffffu, ids[0][k], r);
-                        if (v != 0xffffffffu)
-                            cp_async_16(buf + (size_t)(k * 32 + r) * ROW + 4 * piece, x + (size_t)v * FEAT + 4 * piece);
-                    }
-                }
-            }
-            mbar_arrive_on_copies(&full[s]);
-#pragma unroll
-            for (int a = 0; a + 1 < HUB_ID_AHEAD; a++)
-#pragma unroll
-                for (int k = 0; k < 4; k++) ids[a][k] = ids[a + 1][k];
-            load_ids(c + HUB_ID_AHEAD, ids[HUB_ID_AHEAD - 1]);
+    uint32_t T = 0;  // this thread's count of the CTA's steps (the same in every warp)
+    for (;;) {
+        if (threadIdx.x == 0) item_s = atomicAdd(items, 1u);
+        __syncthreads();
+        const uint32_t it = item_s;
+        if (it >= n_hubs * NG) return;
+        const uint32_t h = it / NG, g = it % NG;
+        const bool ok = hubx_item<MODE, NG, NW>(h, g, T, V, E, hubs, t01, x, sums, hx_smem, full, empty, st);
+        if (__syncthreads_or(!ok)) return;  // a wait gave up: the error is raised
+        if (threadIdx.x == 0) {
+            __threadfence();
+            last_s = atomicAdd(done + h, 1u) == NG - 1;
         }
-        asm volatile("cp.async.wait_all;" ::: "memory");  // leave no copy of ours in flight
-        return;
-    }
-
-    // consumer: warp 0.  Lane l < 16 owns feature l (input layer: lane 0 sums deg/md, lane 1 id/N):
-    // one shared-memory load and one add per row per lane, so the chain runs at the add latency.
-    float acc = 0.0f;
-    for (uint32_t c = 0; c < nchunks; c++) {
-        const uint32_t s = c % HUB_STAGES;
-        if (!mbar_wait(&full[s], (c / HUB_STAGES) & 1u, st)) return;  // the producer stops at its next wait
-        const float *buf = stage + (size_t)s * HUB_ROWS * ROW;
-        const uint32_t cnt = min((uint32_t)HUB_ROWS, end - (beg + c * HUB_ROWS));
-        if (lane < ROW) {
-            if (cnt == HUB_ROWS) {
-                // software pipeline: the next HUB_BATCH staged values are loaded while the current
-                // ones are added, so the chain runs at the add latency, not the shared-load latency
-                float cur[HUB_BATCH], nxt[HUB_BATCH];
-#pragma unroll
-                for (int k = 0; k < HUB_BATCH; k++) cur[k] = buf[k * ROW + lane];
-#pragma unroll
-                for (int r = 0; r < HUB_ROWS; r += HUB_BATCH) {
-                    if (r + HUB_BATCH < HUB_ROWS) {
-#pragma unroll
-                        for (int k = 0; k < HUB_BATCH; k++) nxt[k] = buf[(r + HUB_BATCH + k) * ROW + lane];
-                    }
-#pragma unroll
-                    for (int k = 0; k < HUB_BATCH; k++) acc = __fadd_rn(acc, cur[k]);
-#pragma unroll
-                    for (int k = 0; k < HUB_BATCH; k++) cur[k] = nxt[k];
-                }
-            } else {
-                for (uint32_t r = 0; r < cnt; r++) acc = __fadd_rn(acc, buf[r * ROW + lane]);
-            }
+        __syncthreads();
+        if (last_s && threadIdx.x < 32) {
+            __threadfence();
+            hub_dense<MODE>(h, V, hubs, t01, x, y, key, Wb, sums, threadIdx.x);
         }
-        __syncwarp();
-        if (lane == 0) mbar_arrive(&empty[s]);
-    }
-    // hand the 16 feature sums (or the two input sums) to the quad that runs the dense part
-    const int q = lane & 3;
-    float4 nb;
-    nb.x = __shfl_sync(0xffffffffu, acc, 4 * q + 0);
-    nb.y = __shfl_sync(0xffffffffu, acc, 4 * q + 1);
-    nb.z = __shfl_sync(0xffffffffu, acc, 4 * q + 2);
-    nb.w = __shfl_sync(0xffffffffu, acc, 4 * q + 3);
-    const float in0 = __shfl_sync(0xffffffffu, acc, 0), in1 = __shfl_sync(0xffffffffu, acc, 1);
-    if (lane >= 4) return;
-    const unsigned int mask = 0xfu;
-    const float4 *W4 = reinterpret_cast<const float4 *>(sW);
-    const float4 b4 = reinterpret_cast<const float4 *>(sW + 2 * FEAT * FEAT)[q];
-    const float fd = __uint2float_rn(d);
-    const float4 zero4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    float4 out;
-    if (MODE == MODE_INPUT) {
-        float s0 = in0, s1 = in1;
-        if (fd > 0.0f) {
-            s0 = __fdiv_rn(s0, fd);
-            s1 = __fdiv_rn(s1, fd);
-        }
-        const float2 self = t01[u];
-        out = dense_quad<MODE_INPUT>(W4, b4, q, 0, mask, zero4, zero4, s0, s1, self.x, self.y);
-    } else {
-        if (fd > 0.0f) nb = make_float4(__fdiv_rn(nb.x, fd), __fdiv_rn(nb.y, fd), __fdiv_rn(nb.z, fd), __fdiv_rn(nb.w, fd));
-        const float4 self = reinterpret_cast<const float4 *>(x)[(size_t)u * 4 + q];
-        out = dense_quad<MODE>(W4, b4, q, 0, mask, nb, self, 0.0f, 0.0f, 0.0f, 0.0f);
-    }
-    if (MODE == MODE_OUTPUT) {
-        const float sum = output_sum(out, mask);
-        if (q == 0) key[u] = __float_as_uint(sum);
-    } else {
-        reinterpret_cast<float4 *>(y)[(size_t)u * 4 + q] = out;
     }
 }
 
 template <int MODE>
-gc_status launch_layer(gc_graph *g, const float *Wb, const float *x, float *y, cudaStream_t side,
-                       cudaEvent_t fork, cudaEvent_t join, uint32_t reserve) {
+gc_status launch_layer(gc_graph *g, const float *Wb, const float *x, float *y) {
     gc_ctx *ctx = g->ctx;
     gc_status s;
-    // counters, zeroed here for each layer: bulk items (2..4), thin groups (5); with reserve > 0 the
-    // bulk CTAs that start on SMs 0..reserve-1 leave those SMs to the giant hubs' chains
+    // counters, zeroed for each layer: warp-tier vertices (0), leading four-lane items (1), the rest
+    // (2), thin groups (5)
     uint32_t *ctr = g->gnn_ctr;
     if ((s = gc_check_cuda(ctx, cudaMemsetAsync(ctr, 0, 8 * sizeof(uint32_t), ctx->stream), "gnn work counters")) !=
         GC_OK)
         return s;
+    // hubs: persistent CTAs on the high-priority side stream, beside the layer kernel (whose grid then
+    // leaves one CTA per SM for them)
     if (g->n_hubs) {
-        constexpr int ROW = (MODE == MODE_INPUT) ? 2 : FEAT;
-        constexpr uint32_t NF = (MODE == MODE_INPUT) ? 2 : FEAT;
-        const size_t smem = (size_t)HUB_STAGES * HUB_ROWS * ROW * sizeof(float);
+        constexpr uint32_t NG = (MODE == MODE_INPUT) ? 1 : 4;
+        constexpr uint32_t NW = (MODE == MODE_INPUT) ? 2 : 4;
+        float *sums = reinterpret_cast<float *>(g->hub_aux);
+        uint32_t *done = g->hub_aux + (size_t)FEAT * g->n_hubs;  // n_hubs counters, then the item counter
+        if ((s = gc_check_cuda(ctx, cudaMemsetAsync(done, 0, sizeof(uint32_t) * (g->n_hubs + 1), ctx->stream),
+                               "hub counters")) != GC_OK)
+            return s;
+        cudaStream_t side = ctx->hub_stream ? ctx->hub_stream : ctx->stream;
+        if (side != ctx->stream) {
+            if ((s = gc_check_cuda(ctx, cudaEventRecord(ctx->ev_fork, ctx->stream), "fork")) != GC_OK) return s;
+            if ((s = gc_check_cuda(ctx, cudaStreamWaitEvent(side, ctx->ev_fork, 0), "fork")) != GC_OK) return s;
+        }
+        ProfScope ph(ctx, MODE == MODE_INPUT ? "gnn_hub_input" : (MODE == MODE_HIDDEN ? "gnn_hub_hidden" : "gnn_hub_output"),
+                     side);
+        // CTAs per SM (GC_GNN_HUB_CTAS, default 1): the heaviest hubs' items go first, each warp then
+        // has a scheduler of its own, and those chains bound the kernel
+        const uint32_t per_sm = ctx->gnn_hub_ctas_per_sm;
+        const uint32_t grid = std::min<uint32_t>((uint32_t)ctx->num_sms * per_sm, g->n_hubs * NG);
+        const size_t hsmem =
+            sizeof(float) * HX_TILES * NW * HX_TILE + (size_t)HX_STAGE * HX_TILE * (MODE == MODE_INPUT ? 8 : 16);
         if (!ctx->hub_smem_set[MODE]) {  // once per context: keeps the call out of captured sequences
-            if ((s = gc_check_cuda(ctx, cudaFuncSetAttribute(k_gnn_hub<MODE>,
-                                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+            if ((s = gc_check_cuda(ctx, cudaFuncSetAttribute(k_gnn_hubx<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                             (int)hsmem),
                                    "hub smem")) != GC_OK)
                 return s;
             ctx->hub_smem_set[MODE] = true;
         }
-        if (ctx->gnn_serial) side = ctx->stream;  // hubs first, then the bulk, on one stream
-        if ((s = gc_check_cuda(ctx, cudaEventRecord(fork, ctx->stream), "fork")) != GC_OK) return s;
-        if ((s = gc_check_cuda(ctx, cudaStreamWaitEvent(side, fork, 0), "fork")) != GC_OK) return s;
-        ProfScope ps(ctx, MODE == MODE_INPUT ? "gnn_hub_input" : (MODE == MODE_HIDDEN ? "gnn_hub_hidden" : "gnn_hub_output"),
-                     side);
-        if (g->n_giant) {
-            float *sums = reinterpret_cast<float *>(g->giant_aux);
-            uint32_t *done = g->giant_aux + (size_t)FEAT * g->n_giant;
-            if ((s = gc_check_cuda(ctx, cudaMemsetAsync(done, 0, sizeof(uint32_t) * g->n_giant, side),
-                                   "giant hub counters")) != GC_OK)
-                return s;
-            {
-                ProfScope pg(ctx, "gnn_giant_gather", side);
-                k_gnn_hub_gather<MODE><<<ctx->num_sms * 4, 256, 0, side>>>(g->V, g->E, g->hubs, g->giant, g->n_giant,
-                                                                            g->n_giant_tasks, g->t01, x, g->hub_stage);
-                ctx->launches++;
-            }
-            ProfScope pc(ctx, "gnn_giant_chain", side);
-            const uint32_t warps = g->n_giant * NF;
-            k_gnn_giant_chain<MODE><<<(warps + 3) / 4, 128, 0, side>>>(g->V, g->hubs, g->giant, g->n_giant, g->hub_stage,
-                                                                       g->t01, x, y, g->key, Wb, sums, done);
-            ctx->launches++;
-        }
-        if (g->n_hubs > g->n_giant) {
-            k_gnn_hub<MODE><<<g->n_hubs - g->n_giant, HUB_THREADS, smem, side>>>(
-                g->V, g->E, g->hubs, g->t01, x, y, g->key, Wb, ctx->dstate, g->n_giant);
-            ctx->launches++;
-        }
-        if ((s = gc_check_launch(ctx, "gnn hub layer")) != GC_OK) return s;
+        k_gnn_hubx<MODE><<<grid, (NW + 1) * 32, hsmem, side>>>(g->V, g->E, g->hubs, g->t01, x, y, g->key, Wb, sums,
+                                                               done, done + g->n_hubs, g->n_hubs, ctx->dstate);
+        ctx->launches++;
+        if ((s = gc_check_launch(ctx, "gnn hubs")) != GC_OK) return s;
     }
     int &blocks = ctx->gnn_blocks_per_sm[MODE];
     if (!blocks) {
@@ -956,24 +931,24 @@ gc_status launch_layer(gc_graph *g, const float *Wb, const float *x, float *y, c
         ProfScope ps(ctx, MODE == MODE_INPUT ? "gnn_input" : (MODE == MODE_HIDDEN ? "gnn_hidden" : "gnn_output"),
                      ctx->stream);
         const uint32_t first_thin = g->n_vorder - g->n_thin;
+        const int bb = g->n_hubs && ctx->hub_stream && blocks > 1 ? blocks - 1 : blocks;
         if (first_thin) {
-            k_gnn_layer<MODE><<<ctx->num_sms * blocks, GNN_THREADS, 0, ctx->stream>>>(
-                g->V, g->E, g->vorder, g->n_wide_gnn, first_thin, g->t01, x, y, g->key, Wb, ctr + 2, reserve,
-                ctx->gnn_grab, ctx->gnn_heavy);
+            k_gnn_layer<MODE><<<ctx->num_sms * bb, GNN_THREADS, 0, ctx->stream>>>(
+                g->V, g->E, g->vorder, g->n_wide_gnn, first_thin, g->t01, x, y, g->key, Wb, ctr, ctx->gnn_grab,
+                ctx->gnn_heavy);
             ctx->launches++;
         }
         if (g->n_thin) {
             const uint32_t grid = std::min<uint32_t>((uint32_t)ctx->num_sms * 3, (g->n_thin + THIN_THREADS - 1) / THIN_THREADS);
             k_gnn_thin<MODE><<<grid, THIN_THREADS, 0, ctx->stream>>>(g->V, g->E, g->vorder, first_thin, g->n_vorder,
-                                                                     g->t01, x, y, g->key, Wb, ctr + 5, reserve,
-                                                                     ctx->gnn_grab);
+                                                                     g->t01, x, y, g->key, Wb, ctr + 5, ctx->gnn_grab);
             ctx->launches++;
         }
     }
     if ((s = gc_check_launch(ctx, "gnn layer")) != GC_OK) return s;
-    if (g->n_hubs) {
-        if ((s = gc_check_cuda(ctx, cudaEventRecord(join, side), "join")) != GC_OK) return s;
-        if ((s = gc_check_cuda(ctx, cudaStreamWaitEvent(ctx->stream, join, 0), "join")) != GC_OK) return s;
+    if (g->n_hubs && ctx->hub_stream) {
+        if ((s = gc_check_cuda(ctx, cudaEventRecord(ctx->ev_join, ctx->hub_stream), "join")) != GC_OK) return s;
+        if ((s = gc_check_cuda(ctx, cudaStreamWaitEvent(ctx->stream, ctx->ev_join, 0), "join")) != GC_OK) return s;
     }
     return GC_OK;
 }
@@ -989,40 +964,25 @@ gc_status gc_priority_gnn(gc_graph *g, const gc_model *m) {
     if ((s = gc_alloc(ctx, &g->x, rows * FEAT, "gnn features")) != GC_OK) return s;
     if ((s = gc_alloc(ctx, &g->y, rows * FEAT, "gnn features")) != GC_OK) return s;
     if ((s = gc_alloc(ctx, &g->t01, rows, "gnn input table")) != GC_OK) return s;
-    if (g->n_giant && g->hub_stage_rows < g->giant_rows) {
-        gc_dev_free(ctx, g->hub_stage);
-        g->hub_stage = nullptr;
-        if ((s = gc_alloc(ctx, &g->hub_stage, (size_t)g->giant_rows * FEAT, "giant hub rows")) != GC_OK) return s;
-        g->hub_stage_rows = g->giant_rows;
+    // hubs' feature sums (16 per hub), completion counters (one per hub) and the item counter
+    if (g->n_hubs && g->hub_aux_cap < (size_t)(FEAT + 1) * g->n_hubs + 1) {
+        gc_dev_free(ctx, g->hub_aux);
+        g->hub_aux = nullptr;
+        if ((s = gc_alloc(ctx, &g->hub_aux, (size_t)(FEAT + 1) * g->n_hubs + 1, "hub sums")) != GC_OK) return s;
+        g->hub_aux_cap = (size_t)(FEAT + 1) * g->n_hubs + 1;
     }
-    // giant hubs' feature sums (16 per hub) and completion counters (one per hub)
-    if (g->n_giant && g->giant_aux_cap < (size_t)(FEAT + 1) * g->n_giant) {
-        gc_dev_free(ctx, g->giant_aux);
-        g->giant_aux = nullptr;
-        if ((s = gc_alloc(ctx, &g->giant_aux, (size_t)(FEAT + 1) * g->n_giant, "giant hub sums")) != GC_OK) return s;
-        g->giant_aux_cap = (size_t)(FEAT + 1) * g->n_giant;
-    }
-    // SMs left to the giant hubs' chains (ctx->gnn_hub_sms: -1 one per giant hub, 0 none, n: SMs
-    // 0..n-1).  The bulk work is handed out by counters either way, so CTAs that start late (behind
-    // the hubs' CTAs) take less of it.
-    uint32_t reserve = 0;
-    if (ctx->gnn_hub_sms != 0 && g->n_giant) {
-        reserve = ctx->gnn_hub_sms > 0 ? (uint32_t)ctx->gnn_hub_sms : g->n_giant;
-        reserve = std::min<uint32_t>(reserve, (uint32_t)ctx->num_sms / 6);
-    }
-    if ((s = gc_alloc(ctx, &g->gnn_ctr, 8, "gnn work counters")) != GC_OK) return s;
-    if (ctx->side_stream == nullptr) {
+    if (g->n_hubs && ctx->gnn_hub_side && !ctx->hub_stream) {
         int lo = 0, hi = 0;
         cudaDeviceGetStreamPriorityRange(&lo, &hi);
-        // hub CTAs carry the longest FP32 chains: schedule them ahead of the bulk
-        if ((s = gc_check_cuda(ctx, cudaStreamCreateWithPriority(&ctx->side_stream, cudaStreamNonBlocking, hi),
-                               "stream")) != GC_OK)
+        if ((s = gc_check_cuda(ctx, cudaStreamCreateWithPriority(&ctx->hub_stream, cudaStreamNonBlocking, hi),
+                               "hub stream")) != GC_OK)
             return s;
         if ((s = gc_check_cuda(ctx, cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming), "event")) != GC_OK)
             return s;
         if ((s = gc_check_cuda(ctx, cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming), "event")) != GC_OK)
             return s;
     }
+    if ((s = gc_alloc(ctx, &g->gnn_ctr, 8, "gnn work counters")) != GC_OK) return s;
     {
         ProfScope ps(ctx, "gnn_table0", ctx->stream);
         k_gnn_table0<<<ctx->num_sms * 4, 256, 0, ctx->stream>>>(g->V, g->N, (float)m->md, g->seg_voff, g->n_seg,
@@ -1035,11 +995,11 @@ gc_status gc_priority_gnn(gc_graph *g, const gc_model *m) {
     for (int l = 0; l < L; l++) {
         const float *Wb = m->d_param + (size_t)l * LAYER_PARAMS;
         if (l == 0)
-            s = launch_layer<MODE_INPUT>(g, Wb, nullptr, y, ctx->side_stream, ctx->ev_fork, ctx->ev_join, reserve);
+            s = launch_layer<MODE_INPUT>(g, Wb, nullptr, y);
         else if (l < L - 1)
-            s = launch_layer<MODE_HIDDEN>(g, Wb, x, y, ctx->side_stream, ctx->ev_fork, ctx->ev_join, reserve);
+            s = launch_layer<MODE_HIDDEN>(g, Wb, x, y);
         else
-            s = launch_layer<MODE_OUTPUT>(g, Wb, x, nullptr, ctx->side_stream, ctx->ev_fork, ctx->ev_join, reserve);
+            s = launch_layer<MODE_OUTPUT>(g, Wb, x, nullptr);
         if (s != GC_OK) return s;
         float *t = x;
         x = y;

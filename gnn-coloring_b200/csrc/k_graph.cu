@@ -94,8 +94,6 @@ gc_status gc_graph_prepare(gc_graph *g) {
         g->n_vorder = 0;
         g->n_thin = 0;
         g->n_wide_gnn = 0;
-        g->n_giant = g->n_giant_tasks = 0;
-        g->giant_rows = 0;
         return GC_OK;
     }
     int grid = ctx->num_sms * 8;
@@ -132,8 +130,6 @@ gc_status gc_graph_prepare(gc_graph *g) {
     if ((s = gc_read_state(ctx)) != GC_OK) return s;
     g->n_big_tasks = n_tasks;
     g->n_hubs = n_hubs;
-    g->n_giant = g->n_giant_tasks = 0;
-    g->giant_rows = 0;
     // hubs by descending degree, so the longest FP32 add chains start first
     if (n_hubs > 0) {
         // (vertex, degree) pairs of the hubs, sorted on the host by descending degree
@@ -157,36 +153,6 @@ gc_status gc_graph_prepare(gc_graph *g) {
         if ((s = gc_check_cuda(ctx, cudaMemcpyAsync(g->hubs, h.data(), 4 * (size_t)n_hubs,
                                                     cudaMemcpyHostToDevice, ctx->stream), "hub list")) != GC_OK)
             return s;
-        // giant hubs (the leading ones): staging offsets and gather tasks
-        const uint32_t dmax = hp[2 * idx[0] + 1];
-        const uint32_t thr = ctx->gnn_giant_deg ? ctx->gnn_giant_deg : std::max<uint32_t>(2 * g->hub_deg, dmax / 3);
-        std::vector<uint32_t> gw(1, 0), tasks;
-        uint64_t rows = 0;
-        for (uint32_t i = 0; i < n_hubs; i++) {
-            const uint32_t d = hp[2 * idx[i] + 1];
-            if (d < thr || rows + d + 32 > GC_GIANT_MAX_ROWS) break;
-            for (uint32_t r = 0; r < d; r += GC_GIANT_TASK) {
-                tasks.push_back(i);
-                tasks.push_back(r);
-            }
-            rows += ((uint64_t)d + 31) & ~31ull;
-            gw.push_back((uint32_t)rows);
-            g->n_giant++;
-        }
-        if (g->n_giant) {
-            g->n_giant_tasks = (uint32_t)(tasks.size() / 2);
-            g->giant_rows = rows;
-            gw.insert(gw.end(), tasks.begin(), tasks.end());
-            if (gw.size() > g->giant_cap) {
-                gc_dev_free(ctx, g->giant);
-                g->giant = nullptr;
-                if ((s = gc_alloc(ctx, &g->giant, gw.size(), "giant hub tasks")) != GC_OK) return s;
-                g->giant_cap = gw.size();
-            }
-            if ((s = gc_check_cuda(ctx, cudaMemcpyAsync(g->giant, gw.data(), 4 * gw.size(), cudaMemcpyHostToDevice,
-                                                        ctx->stream), "giant hub tasks")) != GC_OK)
-                return s;
-        }
         if ((s = gc_check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "hub list")) != GC_OK) return s;
     }
     // GNN schedule.  By degree: every non-hub vertex by descending degree (ties by id), so that the

@@ -390,9 +390,10 @@ __global__ void k_jp_records(const uint32_t *__restrict__ order, const uint32_t 
 // whole kernel.  Here one cluster colors tickets [0, K) with every color exchanged through
 // distributed shared memory instead:
 //   - each CTA holds a replica of the K core colors (16 bits each) in its shared memory;
-//   - ticket t belongs to warp (t / C) % W of CTA t % C; a warp takes its tickets in order, so it
-//     waits only on smaller tickets (held by other warps or done) and the oldest unfinished ticket
-//     always progresses;
+//   - tickets go to the CTAs in blocks of B consecutive ones (block k to CTA k % C), so a short link
+//     of a chain often stays inside one SM; a CTA's tickets, in order, go round its W warps.  A warp
+//     takes its tickets in order, so it waits only on smaller tickets (held by other warps or done)
+//     and the oldest unfinished ticket always progresses;
 //   - the owner writes a color into all C replicas (lane i stores into CTA i) and to global memory;
 //     waiting warps poll their own replica;
 //   - a core vertex's predecessors are sources (color 1, known before) or inner vertices with smaller
@@ -404,6 +405,7 @@ __global__ void k_jp_records(const uint32_t *__restrict__ order, const uint32_t 
 constexpr int CORE_WARPS = 16;                 // warps per CTA
 constexpr int CORE_PEND = 256;                 // per warp: uncolored predecessors remembered for polling
 constexpr uint32_t CORE_MAX = 32768;           // most core tickets (16-bit ranks, 64 KB replica)
+constexpr int CORE_LOADS = 8;                  // per lane: predecessor ranks in flight in the first pass
 
 __device__ __forceinline__ unsigned int cluster_rank() {
     unsigned int r;
@@ -477,7 +479,7 @@ __device__ __forceinline__ void core_mark(uint32_t *fb, unsigned int c, uint32_t
 __global__ void __launch_bounds__(CORE_WARPS * 32, 1) k_jp_core(const uint4 *__restrict__ rec,
                                                                 const uint32_t *__restrict__ P, int *color,
                                                                 DevState *st, unsigned int spin_limit,
-                                                                uint32_t kmax) {
+                                                                uint32_t kmax, uint32_t B, unsigned int nap) {
     extern __shared__ __align__(16) unsigned char core_smem[];
     unsigned short *replica = reinterpret_cast<unsigned short *>(core_smem);  // kmax, rounded up to 8
     uint32_t *fb_all = reinterpret_cast<uint32_t *>(core_smem + 2 * (size_t)((kmax + 7u) & ~7u));  // W x 32
@@ -489,8 +491,9 @@ __global__ void __launch_bounds__(CORE_WARPS * 32, 1) k_jp_core(const uint4 *__r
     const unsigned int C = cluster_size(), me = cluster_rank();
     uint32_t *fb = fb_all + warp * 32;
     unsigned short *pend = pend_all + warp * CORE_PEND;
-    const uint32_t stride = C * CORE_WARPS;
-    for (uint32_t t = (uint32_t)warp * C + me; t < K; t += stride) {
+    for (uint32_t i = (uint32_t)warp;; i += CORE_WARPS) {
+        const uint32_t t = ((i / B) * C + me) * B + i % B;  // this CTA's i-th ticket
+        if (t >= K) break;
         const uint4 r = rec[t];
         const uint32_t *list = P + r.y;
         const uint32_t cnt = r.z;
@@ -501,29 +504,41 @@ __global__ void __launch_bounds__(CORE_WARPS * 32, 1) k_jp_core(const uint4 *__r
             __syncwarp();
             if (r.w && window == 0 && lane == 0) core_mark(fb, 1u, 0);
             uint32_t npend = 0;  // warp-uniform
-            for (uint32_t j0 = 0; j0 < cnt; j0 += 32) {
-                const uint32_t j = j0 + lane;
-                const uint32_t rk = j < cnt ? __ldg(list + j) : 0xffffffffu;
-                const unsigned int c = rk != 0xffffffffu ? core_ld(replica + rk) : 0xffffffffu;
-                if (c != 0 && c != 0xffffffffu) core_mark(fb, c, window);
-                const unsigned int zero = __ballot_sync(0xffffffffu, c == 0);
-                if (zero) {
-                    const uint32_t slot = npend + __popc(zero & ((1u << lane) - 1u));
-                    if (c == 0) {
-                        if (slot < CORE_PEND) {
-                            pend[slot] = (unsigned short)rk;
-                        } else {  // list full: wait in place
-                            unsigned int spins = 0, cc;
-                            while ((cc = core_ld(replica + rk)) == 0) {
-                                if (++spins > spin_limit || ((spins & 1023u) == 0 && ld_relaxed_u32(&st->err))) {
-                                    gave_up = true;
-                                    break;
+            for (uint32_t j0 = 0; j0 < cnt; j0 += 32 * CORE_LOADS) {
+                // CORE_LOADS list entries per lane in flight, then their colors from the replica
+                uint32_t rks[CORE_LOADS];
+                unsigned int cs[CORE_LOADS];
+#pragma unroll
+                for (int q = 0; q < CORE_LOADS; q++) {
+                    const uint32_t j = j0 + 32 * q + lane;
+                    rks[q] = j < cnt ? __ldg(list + j) : 0xffffffffu;
+                }
+#pragma unroll
+                for (int q = 0; q < CORE_LOADS; q++) cs[q] = rks[q] != 0xffffffffu ? core_ld(replica + rks[q]) : 0xffffffffu;
+#pragma unroll
+                for (int q = 0; q < CORE_LOADS; q++) {
+                    const uint32_t rk = rks[q];
+                    const unsigned int c = cs[q];
+                    if (c != 0 && c != 0xffffffffu) core_mark(fb, c, window);
+                    const unsigned int zero = __ballot_sync(0xffffffffu, c == 0);
+                    if (zero) {
+                        const uint32_t slot = npend + __popc(zero & ((1u << lane) - 1u));
+                        if (c == 0) {
+                            if (slot < CORE_PEND) {
+                                pend[slot] = (unsigned short)rk;
+                            } else {  // list full: wait in place
+                                unsigned int spins = 0, cc;
+                                while ((cc = core_ld(replica + rk)) == 0) {
+                                    if (++spins > spin_limit || ((spins & 1023u) == 0 && ld_relaxed_u32(&st->err))) {
+                                        gave_up = true;
+                                        break;
+                                    }
                                 }
+                                if (!gave_up) core_mark(fb, cc, window);
                             }
-                            if (!gave_up) core_mark(fb, cc, window);
                         }
+                        npend = min((uint32_t)CORE_PEND, npend + __popc(zero));
                     }
-                    npend = min((uint32_t)CORE_PEND, npend + __popc(zero));
                 }
             }
             __syncwarp();
@@ -545,6 +560,7 @@ __global__ void __launch_bounds__(CORE_WARPS * 32, 1) k_jp_core(const uint4 *__r
                 if (!__any_sync(0xffffffffu, left || gave_up)) break;
                 if (++spins > spin_limit || ((spins & 1023u) == 0 && ld_relaxed_u32(&st->err))) gave_up = true;
                 if (__any_sync(0xffffffffu, gave_up)) break;
+                if (nap) __nanosleep(nap);
             }
             gave_up = __any_sync(0xffffffffu, gave_up);
             if (gave_up) break;
@@ -1029,7 +1045,10 @@ gc_status launch_core(gc_ctx *ctx, gc_graph *g, uint32_t kmax) {
     int *color = g->color;
     DevState *st = ctx->dstate;
     const unsigned int spin = ctx->spin_limit;
-    gc_status s = gc_check_cuda(ctx, cudaLaunchKernelEx(&cfg, k_jp_core, rec, P, color, st, spin, kmax), "jp core");
+    const uint32_t B = ctx->jp_core_block ? ctx->jp_core_block : 1u;
+    const unsigned int nap = ctx->jp_core_nap;
+    gc_status s = gc_check_cuda(ctx, cudaLaunchKernelEx(&cfg, k_jp_core, rec, P, color, st, spin, kmax, B, nap),
+                                "jp core");
     ctx->launches++;
     return s;
 }

@@ -158,10 +158,11 @@ def _one_graph_batch_priorities(ctx, graph, model, hub_degree):
 
 
 @pytest.mark.parametrize("L", [2, 3, 4])
-def test_giant_hub_path_matches_oracle(gpu_ctx, golden, models, L):
-    """Hubs with at least max(2 x hub degree, largest degree / 3) neighbours are summed by the
-    exact binade-step evaluation of the FP32 chain.  Lowering the hub degree sends many vertices
-    of small graphs there; every priority must still equal the oracle's bit for bit."""
+def test_hub_exact_sums_match_oracle(gpu_ctx, golden, models, L):
+    """Hubs (more than the hub degree) have their FP32 neighbour chains evaluated exactly by whole
+    warps, 1,024 values per step (binade increments, parity-resolved ties, serial adds where the
+    sum changes binade).  Lowering the hub degree sends many vertices of small graphs there, the
+    star's id features make exact ties; every priority must still equal the oracle's bit for bit."""
     params, md = golden.model(L)
     graphs = [gcn.gen_rmat(1 << 15, 16, 9), _star(1 << 17), _star(100000), gcn.gen_er(20000, 400000, 4)]
     for graph in graphs:
@@ -172,23 +173,6 @@ def test_giant_hub_path_matches_oracle(gpu_ctx, golden, models, L):
             p, c = _one_graph_batch_priorities(gpu_ctx, graph, models[L], hub)
             assert np.array_equal(p, p_ref), (N, hub, "priorities")
             assert np.array_equal(c, c_ref), (N, hub, "colors")
-
-
-def test_giant_threshold_setting(golden):
-    """GC_GNN_GIANT_DEGREE moves hubs between the CTA path and the exact column path; R-MAT 18's
-    hubs (up to 25,119 neighbours) through either give the oracle's priorities."""
-    N, V, E = gcn.gen_rmat(1 << 18, 16, 2)
-    params, md = golden.model(3)
-    p_ref = O.ordering("GNN", N, V, E, params, md)
-    for giant in ("17000", "1000000"):
-        ctx = _ctx_with({"GC_GNN_GIANT_DEGREE": giant})
-        m = gcn.Model(ctx, params, md)
-        g = gcn.Graph(ctx, N, V, E)
-        g.priority("GNN", m)
-        assert np.array_equal(g.priorities(), p_ref), giant
-        g.close()
-        m.close()
-        ctx.close()
 
 
 def _ctx_with(env: dict):
@@ -204,14 +188,16 @@ def _ctx_with(env: dict):
                 os.environ[k] = v
 
 
-@pytest.mark.parametrize("core,light", [("0", "0"), ("0", "2"), ("64", "2"), ("5000", "6"), ("32768", "0"),
-                                        ("32768", "2"), ("4097", "2")])
-def test_jp_core_sizes_give_the_oracle_colors(golden, core, light):
+@pytest.mark.parametrize("core,light,block", [("0", "0", "16"), ("0", "2", "16"), ("64", "2", "1"), ("5000", "6", "7"),
+                                              ("32768", "0", "16"), ("32768", "2", "16"), ("4097", "2", "64"),
+                                              ("32768", "2", "1")])
+def test_jp_core_sizes_give_the_oracle_colors(golden, core, light, block):
     """The first GC_JP_CORE tickets are colored inside one thread-block cluster (colors exchanged
     through distributed shared memory), the rest by the ticket kernel, split into a heavy and a
-    light stream when GC_JP_LIGHT_WARPS > 0: any combination gives the greedy coloring of the
-    priorities, for float (GNN) and integer (LF) keys and after Culberson rounds."""
-    ctx = _ctx_with({"GC_JP_CORE": core, "GC_JP_LIGHT_WARPS": light})
+    light stream when GC_JP_LIGHT_WARPS > 0, with GC_JP_CORE_BLOCK consecutive core tickets per CTA:
+    any combination gives the greedy coloring of the priorities, for float (GNN) and integer (LF)
+    keys and after Culberson rounds."""
+    ctx = _ctx_with({"GC_JP_CORE": core, "GC_JP_LIGHT_WARPS": light, "GC_JP_CORE_BLOCK": block})
     params, md = golden.model(3)
     m = gcn.Model(ctx, params, md)
     for N, V, E in (gcn.gen_rmat(1 << 17, 16, 2), gcn.gen_er(30000, 300000, 8)):
@@ -221,9 +207,9 @@ def test_jp_core_sizes_give_the_oracle_colors(golden, core, light):
             g.color()
             p = g.priorities()
             c_ref, _ = O.greedy_color(N, V, E, p)
-            assert np.array_equal(g.colors(), c_ref), (core, light, N, heur)
+            assert np.array_equal(g.colors(), c_ref), (core, light, block, N, heur)
         g.recolor(2)
-        assert np.array_equal(g.colors(), O.culberson(N, V, E, c_ref, 2)), (core, light, N)
+        assert np.array_equal(g.colors(), O.culberson(N, V, E, c_ref, 2)), (core, light, block, N)
         g.close()
     m.close()
     ctx.close()
