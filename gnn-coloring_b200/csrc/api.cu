@@ -288,6 +288,7 @@ gc_status gc_ctx_create(int device, gc_ctx **out) {
     if (const char *e = getenv("GC_GNN_HUB_CTAS")) ctx->gnn_hub_ctas_per_sm = std::max<uint32_t>(1u, (uint32_t)strtoul(e, nullptr, 10));
     if (const char *e = getenv("GC_JP_CORE_BLOCK")) ctx->jp_core_block = std::max<uint32_t>(1u, (uint32_t)strtoul(e, nullptr, 10));
     if (const char *e = getenv("GC_JP_CORE_NAP")) ctx->jp_core_nap = (unsigned int)strtoul(e, nullptr, 10);
+    if (const char *e = getenv("GC_JP_CORE_DECIDE")) ctx->jp_core_decide = atoi(e) != 0;
     if (const char *e = getenv("GC_JP_CORE"))
         ctx->jp_core_max = std::min<uint32_t>((uint32_t)strtoul(e, nullptr, 10), 32768u);
     if (const char *e = getenv("GC_JP_NAP")) ctx->jp_nap = (unsigned int)strtoul(e, nullptr, 10);

@@ -48,6 +48,8 @@ struct gc_ctx {
     int jp_core_cluster = -1;            // CTAs of that cluster (16 or 8; 0: unavailable; -1: not yet queried)
     uint32_t jp_core_block = 16;         // consecutive core tickets per CTA (GC_JP_CORE_BLOCK)
     unsigned int jp_core_nap = 0;        // core kernel: sleep between polling rounds, ns (GC_JP_CORE_NAP)
+    bool jp_core_decide = true;          // core kernel: early decisions from published seen colors (GC_JP_CORE_DECIDE)
+    size_t jp_core_smem = 0;             // core kernel: shared memory per CTA (the device's opt-in maximum)
     int jp_light_warps = 2;              // coloring: warps per CTA on the light stream (0: no split; GC_JP_LIGHT_WARPS)
     int gnn_blocks_per_sm[3] = {0, 0, 0};  // resident CTAs of each GNN layer kernel
     uint32_t gnn_warp_deg = GC_GNN_WIDE_DEGREE;  // GNN: above this many neighbours a vertex gets a warp

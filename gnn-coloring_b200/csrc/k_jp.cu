@@ -398,7 +398,12 @@ __global__ void k_jp_records(const uint32_t *__restrict__ order, const uint32_t 
 //     waiting warps poll their own replica;
 //   - a core vertex's predecessors are sources (color 1, known before) or inner vertices with smaller
 //     tickets (core vertices): leaves precede nothing.  A pre-pass rewrites each core ticket's
-//     predecessor list in place as ticket ranks and records whether a source is among them.
+//     predecessor list in place as ticket ranks and records whether a source is among them;
+//   - early decisions: a vertex's color is the mex c of the colors seen so far as soon as no pending
+//     predecessor can take c.  A vertex with p predecessors ends with a color <= p + 1, and one whose
+//     seen colors hold c cannot take c.  So every CTA keeps all core predecessor counts, and a
+//     waiting warp publishes the colors 1..256 it has seen in its CTA's shared memory, where the
+//     warps of every CTA read them.  Bits are only ever set, so a stale read only delays a decision.
 // Waits are bounded (spin_limit polls; on expiry the error is raised and the warp publishes
 // 0xffff, which releases its successors).  A cluster barrier before exit keeps every CTA's shared
 // memory alive while others may still store into it.
@@ -406,6 +411,13 @@ constexpr int CORE_WARPS = 16;                 // warps per CTA
 constexpr int CORE_PEND = 256;                 // per warp: uncolored predecessors remembered for polling
 constexpr uint32_t CORE_MAX = 32768;           // most core tickets (16-bit ranks, 64 KB replica)
 constexpr int CORE_LOADS = 8;                  // per lane: predecessor ranks in flight in the first pass
+constexpr int CORE_PUB = 8;                    // published seen colors per core ticket: 8 words, colors 1..256
+constexpr uint32_t CORE_DECIDE = 32;           // early decisions are tried with at most this many pending
+
+// Tickets one CTA of a C-CTA cluster owns, for K core tickets in blocks of B (an upper bound).
+__host__ __device__ __forceinline__ uint32_t core_owned(uint32_t K, uint32_t B, uint32_t C) {
+    return ((K + B * C - 1) / (B * C)) * B;
+}
 
 __device__ __forceinline__ unsigned int cluster_rank() {
     unsigned int r;
@@ -428,6 +440,21 @@ __device__ __forceinline__ unsigned int core_ld(const unsigned short *p) {
                  : "memory");
     return v;
 }
+// Loads the word at p in CTA `rank`'s shared memory.
+__device__ __forceinline__ uint32_t core_ld_remote(const uint32_t *p, unsigned int rank) {
+    unsigned int remote;
+    uint32_t v;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;"
+                 : "=r"(remote)
+                 : "r"((unsigned int)__cvta_generic_to_shared(p)), "r"(rank));
+    asm volatile("ld.relaxed.cluster.shared::cluster.u32 %0, [%1];" : "=r"(v) : "r"(remote) : "memory");
+    return v;
+}
+// Stores the word v at p in this CTA's shared memory, for loads from the whole cluster.
+__device__ __forceinline__ void core_st_local(uint32_t *p, uint32_t v) {
+    asm volatile("st.relaxed.cluster.shared::cta.u32 [%0], %1;" ::"r"((unsigned int)__cvta_generic_to_shared(p)), "r"(v)
+                 : "memory");
+}
 // Stores v into CTA `rank`'s copy of the replica element p.
 __device__ __forceinline__ void core_st_remote(const unsigned short *p, unsigned int rank, unsigned short v) {
     unsigned int remote;
@@ -439,7 +466,8 @@ __device__ __forceinline__ void core_st_remote(const unsigned short *p, unsigned
 
 // Pre-pass, one warp per core ticket t < K: the predecessor list P[first, first + count) becomes the
 // ranks of its inner predecessors (compacted in place, CSR order kept), rec[t].z their number and
-// rec[t].w = 1 when a source (color 1 from the split) is among the predecessors.
+// rec[t].w = (all predecessors, at most 65,535) << 1 | (1 when a source, color 1 from the split, is
+// among them).
 __global__ void __launch_bounds__(256) k_jp_core_lists(uint4 *__restrict__ rec, uint32_t *__restrict__ P,
                                                        const uint32_t *__restrict__ rank, const int *__restrict__ color,
                                                        const DevState *st, uint32_t kmax) {
@@ -466,7 +494,7 @@ __global__ void __launch_bounds__(256) k_jp_core_lists(uint4 *__restrict__ rec, 
             cnt += __popc(m);
         }
         const bool any_source = __any_sync(0xffffffffu, source);
-        if (lane == 0) rec[t] = make_uint4(r.x, r.y, cnt, any_source ? 1u : 0u);
+        if (lane == 0) rec[t] = make_uint4(r.x, r.y, cnt, (min(r.z, 65535u) << 1) | (any_source ? 1u : 0u));
     }
 }
 
@@ -479,21 +507,31 @@ __device__ __forceinline__ void core_mark(uint32_t *fb, unsigned int c, uint32_t
 __global__ void __launch_bounds__(CORE_WARPS * 32, 1) k_jp_core(const uint4 *__restrict__ rec,
                                                                 const uint32_t *__restrict__ P, int *color,
                                                                 DevState *st, unsigned int spin_limit,
-                                                                uint32_t kmax, uint32_t B, unsigned int nap) {
+                                                                uint32_t kmax, uint32_t B, unsigned int nap,
+                                                                bool decide) {
     extern __shared__ __align__(16) unsigned char core_smem[];
-    unsigned short *replica = reinterpret_cast<unsigned short *>(core_smem);  // kmax, rounded up to 8
-    uint32_t *fb_all = reinterpret_cast<uint32_t *>(core_smem + 2 * (size_t)((kmax + 7u) & ~7u));  // W x 32
+    const unsigned int C = cluster_size(), me = cluster_rank();
+    const uint32_t kr = (kmax + 7u) & ~7u;
+    unsigned short *replica = reinterpret_cast<unsigned short *>(core_smem);  // colors, kr
+    unsigned short *cpc = replica + kr;                                       // predecessor counts, kr
+    uint32_t *pub = reinterpret_cast<uint32_t *>(cpc + kr);                   // this CTA's tickets' seen colors
+    const uint32_t npub = core_owned(kmax, B, C);
+    uint32_t *fb_all = pub + (size_t)npub * CORE_PUB;                         // W x 32
     unsigned short *pend_all = reinterpret_cast<unsigned short *>(fb_all + CORE_WARPS * 32);  // W x CORE_PEND
     const uint32_t K = min(ld_relaxed_u32(&st->ordered), kmax);
-    for (uint32_t i = threadIdx.x; i < K; i += blockDim.x) replica[i] = 0;
+    for (uint32_t i = threadIdx.x; i < K; i += blockDim.x) {
+        replica[i] = 0;
+        cpc[i] = (unsigned short)(rec[i].w >> 1);
+    }
+    for (uint32_t i = threadIdx.x; i < npub * CORE_PUB; i += blockDim.x) pub[i] = 0;
     cluster_sync_all();  // every replica is zeroed before any remote store
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const unsigned int C = cluster_size(), me = cluster_rank();
     uint32_t *fb = fb_all + warp * 32;
     unsigned short *pend = pend_all + warp * CORE_PEND;
     for (uint32_t i = (uint32_t)warp;; i += CORE_WARPS) {
         const uint32_t t = ((i / B) * C + me) * B + i % B;  // this CTA's i-th ticket
         if (t >= K) break;
+        uint32_t *mypub = pub + (size_t)i * CORE_PUB;  // i = the ticket's index among this CTA's
         const uint4 r = rec[t];
         const uint32_t *list = P + r.y;
         const uint32_t cnt = r.z;
@@ -502,7 +540,7 @@ __global__ void __launch_bounds__(CORE_WARPS * 32, 1) k_jp_core(const uint4 *__r
         for (uint32_t window = 0; result < 0 && !gave_up; window++) {
             fb[lane] = 0;
             __syncwarp();
-            if (r.w && window == 0 && lane == 0) core_mark(fb, 1u, 0);
+            if ((r.w & 1u) && window == 0 && lane == 0) core_mark(fb, 1u, 0);
             uint32_t npend = 0;  // warp-uniform
             for (uint32_t j0 = 0; j0 < cnt; j0 += 32 * CORE_LOADS) {
                 // CORE_LOADS list entries per lane in flight, then their colors from the replica
@@ -542,26 +580,63 @@ __global__ void __launch_bounds__(CORE_WARPS * 32, 1) k_jp_core(const uint4 *__r
                 }
             }
             __syncwarp();
-            // poll the pending entries in the local replica
+            const bool publish = decide && window == 0 && npend > 0;
+            if (publish && lane < CORE_PUB) core_st_local(mypub + lane, fb[lane]);
+            // poll the pending entries in the local replica; with at most CORE_DECIDE left, try the
+            // early decision: the candidate c = mex(colors seen) is the color when no pending
+            // predecessor v can take c -- count(v) + 1 < c, or c among the colors v has seen (v's
+            // published set, read from its CTA's shared memory)
             unsigned int spins = 0;
             for (;;) {
-                bool left = false;
-                for (uint32_t i = lane; i < npend && !gave_up; i += 32) {
-                    const unsigned int rk = pend[i];
+                bool progress = false;
+                uint32_t mine = 0;
+                for (uint32_t i2 = lane; i2 < npend && !gave_up; i2 += 32) {
+                    const unsigned int rk = pend[i2];
                     if (rk == 0xffffu) continue;
                     const unsigned int cc = core_ld(replica + rk);
                     if (cc) {
                         core_mark(fb, cc, window);
-                        pend[i] = 0xffffu;
+                        pend[i2] = 0xffffu;
+                        progress = true;
                     } else {
-                        left = true;
+                        mine++;
                     }
                 }
-                if (!__any_sync(0xffffffffu, left || gave_up)) break;
+                const uint32_t nleft = __reduce_add_sync(0xffffffffu, mine);
+                if (nleft == 0 || __any_sync(0xffffffffu, gave_up)) break;
+                const bool prog = __any_sync(0xffffffffu, progress);
+                if (publish && prog) {
+                    __syncwarp();
+                    if (lane < CORE_PUB) core_st_local(mypub + lane, fb[lane]);
+                }
+                if (publish && nleft <= CORE_DECIDE) {
+                    __syncwarp();
+                    const int cand = window_mex(fb, lane, 0);
+                    if (cand > 0) {
+                        bool undecided = false;
+                        for (uint32_t i2 = lane; i2 < npend; i2 += 32) {
+                            const unsigned int rk = pend[i2];
+                            if (rk == 0xffffu) continue;
+                            bool excluded = (unsigned int)cpc[rk] + 1u < (unsigned int)cand;
+                            if (!excluded && cand <= 32 * CORE_PUB) {
+                                const unsigned int owner = (rk / B) % C;
+                                const uint32_t li = (rk / (B * C)) * B + rk % B;
+                                const uint32_t word = core_ld_remote(pub + (size_t)li * CORE_PUB + ((uint32_t)(cand - 1) >> 5), owner);
+                                excluded = (word >> ((uint32_t)(cand - 1) & 31u)) & 1u;
+                            }
+                            if (!excluded) undecided = true;
+                        }
+                        if (!__any_sync(0xffffffffu, undecided)) {
+                            result = cand;
+                            break;
+                        }
+                    }
+                }
                 if (++spins > spin_limit || ((spins & 1023u) == 0 && ld_relaxed_u32(&st->err))) gave_up = true;
                 if (__any_sync(0xffffffffu, gave_up)) break;
-                if (nap) __nanosleep(nap);
+                if (nap && !prog) __nanosleep(nap);
             }
+            if (result > 0) break;  // decided early
             gave_up = __any_sync(0xffffffffu, gave_up);
             if (gave_up) break;
             __syncwarp();
@@ -569,8 +644,8 @@ __global__ void __launch_bounds__(CORE_WARPS * 32, 1) k_jp_core(const uint4 *__r
             __syncwarp();
             if (m) result = m;
         }
-        const unsigned short pub = gave_up ? (unsigned short)0xffffu : (unsigned short)result;
-        if ((unsigned int)lane < C) core_st_remote(replica + t, (unsigned int)lane, pub);
+        const unsigned short val = gave_up ? (unsigned short)0xffffu : (unsigned short)result;
+        if ((unsigned int)lane < C) core_st_remote(replica + t, (unsigned int)lane, val);
         if (lane == 0) {
             if (gave_up) raise_error(st, ERR_WAIT_EXPIRED, r.x);
             st_relaxed(color + r.x, gave_up ? -1 : result);
@@ -985,18 +1060,23 @@ __global__ void k_reset_ticket(DevState *st, unsigned long long *epoch_word, uin
     }
 }
 
-size_t core_smem_bytes(uint32_t kmax) {
-    return 2 * (size_t)((kmax + 7u) & ~7u) + sizeof(uint32_t) * CORE_WARPS * 32 +
-           sizeof(unsigned short) * CORE_WARPS * CORE_PEND;
+size_t core_smem_bytes(uint32_t kmax, uint32_t B, uint32_t C) {
+    return 4 * (size_t)((kmax + 7u) & ~7u) + sizeof(uint32_t) * CORE_PUB * core_owned(kmax, B, C) +
+           sizeof(uint32_t) * CORE_WARPS * 32 + sizeof(unsigned short) * CORE_WARPS * CORE_PEND;
 }
 
 // Once per context: the core kernel's cluster size -- 16 CTAs (a non-portable size) when the device
-// can place such a cluster with this kernel's shared memory, else 8, else 0 (no core phase).
+// can place such a cluster with the most shared memory a CTA may have, else 8, else 0 (no core phase).
 gc_status core_cluster_config(gc_ctx *ctx) {
     if (ctx->jp_core_cluster >= 0) return GC_OK;
     ctx->jp_core_cluster = 0;
-    const size_t smem = core_smem_bytes(CORE_MAX);
-    gc_status s = gc_check_cuda(ctx, cudaFuncSetAttribute(k_jp_core, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+    int optin = 0;
+    gc_status s = gc_check_cuda(ctx, cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device),
+                                "smem per block");
+    if (s != GC_OK) return s;
+    const size_t smem = (size_t)optin;
+    ctx->jp_core_smem = smem;
+    s = gc_check_cuda(ctx, cudaFuncSetAttribute(k_jp_core, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
                                 "core smem");
     if (s != GC_OK) return s;
     if (cudaFuncSetAttribute(k_jp_core, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)
@@ -1026,6 +1106,15 @@ gc_status core_cluster_config(gc_ctx *ctx) {
     return GC_OK;
 }
 
+// The most core tickets, up to kmax, whose replicas and published sets fit the core kernel's shared
+// memory on a cluster of the configured size.
+uint32_t core_fit(const gc_ctx *ctx, uint32_t kmax) {
+    const uint32_t B = ctx->jp_core_block ? ctx->jp_core_block : 1u, C = (uint32_t)ctx->jp_core_cluster;
+    uint32_t k = std::min(kmax, CORE_MAX) & ~7u;
+    while (k && core_smem_bytes(k, B, C) > ctx->jp_core_smem) k -= 8;
+    return k;
+}
+
 gc_status launch_core(gc_ctx *ctx, gc_graph *g, uint32_t kmax) {
     const int C = ctx->jp_core_cluster;
     cudaLaunchConfig_t cfg = {};
@@ -1036,7 +1125,8 @@ gc_status launch_core(gc_ctx *ctx, gc_graph *g, uint32_t kmax) {
     attr[0].val.clusterDim.z = 1;
     cfg.gridDim = dim3(C);
     cfg.blockDim = dim3(CORE_WARPS * 32);
-    cfg.dynamicSmemBytes = core_smem_bytes(kmax);
+    const uint32_t B = ctx->jp_core_block ? ctx->jp_core_block : 1u;
+    cfg.dynamicSmemBytes = core_smem_bytes(kmax, B, (uint32_t)C);
     cfg.stream = ctx->stream;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
@@ -1045,9 +1135,9 @@ gc_status launch_core(gc_ctx *ctx, gc_graph *g, uint32_t kmax) {
     int *color = g->color;
     DevState *st = ctx->dstate;
     const unsigned int spin = ctx->spin_limit;
-    const uint32_t B = ctx->jp_core_block ? ctx->jp_core_block : 1u;
     const unsigned int nap = ctx->jp_core_nap;
-    gc_status s = gc_check_cuda(ctx, cudaLaunchKernelEx(&cfg, k_jp_core, rec, P, color, st, spin, kmax, B, nap),
+    const bool decide = ctx->jp_core_decide;
+    gc_status s = gc_check_cuda(ctx, cudaLaunchKernelEx(&cfg, k_jp_core, rec, P, color, st, spin, kmax, B, nap, decide),
                                 "jp core");
     ctx->launches++;
     return s;
@@ -1175,7 +1265,7 @@ gc_status gc_jp_color(gc_graph *g) {
 
     if ((s = gc_alloc(ctx, &g->jprec, g->cap_N, "ticket records")) != GC_OK) return s;
     uint32_t core = 0;  // core tickets colored in one cluster (at most)
-    if (ctx->jp_core_max && (s = core_cluster_config(ctx)) == GC_OK && ctx->jp_core_cluster > 0) core = ctx->jp_core_max;
+    if (ctx->jp_core_max && (s = core_cluster_config(ctx)) == GC_OK && ctx->jp_core_cluster > 0) core = core_fit(ctx, ctx->jp_core_max);
     if (s != GC_OK) return s;
     if (core && (s = gc_alloc(ctx, &g->rank, g->cap_N, "core ranks")) != GC_OK) return s;
     k_jp_records<<<ctx->num_sms * 4, 256, 0, ctx->stream>>>(g->order, g->V, g->pc, ctx->dstate, g->jprec,
