@@ -293,6 +293,7 @@ gc_status gc_ctx_create(int device, gc_ctx **out) {
         ctx->jp_core_max = std::min<uint32_t>((uint32_t)strtoul(e, nullptr, 10), 32768u);
     if (const char *e = getenv("GC_JP_NAP")) ctx->jp_nap = (unsigned int)strtoul(e, nullptr, 10);
     if (const char *e = getenv("GC_GNN_WARP_DEGREE")) ctx->gnn_warp_deg = (uint32_t)strtoul(e, nullptr, 10);
+    if (const char *e = getenv("GC_HUB_DEGREE")) ctx->hub_deg = std::max<uint32_t>(256u, (uint32_t)strtoul(e, nullptr, 10));
     if (const char *e = getenv("GC_GNN_GRAB")) ctx->gnn_grab = std::max<uint32_t>(1u, (uint32_t)strtoul(e, nullptr, 10));
     if (const char *e = getenv("GC_GNN_HEAVY")) ctx->gnn_heavy = (uint32_t)strtoul(e, nullptr, 10);
     if (const char *e = getenv("GC_GNN_THIN_DEGREE")) ctx->gnn_thin_deg = (uint32_t)strtoul(e, nullptr, 10);
@@ -408,6 +409,7 @@ gc_status gc_graph_upload(gc_ctx *ctx, uint32_t N, const uint32_t *V, const uint
     gc_graph *g = new gc_graph();
     g->ctx = ctx;
     g->gnn_warp_deg = ctx->gnn_warp_deg;
+    g->hub_deg = ctx->hub_deg;
     ctx_retain(ctx);
     if ((s = gc_graph_alloc(ctx, g, N, V[N], true)) != GC_OK) {
         gc_graph_free(g);
@@ -428,6 +430,7 @@ gc_status gc_graph_create(gc_ctx *ctx, uint32_t cap_N, uint32_t cap_M, gc_graph 
     gc_graph *g = new gc_graph();
     g->ctx = ctx;
     g->gnn_warp_deg = ctx->gnn_warp_deg;
+    g->hub_deg = ctx->hub_deg;
     ctx_retain(ctx);
     gc_status s = gc_graph_alloc(ctx, g, cap_N, cap_M, true);
     if (s != GC_OK) {
@@ -465,6 +468,7 @@ gc_status gc_graph_wrap_device(gc_ctx *ctx, uint32_t N, uint32_t M, const uint32
     gc_graph *g = new gc_graph();
     g->ctx = ctx;
     g->gnn_warp_deg = ctx->gnn_warp_deg;
+    g->hub_deg = ctx->hub_deg;
     ctx_retain(ctx);
     g->owns_csr = false;
     g->V = const_cast<uint32_t *>(dV);

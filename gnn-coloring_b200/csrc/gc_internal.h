@@ -53,6 +53,7 @@ struct gc_ctx {
     int jp_light_warps = 2;              // coloring: warps per CTA on the light stream (0: no split; GC_JP_LIGHT_WARPS)
     int gnn_blocks_per_sm[3] = {0, 0, 0};  // resident CTAs of each GNN layer kernel
     uint32_t gnn_warp_deg = GC_GNN_WIDE_DEGREE;  // GNN: above this many neighbours a vertex gets a warp
+    uint32_t hub_deg = GC_GNN_HUB_DEGREE;    // plain graphs: above this many neighbours a vertex is a hub (GC_HUB_DEGREE)
     uint32_t gnn_thin_deg = 16;          // GNN: vertices with at most this many neighbours get one lane each
     uint32_t gnn_grab = 2;               // GNN counter hand-out: items per grab (GC_GNN_GRAB; 1-2 best, 8 +4 %, 16 +17 %)
     uint32_t gnn_heavy = 16384;          // GNN counter hand-out: leading four-lane items taken singly (GC_GNN_HEAVY)

@@ -624,15 +624,10 @@ __device__ __forceinline__ void exact_step(float &s, const float *col, int lane)
     }
 }
 
-// Hubs (more than the hub degree), beside each layer kernel on a high-priority stream: persistent
-// CTAs, one per SM, take (hub, group of 4 features) items from a counter, heaviest hub first -- one
-// group of the two layer-0 inputs in the input layer -- with one warp per feature.  Per step
-// the CTA gathers 1,024 neighbour rows (its group's float4, or the float2 of layer-0 inputs; each warp
-// a quarter or half) into a feature-major tile in shared memory, XOR-swizzled so that both the
-// gather's stores (32 consecutive rows) and each warp's read of its contiguous per-lane runs hit 32
-// distinct banks; the rows of the next step are in flight while the current one is summed.  The
-// hub's last CTA to finish (a counter per hub, zeroed before the layer) runs the dense part: mean,
-// 32 x 16 FMA chain in order, ReLU, and in the output layer the reference's fixed-tree sum.
+// Hub items share one layout: per step, the group pieces of 1,024 neighbour rows (a float4 of four
+// features, or the float2 of the layer-0 inputs) become a feature-major tile in shared memory,
+// XOR-swizzled (hx_pos) so that both the producer's stores of 32 consecutive rows and each feature
+// warp's reads of its contiguous per-lane runs hit 32 distinct banks.
 
 constexpr int HX_STAGE = 3;  // staging ring: steps of rows in flight (cp.async)
 constexpr int HX_TILES = 3;  // column tiles ready or being summed: how far the feature warps may drift
@@ -884,8 +879,8 @@ gc_status launch_layer(gc_graph *g, const float *Wb, const float *x, float *y) {
     if ((s = gc_check_cuda(ctx, cudaMemsetAsync(ctr, 0, 8 * sizeof(uint32_t), ctx->stream), "gnn work counters")) !=
         GC_OK)
         return s;
-    // hubs: persistent CTAs on the high-priority side stream, beside the layer kernel (whose grid then
-    // leaves one CTA per SM for them)
+    // hubs: persistent CTAs before the layer kernel, on the library's stream (GC_GNN_HUB_SIDE=1 puts
+    // them on a high-priority side stream beside it, the layer grid then leaving one CTA per SM)
     if (g->n_hubs) {
         constexpr uint32_t NG = (MODE == MODE_INPUT) ? 1 : 4;
         constexpr uint32_t NW = (MODE == MODE_INPUT) ? 2 : 4;

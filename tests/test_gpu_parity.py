@@ -188,16 +188,20 @@ def _ctx_with(env: dict):
                 os.environ[k] = v
 
 
-@pytest.mark.parametrize("core,light,block", [("0", "0", "16"), ("0", "2", "16"), ("64", "2", "1"), ("5000", "6", "7"),
-                                              ("32768", "0", "16"), ("32768", "2", "16"), ("4097", "2", "64"),
-                                              ("32768", "2", "1")])
-def test_jp_core_sizes_give_the_oracle_colors(golden, core, light, block):
+@pytest.mark.parametrize("core,light,block,decide", [("0", "0", "16", "1"), ("0", "2", "16", "1"), ("64", "2", "1", "1"),
+                                                     ("5000", "6", "7", "1"), ("32768", "0", "16", "1"),
+                                                     ("32768", "2", "16", "1"), ("4097", "2", "64", "1"),
+                                                     ("32768", "2", "1", "1"), ("32768", "2", "16", "0"),
+                                                     ("777", "2", "3", "0")])
+def test_jp_core_sizes_give_the_oracle_colors(golden, core, light, block, decide):
     """The first GC_JP_CORE tickets are colored inside one thread-block cluster (colors exchanged
-    through distributed shared memory), the rest by the ticket kernel, split into a heavy and a
-    light stream when GC_JP_LIGHT_WARPS > 0, with GC_JP_CORE_BLOCK consecutive core tickets per CTA:
-    any combination gives the greedy coloring of the priorities, for float (GNN) and integer (LF)
-    keys and after Culberson rounds."""
-    ctx = _ctx_with({"GC_JP_CORE": core, "GC_JP_LIGHT_WARPS": light, "GC_JP_CORE_BLOCK": block})
+    through distributed shared memory; early decisions from published seen colors unless
+    GC_JP_CORE_DECIDE=0), the rest by the ticket kernel, split into a heavy and a light stream when
+    GC_JP_LIGHT_WARPS > 0, with GC_JP_CORE_BLOCK consecutive core tickets per CTA: any combination
+    gives the greedy coloring of the priorities, for float (GNN) and integer (LF) keys and after
+    Culberson rounds."""
+    ctx = _ctx_with({"GC_JP_CORE": core, "GC_JP_LIGHT_WARPS": light, "GC_JP_CORE_BLOCK": block,
+                     "GC_JP_CORE_DECIDE": decide})
     params, md = golden.model(3)
     m = gcn.Model(ctx, params, md)
     for N, V, E in (gcn.gen_rmat(1 << 17, 16, 2), gcn.gen_er(30000, 300000, 8)):
@@ -207,9 +211,9 @@ def test_jp_core_sizes_give_the_oracle_colors(golden, core, light, block):
             g.color()
             p = g.priorities()
             c_ref, _ = O.greedy_color(N, V, E, p)
-            assert np.array_equal(g.colors(), c_ref), (core, light, block, N, heur)
+            assert np.array_equal(g.colors(), c_ref), (core, light, block, decide, N, heur)
         g.recolor(2)
-        assert np.array_equal(g.colors(), O.culberson(N, V, E, c_ref, 2)), (core, light, block, N)
+        assert np.array_equal(g.colors(), O.culberson(N, V, E, c_ref, 2)), (core, light, block, decide, N)
         g.close()
     m.close()
     ctx.close()
