@@ -518,36 +518,58 @@ __device__ __forceinline__ Xd xd_after(const Xd &f, const Xd &g) {  // f, then g
     return h;
 }
 
-__device__ __forceinline__ uint32_t hx_pos(uint32_t r) { return (r & ~31u) | ((r ^ (r >> 5)) & 31u); }
+// Value r of a column sits at hx_pos(r): lane l's 32 values (r = 32l + k) fill the 32-word block l,
+// their 16-byte chunk k >> 2 at chunk (k >> 2) ^ (l & 7).  A lane reads its block as 8 float4s, and
+// the 8 lanes of each quarter warp then touch 8 distinct chunks (no bank conflict); the producer's
+// stores of 32 consecutive rows (one block) hit 32 distinct banks.
+__device__ __forceinline__ uint32_t hx_pos(uint32_t r) {
+    return (r & ~31u) | (((((r >> 2) ^ (r >> 5)) & 7u)) << 2) | (r & 3u);
+}
+__device__ __forceinline__ uint32_t hx_slot(uint32_t k, uint32_t l) { return ((((k >> 2) ^ l) & 7u) << 2) | (k & 3u); }
 
 // The 32 values of lane c added to s with FP32 adds, in order (every lane reads them: broadcasts).
 __device__ __forceinline__ void serial_lane(float &s, const float *col, uint32_t c) {
     const float *cp = col + 32u * c;
 #pragma unroll 8
-    for (uint32_t k = 0; k < 32; k++) s = __fadd_rn(s, cp[k ^ c]);
+    for (uint32_t k = 0; k < 32; k++) s = __fadd_rn(s, cp[hx_slot(k, c)]);
 }
 
 // Parity (0/1) of the increments at the positions of mask m.
 __device__ __forceinline__ uint32_t par(uint32_t pm, uint32_t m) { return (uint32_t)__popc(pm & m) & 1u; }
 
+// Increment of one value in units of the binade's grid, ties counted as q (r = 1/2 exactly).
+__device__ __forceinline__ uint32_t grid_increment(float xv, bool &tie) {
+    const float qf = floorf(xv);
+    const float r = __fsub_rn(xv, qf);
+    tie = r == 0.5f;
+    return __float2uint_rz(qf) + (r > 0.5f ? 1u : 0u);
+}
+
 // Adds one step of 1,024 values to s, bit-identical to the serial chain.  col is the step's column
 // in shared memory, value r at col[hx_pos(r)], +0 past the column's end; lane l takes values
-// 32l .. 32l+31 (slot k ^ l of its 32-word block: 32 distinct banks per load).
+// 32l .. 32l+31.
 //
-// A lane's transducer from its increments nt_k (rounded to nearest, ties counted as q) and two bit
-// masks, pm (nt_k odd) and tm (value k is a tie): with ties at k_1 < ... < k_n, the first tie adds one
-// more when P + (increments up to and including k_1) is odd (P = the start parity), each later tie k_j
-// adds one when the increments in (k_{j-1}, k_j] have odd sum, and after a tie the parity is that of
-// the increments after the last one.
+// A lane's transducer: without ties it adds the total t of its increments (rounded to nearest) and
+// flips the parity by t's.  With ties at k_1 < ... < k_n, built from two bit masks, pm (increment odd)
+// and tm (value k is a tie, counted as q): the first tie adds one more when P + (increments up to and
+// including k_1) is odd (P = the start parity), each later tie k_j adds one when the increments in
+// (k_{j-1}, k_j] have odd sum, and after a tie the parity is that of the increments after the last
+// one.  The masks are only built (a second pass over the lane's values) when a tie was seen.  Values
+// with a/u >= 2^24, negative ones (-0 included), Inf and NaN all have float bits >= those of 2^24 once
+// scaled, so one unsigned maximum flags them, and their lane is added serially.
 __device__ __forceinline__ void exact_step(float &s, const float *col, int lane) {
     uint32_t start = 0;  // lanes [0, start) are in s (warp-uniform)
-    const float *colp = col + 32u * (uint32_t)lane;
+    const float4 *colp = reinterpret_cast<const float4 *>(col + 32u * (uint32_t)lane);
+    const uint32_t sw = (uint32_t)lane & 7u;
     while (start < 32) {
         const bool act = (uint32_t)lane >= start;
         if (s == 0.0f) {
             bool nz = false;
-#pragma unroll 8
-            for (uint32_t k = 0; k < 32; k++) nz |= colp[k ^ (uint32_t)lane] != 0.0f;
+#pragma unroll
+            for (uint32_t j = 0; j < 8; j++) {
+                const float4 v = colp[j ^ sw];
+                nz |= (v.x != 0.0f) | (v.y != 0.0f) | (v.z != 0.0f) | (v.w != 0.0f);
+            }
             const unsigned int nzm = __ballot_sync(FULL, act && nz);
             if (!nzm) return;
             const uint32_t c = (uint32_t)(__ffs(nzm) - 1);
@@ -566,26 +588,44 @@ __device__ __forceinline__ void exact_step(float &s, const float *col, int lane)
         Xd x = {0u, 0u, 0u, 1u};
         bool bad = false;
         if (act) {
-            uint32_t ta = 0, tb = 0, pm = 0, tm = 0;  // two partial sums in flight
+            uint32_t ta = 0, tb = 0, umax = 0;  // two partial sums in flight
+            bool anytie = false;
 #pragma unroll
-            for (uint32_t k = 0; k < 32; k++) {
-                const float xv = __fmul_rn(colp[k ^ (uint32_t)lane], scale);
-                bad |= !(xv < 16777216.0f);  // also Inf and NaN
-                const float xs = fminf(xv, 16777216.0f);
-                const float qf = floorf(xs);
-                const float r = __fsub_rn(xs, qf);
-                const uint32_t nt = __float2uint_rz(qf) + (r > 0.5f ? 1u : 0u);
-                if (k & 1) tb += nt;
-                else ta += nt;
-                pm |= (nt & 1u) << k;
-                tm |= (r == 0.5f ? 1u : 0u) << k;
+            for (uint32_t j = 0; j < 8; j++) {
+                const float4 v = colp[j ^ sw];
+                const float xs[4] = {__fmul_rn(v.x, scale), __fmul_rn(v.y, scale), __fmul_rn(v.z, scale),
+                                     __fmul_rn(v.w, scale)};
+#pragma unroll
+                for (int i = 0; i < 4; i++) {
+                    umax = max(umax, __float_as_uint(xs[i]));
+                    bool tie;
+                    const uint32_t nt = grid_increment(xs[i], tie);
+                    anytie |= tie;
+                    if (i & 1) tb += nt;
+                    else ta += nt;
+                }
             }
-            const uint32_t t = min(ta + tb, EXACT_SAT);  // at most 32 (2^24 + 1)
-            if (!tm) {
+            bad = umax >= 0x4B800000u;               // 2^24
+            const uint32_t t = min(ta + tb, EXACT_SAT);  // without bad values at most 32 (2^24 - 1)
+            if (!anytie || bad) {
                 x.t0 = x.t1 = t;
-                x.p0 = par(pm, 0xffffffffu);
+                x.p0 = t & 1u;
                 x.p1 = x.p0 ^ 1u;
             } else {
+                uint32_t pm = 0, tm = 0;
+#pragma unroll
+                for (uint32_t j = 0; j < 8; j++) {
+                    const float4 v = colp[j ^ sw];
+                    const float xs[4] = {__fmul_rn(v.x, scale), __fmul_rn(v.y, scale), __fmul_rn(v.z, scale),
+                                         __fmul_rn(v.w, scale)};
+#pragma unroll
+                    for (int i = 0; i < 4; i++) {
+                        bool tie;
+                        const uint32_t nt = grid_increment(xs[i], tie);
+                        pm |= (nt & 1u) << (4 * j + i);
+                        tm |= (tie ? 1u : 0u) << (4 * j + i);
+                    }
+                }
                 const int k1 = __ffs(tm) - 1;
                 const uint32_t first = par(pm, 0xffffffffu >> (31 - k1));  // increments 0 .. k1
                 uint32_t extra = 0, rest = tm & (tm - 1u), prev = (uint32_t)k1;

@@ -582,49 +582,57 @@ __global__ void __launch_bounds__(CORE_WARPS * 32, 1) k_jp_core(const uint4 *__r
             __syncwarp();
             const bool publish = decide && window == 0 && npend > 0;
             if (publish && lane < CORE_PUB) core_st_local(mypub + lane, fb[lane]);
-            // poll the pending entries in the local replica; with at most CORE_DECIDE left, try the
-            // early decision: the candidate c = mex(colors seen) is the color when no pending
-            // predecessor v can take c -- count(v) + 1 < c, or c among the colors v has seen (v's
-            // published set, read from its CTA's shared memory)
+            // poll the pending entries in the local replica, moving those still uncolored to the front
+            // of the list, so that a round costs one load per lane once few are left.  With at most
+            // CORE_DECIDE left (one per lane), try the early decision: the candidate c = mex(colors
+            // seen) is the color when no pending predecessor v can take c -- count(v) + 1 < c, or c
+            // among the colors v has seen (v's published set, read from its CTA's shared memory; the
+            // lanes' loads are in flight together).  Without progress, a decision is re-tried every
+            // other round, so the remote loads do not slow the polling of the local replica.
             unsigned int spins = 0;
+            bool retry = true;
             for (;;) {
                 bool progress = false;
-                uint32_t mine = 0;
-                for (uint32_t i2 = lane; i2 < npend && !gave_up; i2 += 32) {
-                    const unsigned int rk = pend[i2];
-                    if (rk == 0xffffu) continue;
-                    const unsigned int cc = core_ld(replica + rk);
-                    if (cc) {
-                        core_mark(fb, cc, window);
-                        pend[i2] = 0xffffu;
-                        progress = true;
-                    } else {
-                        mine++;
+                uint32_t kept = 0;
+                for (uint32_t c0 = 0; c0 < npend; c0 += 32) {
+                    const uint32_t i2 = c0 + (uint32_t)lane;
+                    unsigned short rk = 0;
+                    bool keep = false;
+                    if (i2 < npend) {
+                        rk = pend[i2];
+                        const unsigned int cc = core_ld(replica + rk);
+                        if (cc) {
+                            core_mark(fb, cc, window);
+                            progress = true;
+                        } else {
+                            keep = true;
+                        }
                     }
+                    const unsigned int km = __ballot_sync(0xffffffffu, keep);
+                    __syncwarp();  // every lane has read its entry before any is moved
+                    if (keep) pend[kept + __popc(km & ((1u << lane) - 1u))] = rk;
+                    kept += __popc(km);
                 }
-                const uint32_t nleft = __reduce_add_sync(0xffffffffu, mine);
-                if (nleft == 0 || __any_sync(0xffffffffu, gave_up)) break;
+                npend = kept;
+                __syncwarp();
+                if (npend == 0) break;
                 const bool prog = __any_sync(0xffffffffu, progress);
-                if (publish && prog) {
-                    __syncwarp();
-                    if (lane < CORE_PUB) core_st_local(mypub + lane, fb[lane]);
-                }
-                if (publish && nleft <= CORE_DECIDE) {
-                    __syncwarp();
+                if (publish && prog && lane < CORE_PUB) core_st_local(mypub + lane, fb[lane]);
+                if (publish && npend <= CORE_DECIDE && (prog || retry)) {
                     const int cand = window_mex(fb, lane, 0);
                     if (cand > 0) {
                         bool undecided = false;
-                        for (uint32_t i2 = lane; i2 < npend; i2 += 32) {
-                            const unsigned int rk = pend[i2];
-                            if (rk == 0xffffu) continue;
+                        if ((uint32_t)lane < npend) {
+                            const unsigned int rk = pend[lane];
                             bool excluded = (unsigned int)cpc[rk] + 1u < (unsigned int)cand;
                             if (!excluded && cand <= 32 * CORE_PUB) {
                                 const unsigned int owner = (rk / B) % C;
                                 const uint32_t li = (rk / (B * C)) * B + rk % B;
-                                const uint32_t word = core_ld_remote(pub + (size_t)li * CORE_PUB + ((uint32_t)(cand - 1) >> 5), owner);
+                                const uint32_t word =
+                                    core_ld_remote(pub + (size_t)li * CORE_PUB + ((uint32_t)(cand - 1) >> 5), owner);
                                 excluded = (word >> ((uint32_t)(cand - 1) & 31u)) & 1u;
                             }
-                            if (!excluded) undecided = true;
+                            undecided = !excluded;
                         }
                         if (!__any_sync(0xffffffffu, undecided)) {
                             result = cand;
@@ -632,6 +640,7 @@ __global__ void __launch_bounds__(CORE_WARPS * 32, 1) k_jp_core(const uint4 *__r
                         }
                     }
                 }
+                retry = !retry || prog;
                 if (++spins > spin_limit || ((spins & 1023u) == 0 && ld_relaxed_u32(&st->err))) gave_up = true;
                 if (__any_sync(0xffffffffu, gave_up)) break;
                 if (nap && !prog) __nanosleep(nap);
