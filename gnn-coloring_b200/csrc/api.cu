@@ -287,6 +287,7 @@ gc_status gc_ctx_create(int device, gc_ctx **out) {
     if (const char *e = getenv("GC_GNN_HUB_SIDE")) ctx->gnn_hub_side = atoi(e) != 0;
     if (const char *e = getenv("GC_GNN_HUB_CTAS")) ctx->gnn_hub_ctas_per_sm = std::max<uint32_t>(1u, (uint32_t)strtoul(e, nullptr, 10));
     if (const char *e = getenv("GC_JP_CORE_BLOCK")) ctx->jp_core_block = std::max<uint32_t>(1u, (uint32_t)strtoul(e, nullptr, 10));
+    if (const char *e = getenv("GC_JP_CORE_WARPS")) ctx->jp_core_warps = atoi(e);
     if (const char *e = getenv("GC_JP_CORE_NAP")) ctx->jp_core_nap = (unsigned int)strtoul(e, nullptr, 10);
     if (const char *e = getenv("GC_JP_CORE_DECIDE")) ctx->jp_core_decide = atoi(e) != 0;
     if (const char *e = getenv("GC_JP_CORE"))
@@ -296,6 +297,7 @@ gc_status gc_ctx_create(int device, gc_ctx **out) {
     if (const char *e = getenv("GC_HUB_DEGREE")) ctx->hub_deg = std::max<uint32_t>(256u, (uint32_t)strtoul(e, nullptr, 10));
     if (const char *e = getenv("GC_GNN_GRAB")) ctx->gnn_grab = std::max<uint32_t>(1u, (uint32_t)strtoul(e, nullptr, 10));
     if (const char *e = getenv("GC_GNN_HEAVY")) ctx->gnn_heavy = (uint32_t)strtoul(e, nullptr, 10);
+    if (const char *e = getenv("GC_GNN_FUSE_ISOLATED")) ctx->gnn_fuse_isolated = atoi(e) != 0;
     if (const char *e = getenv("GC_GNN_THIN_DEGREE")) ctx->gnn_thin_deg = (uint32_t)strtoul(e, nullptr, 10);
     if (s != GC_OK) {
         gc_ctx_destroy(ctx);

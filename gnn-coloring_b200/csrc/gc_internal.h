@@ -48,6 +48,7 @@ struct gc_ctx {
     int jp_core_cluster = -1;            // CTAs of that cluster (16 or 8; 0: unavailable; -1: not yet queried)
     uint32_t jp_core_block = 16;         // consecutive core tickets per CTA (GC_JP_CORE_BLOCK)
     unsigned int jp_core_nap = 0;        // core kernel: sleep between polling rounds, ns (GC_JP_CORE_NAP)
+    int jp_core_warps = 16;              // core kernel: warps per CTA, 1..32 (GC_JP_CORE_WARPS)
     bool jp_core_decide = true;          // core kernel: early decisions from published seen colors (GC_JP_CORE_DECIDE)
     size_t jp_core_smem = 0;             // core kernel: shared memory per CTA (the device's opt-in maximum)
     int jp_light_warps = 2;              // coloring: warps per CTA on the light stream (0: no split; GC_JP_LIGHT_WARPS)
@@ -55,6 +56,7 @@ struct gc_ctx {
     uint32_t gnn_warp_deg = GC_GNN_WIDE_DEGREE;  // GNN: above this many neighbours a vertex gets a warp
     uint32_t hub_deg = GC_GNN_HUB_DEGREE;    // plain graphs: above this many neighbours a vertex is a hub (GC_HUB_DEGREE)
     uint32_t gnn_thin_deg = 16;          // GNN: vertices with at most this many neighbours get one lane each
+    bool gnn_fuse_isolated = true;       // GNN: vertices without neighbours run all layers at once (GC_GNN_FUSE_ISOLATED)
     uint32_t gnn_grab = 2;               // GNN counter hand-out: items per grab (GC_GNN_GRAB; 1-2 best, 8 +4 %, 16 +17 %)
     uint32_t gnn_heavy = 16384;          // GNN counter hand-out: leading four-lane items taken singly (GC_GNN_HEAVY)
     cudaMemPool_t pool = nullptr;        // when set, graph buffers are stream-ordered allocations from this pool
@@ -132,6 +134,7 @@ struct gc_graph {
     uint32_t n_wide_gnn = 0;         // leading vorder entries the GNN gives a warp (more than gnn_warp_deg)
     uint32_t gnn_warp_deg = GC_GNN_WIDE_DEGREE;
     uint32_t n_thin = 0;             // trailing vorder entries with at most ctx->gnn_thin_deg neighbours
+    uint32_t n_iso = 0;              // of those, the trailing entries without neighbours (degree schedule only)
                                      // (degree schedule only; 0 with the graph-major schedule)
     // GNN scratch (allocated on first use)
     float *x = nullptr, *y = nullptr;

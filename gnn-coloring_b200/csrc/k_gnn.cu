@@ -326,6 +326,73 @@ __global__ void __launch_bounds__(GNN_THREADS, 4) k_gnn_layer(const uint32_t *__
     }
 }
 
+// ---- vertices without neighbours: every layer at once -----------------------------------------
+//
+// A vertex without neighbours has a neighbour mean of +0 in every layer (no sum, no division), and
+// nothing reads its features but itself.  So its whole network runs in one pass, one vertex per lane,
+// from its layer-0 inputs to the key, and its rows of x and y are never written.  Each output's FMA
+// chain runs over the inputs in the reference's order; the leading inputs are the same for every
+// such vertex (the +0 means, and in layer 0 also deg/md = 0/md), so that prefix of each chain is
+// evaluated once per CTA, with the same operations, and each vertex continues from it.  These
+// vertices are the tail vorder[first, n) of the degree order.
+constexpr int ISO_THREADS = 256;
+constexpr int ISO_MAX_LAYERS = 16;
+
+__global__ void __launch_bounds__(ISO_THREADS) k_gnn_isolated(const uint32_t *__restrict__ vorder, uint32_t first,
+                                                             uint32_t n, const float2 *__restrict__ t01,
+                                                             uint32_t *__restrict__ key, const float *__restrict__ params,
+                                                             int layers) {
+    extern __shared__ __align__(16) float sP[];  // layers x LAYER_PARAMS
+    __shared__ float c0[ISO_MAX_LAYERS][FEAT];   // each output's chain over the common leading inputs
+    for (int i = threadIdx.x; i < layers * LAYER_PARAMS; i += blockDim.x) sP[i] = params[i];
+    __syncthreads();
+    if (threadIdx.x < layers * FEAT) {
+        const int l = threadIdx.x / FEAT, j = threadIdx.x % FEAT;
+        const float *W = sP + l * LAYER_PARAMS;
+        float c = W[2 * FEAT * FEAT + j];
+        if (l == 0) {
+            const float deg0 = t01[vorder[first]].x;  // 0 / md, the same for every vertex here
+            for (int i = 0; i < 24; i++) c = __fmaf_rn(W[i * FEAT + j], i < 16 ? 0.0f : deg0, c);
+        } else {
+            for (int i = 0; i < FEAT; i++) c = __fmaf_rn(W[i * FEAT + j], 0.0f, c);
+        }
+        c0[l][j] = c;
+    }
+    __syncthreads();
+    for (uint32_t slot = first + blockIdx.x * blockDim.x + threadIdx.x; slot < n; slot += gridDim.x * blockDim.x) {
+        const uint32_t u = vorder[slot];
+        const float id = t01[u].y;
+        float h[FEAT];
+        for (int l = 0; l < layers; l++) {
+            const float4 *W4 = reinterpret_cast<const float4 *>(sP + l * LAYER_PARAMS);
+            float c[FEAT];
+#pragma unroll
+            for (int j = 0; j < FEAT; j++) c[j] = c0[l][j];
+            const int i0 = l == 0 ? 24 : FEAT;
+            for (int i = i0; i < 32; i++) {
+                const float a = l == 0 ? id : h[i - FEAT];
+#pragma unroll
+                for (int jq = 0; jq < 4; jq++) {
+                    const float4 w = W4[i * 4 + jq];
+                    c[4 * jq + 0] = __fmaf_rn(w.x, a, c[4 * jq + 0]);
+                    c[4 * jq + 1] = __fmaf_rn(w.y, a, c[4 * jq + 1]);
+                    c[4 * jq + 2] = __fmaf_rn(w.z, a, c[4 * jq + 2]);
+                    c[4 * jq + 3] = __fmaf_rn(w.w, a, c[4 * jq + 3]);
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < FEAT; j++) h[j] = relu(c[j]);
+        }
+        // t_k = o_k + o_{k+8}, then ((t0+t1)+(t2+t3)) + ((t4+t5)+(t6+t7))  (dense_kernel_output)
+        float t[8];
+#pragma unroll
+        for (int k = 0; k < 8; k++) t[k] = __fadd_rn(h[k], h[k + 8]);
+        const float sum = __fadd_rn(__fadd_rn(__fadd_rn(t[0], t[1]), __fadd_rn(t[2], t[3])),
+                                    __fadd_rn(__fadd_rn(t[4], t[5]), __fadd_rn(t[6], t[7])));
+        key[u] = __float_as_uint(sum);
+    }
+}
+
 // ---- thin tier: one vertex per lane --------------------------------------------------------------
 
 // Vertices with at most ctx->gnn_thin_deg neighbours (the tail of the degree order, vorder[first,
@@ -909,8 +976,9 @@ __global__ void __launch_bounds__(160) k_gnn_hubx(const uint32_t *__restrict__ V
     }
 }
 
+// n_iso: trailing vertices of the degree order without neighbours that k_gnn_isolated has done.
 template <int MODE>
-gc_status launch_layer(gc_graph *g, const float *Wb, const float *x, float *y) {
+gc_status launch_layer(gc_graph *g, const float *Wb, const float *x, float *y, uint32_t n_iso) {
     gc_ctx *ctx = g->ctx;
     gc_status s;
     // counters, zeroed for each layer: warp-tier vertices (0), leading four-lane items (1), the rest
@@ -973,9 +1041,11 @@ gc_status launch_layer(gc_graph *g, const float *Wb, const float *x, float *y) {
                 ctx->gnn_heavy);
             ctx->launches++;
         }
-        if (g->n_thin) {
-            const uint32_t grid = std::min<uint32_t>((uint32_t)ctx->num_sms * 3, (g->n_thin + THIN_THREADS - 1) / THIN_THREADS);
-            k_gnn_thin<MODE><<<grid, THIN_THREADS, 0, ctx->stream>>>(g->V, g->E, g->vorder, first_thin, g->n_vorder,
+        const uint32_t end_thin = g->n_vorder - n_iso;
+        if (end_thin > first_thin) {
+            const uint32_t grid = std::min<uint32_t>((uint32_t)ctx->num_sms * 3,
+                                                     (end_thin - first_thin + THIN_THREADS - 1) / THIN_THREADS);
+            k_gnn_thin<MODE><<<grid, THIN_THREADS, 0, ctx->stream>>>(g->V, g->E, g->vorder, first_thin, end_thin,
                                                                      g->t01, x, y, g->key, Wb, ctr + 5, ctx->gnn_grab);
             ctx->launches++;
         }
@@ -1026,15 +1096,26 @@ gc_status gc_priority_gnn(gc_graph *g, const gc_model *m) {
     ctx->launches++;
     if ((s = gc_check_launch(ctx, "gnn input table")) != GC_OK) return s;
     const int L = m->layers;
+    const uint32_t n_iso = ctx->gnn_fuse_isolated && L <= ISO_MAX_LAYERS ? g->n_iso : 0u;
+    if (n_iso) {
+        ProfScope ps(ctx, "gnn_isolated", ctx->stream);
+        const uint32_t first = g->n_vorder - g->n_iso;
+        const uint32_t grid = std::min<uint32_t>((uint32_t)ctx->num_sms * 4, (g->n_iso + ISO_THREADS - 1) / ISO_THREADS);
+        const size_t smem = sizeof(float) * LAYER_PARAMS * (size_t)L;
+        k_gnn_isolated<<<grid, ISO_THREADS, smem, ctx->stream>>>(g->vorder, first, g->n_vorder, g->t01, g->key,
+                                                                 m->d_param, L);
+        ctx->launches++;
+        if ((s = gc_check_launch(ctx, "gnn isolated vertices")) != GC_OK) return s;
+    }
     float *x = g->x, *y = g->y;
     for (int l = 0; l < L; l++) {
         const float *Wb = m->d_param + (size_t)l * LAYER_PARAMS;
         if (l == 0)
-            s = launch_layer<MODE_INPUT>(g, Wb, nullptr, y);
+            s = launch_layer<MODE_INPUT>(g, Wb, nullptr, y, n_iso);
         else if (l < L - 1)
-            s = launch_layer<MODE_HIDDEN>(g, Wb, x, y);
+            s = launch_layer<MODE_HIDDEN>(g, Wb, x, y, n_iso);
         else
-            s = launch_layer<MODE_OUTPUT>(g, Wb, x, nullptr);
+            s = launch_layer<MODE_OUTPUT>(g, Wb, x, nullptr, n_iso);
         if (s != GC_OK) return s;
         float *t = x;
         x = y;

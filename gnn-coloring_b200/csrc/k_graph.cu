@@ -42,6 +42,7 @@ __global__ void k_degree_classes(const uint32_t *__restrict__ V, uint32_t N, uin
         }
         if (d > gnn_warp_deg && d <= hub_deg) atomicAdd(&st->gnn_wide, 1u);  // counts the GNN warp tier
         if (d <= thin_deg && d <= gnn_warp_deg) atomicAdd(&st->thin, 1u);     // counts the GNN thin tier
+        if (d == 0) atomicAdd(&st->isolated, 1u);
     }
 }
 
@@ -93,6 +94,7 @@ gc_status gc_graph_prepare(gc_graph *g) {
         g->n_hubs = 0;
         g->n_vorder = 0;
         g->n_thin = 0;
+        g->n_iso = 0;
         g->n_wide_gnn = 0;
         return GC_OK;
     }
@@ -111,6 +113,7 @@ gc_status gc_graph_prepare(gc_graph *g) {
     uint32_t n_tasks = ctx->hstate->count, n_hubs = ctx->hstate->count2;
     g->n_wide = ctx->hstate->min_deg;
     g->n_thin = g->sched == GC_SCHEDULE_DEGREE ? ctx->hstate->thin : 0u;
+    g->n_iso = g->sched == GC_SCHEDULE_DEGREE ? ctx->hstate->isolated : 0u;  // the last entries of the degree order
     g->n_wide_gnn = g->sched == GC_SCHEDULE_DEGREE ? ctx->hstate->gnn_wide : g->n_wide;
     // lists: the hub list and the degree order fit in cap_N; the task list grows when needed
     if (2 * (size_t)n_tasks > g->big_cap) {

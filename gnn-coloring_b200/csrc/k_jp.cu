@@ -41,6 +41,8 @@ using namespace gc;
 // GC_GNN_WARP_DEGREE neighbours) one per warp, the rest eight per warp with four lanes each.  A
 // vertex is owned by one warp or quad, so its predecessors are packed with ballots alone.  Hubs
 // (not in the degree order) are split by k_jp_split_big.
+constexpr int SPLIT_LOADS = 4;  // per lane and step of the split: neighbour ids (then their keys) in flight
+
 __global__ void __launch_bounds__(256) k_jp_split(const uint32_t *__restrict__ V, const uint32_t *__restrict__ E,
                                                   const uint32_t *__restrict__ key, const uint32_t *__restrict__ vorder,
                                                   uint32_t n_wide, uint32_t n_vorder, uint32_t *__restrict__ P,
@@ -55,17 +57,23 @@ __global__ void __launch_bounds__(256) k_jp_split(const uint32_t *__restrict__ V
             const uint32_t u = vorder[it];
             const uint32_t beg = V[u], d = V[u + 1] - beg, ku = key[u];
             uint32_t cnt = 0;
-            for (uint32_t c = 0; c < d; c += 64) {
-                const uint32_t ia = c + lane, ib = c + 32 + lane;
-                const uint32_t va = ia < d ? ld_stream(E + beg + ia) : 0u, vb = ib < d ? ld_stream(E + beg + ib) : 0u;
-                const bool pa = ia < d && precedes(__ldg(key + va), va, ku, u);
-                const bool pb = ib < d && precedes(__ldg(key + vb), vb, ku, u);
-                const unsigned int ma = __ballot_sync(0xffffffffu, pa);
-                if (pa) P[beg + cnt + __popc(ma & lt)] = va;
-                cnt += __popc(ma);
-                const unsigned int mb = __ballot_sync(0xffffffffu, pb);
-                if (pb) P[beg + cnt + __popc(mb & lt)] = vb;
-                cnt += __popc(mb);
+            for (uint32_t c = 0; c < d; c += 32 * SPLIT_LOADS) {
+                // SPLIT_LOADS ids and then their keys in flight per lane
+                uint32_t v[SPLIT_LOADS], kv[SPLIT_LOADS];
+#pragma unroll
+                for (int k = 0; k < SPLIT_LOADS; k++) {
+                    const uint32_t i = c + 32 * k + lane;
+                    v[k] = i < d ? ld_stream(E + beg + i) : 0u;
+                }
+#pragma unroll
+                for (int k = 0; k < SPLIT_LOADS; k++) kv[k] = c + 32 * k + lane < d ? __ldg(key + v[k]) : 0u;
+#pragma unroll
+                for (int k = 0; k < SPLIT_LOADS; k++) {
+                    const bool pk = c + 32 * k + lane < d && precedes(kv[k], v[k], ku, u);
+                    const unsigned int mk = __ballot_sync(0xffffffffu, pk);
+                    if (pk) P[beg + cnt + __popc(mk & lt)] = v[k];
+                    cnt += __popc(mk);
+                }
             }
             if (lane == 0) pc[u] = cnt;
             continue;
@@ -78,13 +86,23 @@ __global__ void __launch_bounds__(256) k_jp_split(const uint32_t *__restrict__ V
         const uint32_t dmax = __reduce_max_sync(0xffffffffu, d);
         const unsigned int qlt = (1u << q) - 1u;
         uint32_t cnt = 0;
-        for (uint32_t c = 0; c < dmax; c += 4) {
-            const uint32_t i = c + q;
-            const uint32_t v = i < d ? ld_stream(E + beg + i) : 0u;
-            const bool p = i < d && precedes(__ldg(key + v), v, ku, u);
-            const unsigned int qm = (__ballot_sync(0xffffffffu, p) >> qbase) & 0xfu;
-            if (p) P[beg + cnt + __popc(qm & qlt)] = v;
-            cnt += __popc(qm);
+        for (uint32_t c = 0; c < dmax; c += 4 * SPLIT_LOADS) {
+            // SPLIT_LOADS ids and then their keys in flight per lane (entries c + 4k + q)
+            uint32_t v[SPLIT_LOADS], kv[SPLIT_LOADS];
+#pragma unroll
+            for (int k = 0; k < SPLIT_LOADS; k++) {
+                const uint32_t i = c + 4 * k + q;
+                v[k] = i < d ? ld_stream(E + beg + i) : 0u;
+            }
+#pragma unroll
+            for (int k = 0; k < SPLIT_LOADS; k++) kv[k] = c + 4 * k + q < d ? __ldg(key + v[k]) : 0u;
+#pragma unroll
+            for (int k = 0; k < SPLIT_LOADS; k++) {
+                const bool pk = c + 4 * k + q < d && precedes(kv[k], v[k], ku, u);
+                const unsigned int qm = (__ballot_sync(0xffffffffu, pk) >> qbase) & 0xfu;
+                if (pk) P[beg + cnt + __popc(qm & qlt)] = v[k];
+                cnt += __popc(qm);
+            }
         }
         if (valid && q == 0) pc[u] = cnt;
     }
@@ -407,7 +425,7 @@ __global__ void k_jp_records(const uint32_t *__restrict__ order, const uint32_t 
 // Waits are bounded (spin_limit polls; on expiry the error is raised and the warp publishes
 // 0xffff, which releases its successors).  A cluster barrier before exit keeps every CTA's shared
 // memory alive while others may still store into it.
-constexpr int CORE_WARPS = 16;                 // warps per CTA
+constexpr int CORE_WARPS = 32;                 // most warps per CTA (the launch takes ctx->jp_core_warps)
 constexpr int CORE_PEND = 256;                 // per warp: uncolored predecessors remembered for polling
 constexpr uint32_t CORE_MAX = 32768;           // most core tickets (16-bit ranks, 64 KB replica)
 constexpr int CORE_LOADS = 8;                  // per lane: predecessor ranks in flight in the first pass
@@ -528,7 +546,8 @@ __global__ void __launch_bounds__(CORE_WARPS * 32, 1) k_jp_core(const uint4 *__r
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     uint32_t *fb = fb_all + warp * 32;
     unsigned short *pend = pend_all + warp * CORE_PEND;
-    for (uint32_t i = (uint32_t)warp;; i += CORE_WARPS) {
+    const uint32_t W = blockDim.x >> 5;
+    for (uint32_t i = (uint32_t)warp;; i += W) {
         const uint32_t t = ((i / B) * C + me) * B + i % B;  // this CTA's i-th ticket
         if (t >= K) break;
         uint32_t *mypub = pub + (size_t)i * CORE_PUB;  // i = the ticket's index among this CTA's
@@ -1133,7 +1152,7 @@ gc_status launch_core(gc_ctx *ctx, gc_graph *g, uint32_t kmax) {
     attr[0].val.clusterDim.y = 1;
     attr[0].val.clusterDim.z = 1;
     cfg.gridDim = dim3(C);
-    cfg.blockDim = dim3(CORE_WARPS * 32);
+    cfg.blockDim = dim3(32 * std::min(std::max(ctx->jp_core_warps, 1), CORE_WARPS));
     const uint32_t B = ctx->jp_core_block ? ctx->jp_core_block : 1u;
     cfg.dynamicSmemBytes = core_smem_bytes(kmax, B, (uint32_t)C);
     cfg.stream = ctx->stream;

@@ -175,6 +175,36 @@ def test_hub_exact_sums_match_oracle(gpu_ctx, golden, models, L):
             assert np.array_equal(c, c_ref), (N, hub, "colors")
 
 
+@pytest.mark.parametrize("fuse", ["1", "0"])
+def test_isolated_vertices_match_oracle(golden, fuse):
+    """Vertices without neighbours run every layer at once (k_gnn_isolated, the FMA prefix over the
+    inputs common to all of them evaluated once per CTA) unless GC_GNN_FUSE_ISOLATED=0; either way
+    every priority equals the oracle's bit for bit, for 2, 3 and 4 layers, in a plain graph and in
+    a batch (segment-local id features)."""
+    ctx = _ctx_with({"GC_GNN_FUSE_ISOLATED": fuse})
+    N0, V0, E0 = gcn.gen_rmat(1 << 16, 4, 11)  # R-MAT with a sparse edge factor: many isolated ids
+    graphs = [(N0, V0, E0), (3000, np.zeros(3001, np.uint32), np.zeros(0, np.uint32))]
+    for L in (2, 3, 4):
+        params, md = golden.model(L)
+        m = gcn.Model(ctx, params, md)
+        for N, V, E in graphs:
+            g = gcn.Graph(ctx, N, V, E)
+            g.priority("GNN", m)
+            assert np.array_equal(g.priorities(), O.ordering("GNN", N, V, E, params, md)), (fuse, L, N)
+            g.close()
+        b = gcn.Batch(ctx, graphs=graphs)
+        b.color("GNN", m)
+        p = b.priorities()
+        off = 0
+        for N, V, E in graphs:
+            assert np.array_equal(p[off:off + N], O.ordering("GNN", N, V, E, params, md)), (fuse, L, "batch", N)
+            off += N
+        b.close()
+        m.close()
+    assert int(np.sum(np.diff(V0.astype(np.int64)) == 0)) > 1000
+    ctx.close()
+
+
 def _ctx_with(env: dict):
     old = {k: os.environ.get(k) for k in env}
     os.environ.update(env)
