@@ -27,7 +27,7 @@ struct DevState {
     unsigned int ticket_light;  // coloring: next ticket of the light stream
     unsigned int n_heavy;       // coloring: tickets of the heavy stream (after the core)
     unsigned int n_light;       // coloring: tickets of the light stream (after the core)
-    unsigned int pad;
+    unsigned int isolated;      // preparation: vertices without neighbours (outside the hub list)
 };
 
 enum DevErr : unsigned int {
@@ -50,6 +50,9 @@ __device__ __forceinline__ unsigned int ld_relaxed_u32(const unsigned int *p) {
 }
 __device__ __forceinline__ void st_relaxed(int *p, int v) {
     asm volatile("st.relaxed.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ void st_relaxed_u32(unsigned int *p, unsigned int v) {
+    asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 __device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long *p) {
     unsigned long long v;
