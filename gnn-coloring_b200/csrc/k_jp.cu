@@ -181,6 +181,18 @@ __device__ __forceinline__ int window_mex(const uint32_t *fb, int lane, uint32_t
     return (int)(window * WINDOW + (uint32_t)l * 32 + (uint32_t)(__ffs(fw) - 1) + 1);
 }
 
+// The smallest free color of the window other than c (a free color of the window); 0 if none.
+__device__ __forceinline__ int window_mex_after(const uint32_t *fb, int lane, uint32_t window, int c) {
+    const uint32_t idx = (uint32_t)(c - 1) - window * WINDOW;
+    uint32_t free_bits = ~fb[lane];
+    if ((uint32_t)lane == idx >> 5) free_bits &= ~(1u << (idx & 31u));
+    const unsigned int has = __ballot_sync(0xffffffffu, free_bits != 0);
+    if (!has) return 0;
+    const int l = __ffs(has) - 1;
+    const uint32_t fw = __shfl_sync(0xffffffffu, free_bits, l);
+    return (int)(window * WINDOW + (uint32_t)l * 32 + (uint32_t)(__ffs(fw) - 1) + 1);
+}
+
 // Colors one vertex whose predecessors are list[0..cnt): the smallest color >= 1 none of them
 // has.  Predecessor colors are loaded without waiting first (LOADS per lane in flight); lane
 // entries found uncolored are remembered in a bitmask (the first TRACK entries of each lane) and
@@ -611,6 +623,55 @@ __global__ void __launch_bounds__(CORE_WARPS * 32, 1) k_jp_core(const uint4 *__r
             unsigned int spins = 0;
             bool retry = true;
             for (;;) {
+                if (npend == 1) {
+                    // one predecessor left: both outcomes are known in advance -- c1 = mex(colors
+                    // seen), or the next free color c2 if the predecessor takes c1 -- so the warp
+                    // polls that one entry alone and answers the moment its color lands (early
+                    // decisions re-tried every 64 polls)
+                    __syncwarp();
+                    const int c1 = window_mex(fb, lane, window);
+                    const int c2 = c1 > 0 ? window_mex_after(fb, lane, window, c1) : 0;
+                    const unsigned int rk0 = pend[0];
+                    unsigned int cc = 0;
+                    for (;;) {  // lane 0 reads, the warp follows its values
+                        cc = __shfl_sync(0xffffffffu, lane == 0 ? core_ld(replica + rk0) : 0u, 0);
+                        if (cc) break;
+                        bool stop = ++spins > spin_limit;
+                        if ((spins & 1023u) == 0) stop |= __shfl_sync(0xffffffffu, lane == 0 ? ld_relaxed_u32(&st->err) : 0u, 0) != 0;
+                        if (stop) {
+                            gave_up = true;
+                            break;
+                        }
+                        if (publish && c1 > 0 && (spins & 63u) == 1u) {
+                            bool excluded = (unsigned int)cpc[rk0] + 1u < (unsigned int)c1;
+                            if (!excluded && c1 <= 32 * CORE_PUB) {
+                                const unsigned int owner = (rk0 / B) % C;
+                                const uint32_t li = (rk0 / (B * C)) * B + rk0 % B;
+                                const uint32_t word = __shfl_sync(
+                                    0xffffffffu,
+                                    lane == 0 ? core_ld_remote(pub + (size_t)li * CORE_PUB + ((uint32_t)(c1 - 1) >> 5), owner)
+                                              : 0u,
+                                    0);
+                                excluded = (word >> ((uint32_t)(c1 - 1) & 31u)) & 1u;
+                            }
+                            if (excluded) {
+                                result = c1;
+                                break;
+                            }
+                        }
+                        if (nap) __nanosleep(nap);
+                    }
+                    if (gave_up || result > 0) break;
+                    if (c1 > 0 && (cc != (unsigned int)c1 || c2 > 0)) {
+                        result = cc == (unsigned int)c1 ? c2 : c1;
+                        break;
+                    }
+                    // the window holds no answer: record the color and go on to the next window
+                    if (lane == 0) core_mark(fb, cc, window);
+                    npend = 0;
+                    __syncwarp();
+                    break;
+                }
                 bool progress = false;
                 uint32_t kept = 0;
                 for (uint32_t c0 = 0; c0 < npend; c0 += 32) {

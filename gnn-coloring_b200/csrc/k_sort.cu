@@ -178,6 +178,155 @@ __global__ void __launch_bounds__(SORT_THREADS) k_sort_scatter(SortIn in, int sh
     }
 }
 
+// ---- single-sweep passes (vertex sorts) ----------------------------------------------------------
+//
+// The vertex sorts run every digit pass as one kernel: a histogram kernel first counts the digits of
+// all passes at once (the first pass's filter decides which vertices take part), one CTA scans those
+// totals into each digit's first output position per pass, and then each pass is a single kernel in
+// which a CTA takes the next tile from a counter, ranks it (stable, as above), publishes its digit
+// counts and finds the counts of all earlier tiles by decoupled look-back: tile k's status word per
+// digit holds its own count (flag AGG) and, once known, the count of tiles 0..k (flag INC); a tile
+// walks back from k-1, adding AGG counts, until it meets an INC.  Tiles are taken in order, so every
+// tile looked at is running or done; each wait is bounded (SW_WAIT_LIMIT polls, then ERR_WAIT_EXPIRED:
+// a fixed bound, since these waits only end a pass, unlike the coloring's configurable ones).
+constexpr uint32_t SW_AGG = 1u << 30, SW_INC = 2u << 30, SW_VAL = SW_AGG - 1u;
+constexpr int SW_WINDOW = 4;  // predecessor status words in flight per look-back step
+constexpr unsigned int SW_WAIT_LIMIT = 1u << 22;
+
+__global__ void __launch_bounds__(SORT_THREADS) k_sort_hist_all(SortIn in, int passes, uint32_t mask,
+                                                                uint32_t *__restrict__ totals) {
+    __shared__ uint32_t hist[4][RADIX];
+    for (int i = threadIdx.x; i < 4 * RADIX; i += SORT_THREADS) (&hist[0][0])[i] = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const uint32_t n = in.N;  // the first pass's input: every vertex
+    for (uint32_t base = blockIdx.x * SORT_THREADS; base < n; base += gridDim.x * SORT_THREADS) {
+        uint32_t k, v;
+        const bool valid = sort_elem(in, base + threadIdx.x, n, k, v);
+        for (int p = 0; p < passes; p++) {
+            const uint32_t d = valid ? digit_of(k, 8 * p, mask) : 0xffffffffu;
+            const unsigned int peers = __match_any_sync(0xffffffffu, d);
+            if (valid && lane == __ffs(peers) - 1) atomicAdd(&hist[p][d], (uint32_t)__popc(peers));
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < passes * RADIX; i += SORT_THREADS) {
+        const uint32_t c = (&hist[0][0])[i];
+        if (c) atomicAdd(&totals[i], c);
+    }
+}
+
+// Per pass: exclusive scan of the digit totals into the digits' first output positions (one CTA of
+// RADIX threads); the element count goes to *d_count.
+__global__ void __launch_bounds__(RADIX) k_sort_scan_all(const uint32_t *__restrict__ totals, int passes,
+                                                         uint32_t *__restrict__ bases, uint32_t *d_count) {
+    __shared__ uint32_t part[RADIX];
+    for (int p = 0; p < passes; p++) {
+        part[threadIdx.x] = totals[p * RADIX + threadIdx.x];
+        __syncthreads();
+        for (int off = 1; off < RADIX; off <<= 1) {
+            const uint32_t v = threadIdx.x >= (unsigned)off ? part[threadIdx.x - off] : 0;
+            __syncthreads();
+            part[threadIdx.x] += v;
+            __syncthreads();
+        }
+        bases[p * RADIX + threadIdx.x] = threadIdx.x ? part[threadIdx.x - 1] : 0;
+        if (p == 0 && d_count && threadIdx.x == RADIX - 1) *d_count = part[RADIX - 1];
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(SORT_THREADS) k_sort_sweep(SortIn in, int shift, uint32_t mask,
+                                                             const uint32_t *__restrict__ bases,
+                                                             uint32_t *__restrict__ status, uint32_t *tile_ctr,
+                                                             uint32_t *__restrict__ kout, uint32_t *__restrict__ vout,
+                                                             DevState *st) {
+    __shared__ uint32_t wcnt[SORT_WARPS][RADIX];
+    __shared__ uint32_t gbase[RADIX];
+    __shared__ uint32_t tile_s;
+    if (threadIdx.x == 0) tile_s = atomicAdd(tile_ctr, 1u);
+    __syncthreads();
+    const uint32_t tile = tile_s;
+    const uint32_t n = pass_len(in);
+    if (tile * SORT_TILE >= n) return;  // later tiles are empty too: nobody looks at this one
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int d = lane; d < RADIX; d += 32) wcnt[warp][d] = 0;
+    __syncwarp();
+    const uint32_t wbase = tile * SORT_TILE + warp * (32 * SORT_ITEMS);
+    uint32_t k[SORT_ITEMS], v[SORT_ITEMS], pos[SORT_ITEMS];
+    uint32_t valid_mask = 0;
+    const unsigned int lt = (1u << lane) - 1u;
+#pragma unroll
+    for (int s = 0; s < SORT_ITEMS; s++) {
+        const uint32_t j = wbase + s * 32 + lane;
+        const bool valid = sort_elem(in, j, n, k[s], v[s]);
+        if (valid) valid_mask |= 1u << s;
+        const uint32_t d = valid ? digit_of(k[s], shift, mask) : 0xffffffffu;
+        const unsigned int peers = __match_any_sync(0xffffffffu, d);
+        const uint32_t before = valid ? wcnt[warp][d] : 0;
+        pos[s] = before + __popc(peers & lt);
+        __syncwarp();
+        if (valid && lane == __ffs(peers) - 1) wcnt[warp][d] = before + __popc(peers);
+        __syncwarp();
+    }
+    __syncthreads();
+    // per digit: exclusive prefix across warps, the tile's count, its status, then the look-back
+    for (int d = threadIdx.x; d < RADIX; d += SORT_THREADS) {
+        uint32_t run = 0;
+        for (int w = 0; w < SORT_WARPS; w++) {
+            const uint32_t c = wcnt[w][d];
+            wcnt[w][d] = run;
+            run += c;
+        }
+        uint32_t *mine = status + (size_t)tile * RADIX + d;
+        uint32_t excl = 0;
+        if (tile == 0) {
+            st_relaxed_u32(mine, SW_INC | run);
+        } else {
+            st_relaxed_u32(mine, SW_AGG | run);
+            int32_t j = (int32_t)tile - 1;
+            unsigned int spins = 0;
+            bool done = false;
+            while (!done) {
+                uint32_t w[SW_WINDOW];
+#pragma unroll
+                for (int q = 0; q < SW_WINDOW; q++)
+                    w[q] = j - q >= 0 ? ld_relaxed_u32(status + (size_t)(j - q) * RADIX + d) : SW_INC;
+                int q = 0;
+                for (; q < SW_WINDOW; q++) {
+                    if (!(w[q] & (SW_AGG | SW_INC))) break;  // not published yet: reload from here
+                    excl += w[q] & SW_VAL;
+                    if (w[q] & SW_INC) {
+                        done = true;
+                        break;
+                    }
+                }
+                j -= q;
+                if (!done && q < SW_WINDOW && ++spins > SW_WAIT_LIMIT) {
+                    raise_error(st, ERR_WAIT_EXPIRED, tile);
+                    break;
+                }
+            }
+            st_relaxed_u32(mine, SW_INC | (excl + run));
+        }
+        gbase[d] = bases[d] + excl;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int s = 0; s < SORT_ITEMS; s++) {
+        if (valid_mask & (1u << s)) {
+            const uint32_t d = digit_of(k[s], shift, mask);
+            const uint32_t dst = gbase[d] + wcnt[warp][d] + pos[s];
+            if (dst < in.N) {
+                kout[dst] = k[s];
+                vout[dst] = v[s];
+            } else {
+                raise_error(st, ERR_BOUND, dst);
+            }
+        }
+    }
+}
+
 }  // namespace
 
 // Sorts vertex ids by descending key (ascending id on ties) into `out`.  key_bits: number of low
@@ -190,20 +339,23 @@ gc_status gc_sort_vertices(gc_graph *g, const uint32_t *keys, int key_bits, int 
     const uint32_t N = g->N;
     if (N == 0) return GC_OK;
     if ((s = gc_alloc(ctx, &g->sort_buf, 4 * (size_t)g->cap_N, "sort buffers")) != GC_OK) return s;
+    const int passes = key_bits <= 0 ? 1 : (key_bits + 7) / 8;
     const uint32_t ntiles = (N + SORT_TILE - 1) / SORT_TILE;
-    // tile counts, then per pass: digit totals and digit bases (4 passes at most)
-    const size_t hist_words = (size_t)RADIX * ntiles + 4 * 2 * RADIX;
-    if (g->sort_hist_cap < hist_words) {
+    // digit totals and bases (4 passes at most), tile counters, then the tiles' status words per pass
+    const size_t head = 2 * 4 * RADIX + 4;
+    const size_t words = head + (size_t)passes * ntiles * RADIX;
+    if (g->sort_hist_cap < words) {
         gc_dev_free(ctx, g->sort_hist);
         g->sort_hist = nullptr;
-        if ((s = gc_alloc(ctx, &g->sort_hist, hist_words, "sort histogram")) != GC_OK) return s;
-        g->sort_hist_cap = (uint32_t)hist_words;
+        if ((s = gc_alloc(ctx, &g->sort_hist, words, "sort histogram")) != GC_OK) return s;
+        g->sort_hist_cap = (uint32_t)words;
     }
-    uint32_t *digit_words = g->sort_hist + (size_t)RADIX * ntiles;
-    if ((s = gc_check_cuda(ctx, cudaMemsetAsync(digit_words, 0, sizeof(uint32_t) * 4 * 2 * RADIX, ctx->stream),
-                           "sort digit totals")) != GC_OK)
+    uint32_t *totals = g->sort_hist, *bases = totals + 4 * RADIX, *tile_ctr = bases + 4 * RADIX;
+    uint32_t *status = g->sort_hist + head;
+    ProfScope ps(ctx, "sort", ctx->stream);
+    if ((s = gc_check_cuda(ctx, cudaMemsetAsync(g->sort_hist, 0, sizeof(uint32_t) * words, ctx->stream),
+                           "sort state")) != GC_OK)
         return s;
-    const int passes = key_bits <= 0 ? 1 : (key_bits + 7) / 8;
     uint32_t *k0 = g->sort_buf, *v0 = g->sort_buf + g->cap_N;
     uint32_t *k1 = g->sort_buf + 2 * (size_t)g->cap_N, *v1 = g->sort_buf + 3 * (size_t)g->cap_N;
     SortIn in{};
@@ -214,19 +366,20 @@ gc_status gc_sort_vertices(gc_graph *g, const uint32_t *keys, int key_bits, int 
     in.N = N;
     in.max_deg = max_deg;
     in.filter = filter;
-    ProfScope ps(ctx, "sort", ctx->stream);
+    in.first = 1;
+    const uint32_t mask = key_bits <= 0 ? 0u : (uint32_t)(RADIX - 1);
+    k_sort_hist_all<<<std::min<uint32_t>(ntiles, (uint32_t)ctx->num_sms * 4), SORT_THREADS, 0, ctx->stream>>>(
+        in, passes, mask, totals);
+    k_sort_scan_all<<<1, RADIX, 0, ctx->stream>>>(totals, passes, bases, d_count);
+    ctx->launches += 2;
     for (int p = 0; p < passes; p++) {
-        const int shift = 8 * p;
-        const uint32_t mask = key_bits <= 0 ? 0u : (uint32_t)(RADIX - 1);
         in.first = (p == 0);
         uint32_t *kout = (p & 1) ? k1 : k0, *vout = (p & 1) ? v1 : v0;
         if (p == passes - 1) vout = out;  // last pass writes the result directly
-        uint32_t *digit_total = digit_words + 2 * RADIX * p, *digit_base = digit_total + RADIX;
-        k_sort_hist<<<ntiles, SORT_THREADS, 0, ctx->stream>>>(in, shift, mask, g->sort_hist, ntiles, digit_total);
-        k_sort_scan_digits<<<1, RADIX, 0, ctx->stream>>>(digit_total, digit_base, p == 0 ? d_count : nullptr);
-        k_sort_scan_tiles<<<RADIX, SCAN_THREADS, 0, ctx->stream>>>(g->sort_hist, ntiles, digit_base);
-        k_sort_scatter<<<ntiles, SORT_THREADS, 0, ctx->stream>>>(in, shift, mask, g->sort_hist, ntiles, kout, vout);
-        ctx->launches += 4;
+        k_sort_sweep<<<ntiles, SORT_THREADS, 0, ctx->stream>>>(in, 8 * p, mask, bases + p * RADIX,
+                                                                status + (size_t)p * ntiles * RADIX, tile_ctr + p,
+                                                                kout, vout, ctx->dstate);
+        ctx->launches++;
         if ((s = gc_check_launch(ctx, "radix sort")) != GC_OK) return s;
         in.kin = kout;
         in.vin = vout;
