@@ -442,7 +442,8 @@ constexpr int CORE_PEND = 256;                 // per warp: uncolored predecesso
 constexpr uint32_t CORE_MAX = 32768;           // most core tickets (16-bit ranks, 64 KB replica)
 constexpr int CORE_LOADS = 8;                  // per lane: predecessor ranks in flight in the first pass
 constexpr int CORE_PUB = 8;                    // published seen colors per core ticket: 8 words, colors 1..256
-constexpr uint32_t CORE_DECIDE = 32;           // early decisions are tried with at most this many pending
+constexpr uint32_t CORE_DECIDE = 32;           // at most this many pending: one per lane, early decisions tried
+static_assert(CORE_DECIDE <= 32, "one pending predecessor per lane");
 
 // Tickets one CTA of a C-CTA cluster owns, for K core tickets in blocks of B (an upper bound).
 __host__ __device__ __forceinline__ uint32_t core_owned(uint32_t K, uint32_t B, uint32_t C) {
@@ -613,65 +614,16 @@ __global__ void __launch_bounds__(CORE_WARPS * 32, 1) k_jp_core(const uint4 *__r
             __syncwarp();
             const bool publish = decide && window == 0 && npend > 0;
             if (publish && lane < CORE_PUB) core_st_local(mypub + lane, fb[lane]);
-            // poll the pending entries in the local replica, moving those still uncolored to the front
-            // of the list, so that a round costs one load per lane once few are left.  With at most
-            // CORE_DECIDE left (one per lane), try the early decision: the candidate c = mex(colors
-            // seen) is the color when no pending predecessor v can take c -- count(v) + 1 < c, or c
-            // among the colors v has seen (v's published set, read from its CTA's shared memory; the
-            // lanes' loads are in flight together).  Without progress, a decision is re-tried every
-            // other round, so the remote loads do not slow the polling of the local replica.
+            // Polling.  With more than CORE_DECIDE pending, rounds over the shared list, moving the entries
+            // still uncolored to its front.  Then each lane holds at most one pending rank in a
+            // register and polls it in the local replica, and the warp acts only when a color
+            // arrives.  With one left, both outcomes are precomputed (below).  Early decisions (at
+            // most CORE_DECIDE pending): the candidate c = mex(colors seen) is the color when no
+            // pending predecessor v can take c -- count(v) + 1 < c, or c among the colors v has seen
+            // (v's published set, read from its CTA's shared memory; the lanes' loads in flight
+            // together) -- tried after each arrival and every 64 polls.
             unsigned int spins = 0;
-            bool retry = true;
-            for (;;) {
-                if (npend == 1) {
-                    // one predecessor left: both outcomes are known in advance -- c1 = mex(colors
-                    // seen), or the next free color c2 if the predecessor takes c1 -- so the warp
-                    // polls that one entry alone and answers the moment its color lands (early
-                    // decisions re-tried every 64 polls)
-                    __syncwarp();
-                    const int c1 = window_mex(fb, lane, window);
-                    const int c2 = c1 > 0 ? window_mex_after(fb, lane, window, c1) : 0;
-                    const unsigned int rk0 = pend[0];
-                    unsigned int cc = 0;
-                    for (;;) {  // lane 0 reads, the warp follows its values
-                        cc = __shfl_sync(0xffffffffu, lane == 0 ? core_ld(replica + rk0) : 0u, 0);
-                        if (cc) break;
-                        bool stop = ++spins > spin_limit;
-                        if ((spins & 1023u) == 0) stop |= __shfl_sync(0xffffffffu, lane == 0 ? ld_relaxed_u32(&st->err) : 0u, 0) != 0;
-                        if (stop) {
-                            gave_up = true;
-                            break;
-                        }
-                        if (publish && c1 > 0 && (spins & 63u) == 1u) {
-                            bool excluded = (unsigned int)cpc[rk0] + 1u < (unsigned int)c1;
-                            if (!excluded && c1 <= 32 * CORE_PUB) {
-                                const unsigned int owner = (rk0 / B) % C;
-                                const uint32_t li = (rk0 / (B * C)) * B + rk0 % B;
-                                const uint32_t word = __shfl_sync(
-                                    0xffffffffu,
-                                    lane == 0 ? core_ld_remote(pub + (size_t)li * CORE_PUB + ((uint32_t)(c1 - 1) >> 5), owner)
-                                              : 0u,
-                                    0);
-                                excluded = (word >> ((uint32_t)(c1 - 1) & 31u)) & 1u;
-                            }
-                            if (excluded) {
-                                result = c1;
-                                break;
-                            }
-                        }
-                        if (nap) __nanosleep(nap);
-                    }
-                    if (gave_up || result > 0) break;
-                    if (c1 > 0 && (cc != (unsigned int)c1 || c2 > 0)) {
-                        result = cc == (unsigned int)c1 ? c2 : c1;
-                        break;
-                    }
-                    // the window holds no answer: record the color and go on to the next window
-                    if (lane == 0) core_mark(fb, cc, window);
-                    npend = 0;
-                    __syncwarp();
-                    break;
-                }
+            while (npend > CORE_DECIDE && !gave_up) {
                 bool progress = false;
                 uint32_t kept = 0;
                 for (uint32_t c0 = 0; c0 < npend; c0 += 32) {
@@ -695,35 +647,110 @@ __global__ void __launch_bounds__(CORE_WARPS * 32, 1) k_jp_core(const uint4 *__r
                 }
                 npend = kept;
                 __syncwarp();
-                if (npend == 0) break;
                 const bool prog = __any_sync(0xffffffffu, progress);
                 if (publish && prog && lane < CORE_PUB) core_st_local(mypub + lane, fb[lane]);
-                if (publish && npend <= CORE_DECIDE && (prog || retry)) {
-                    const int cand = window_mex(fb, lane, 0);
-                    if (cand > 0) {
-                        bool undecided = false;
-                        if ((uint32_t)lane < npend) {
-                            const unsigned int rk = pend[lane];
-                            bool excluded = (unsigned int)cpc[rk] + 1u < (unsigned int)cand;
-                            if (!excluded && cand <= 32 * CORE_PUB) {
-                                const unsigned int owner = (rk / B) % C;
-                                const uint32_t li = (rk / (B * C)) * B + rk % B;
-                                const uint32_t word =
-                                    core_ld_remote(pub + (size_t)li * CORE_PUB + ((uint32_t)(cand - 1) >> 5), owner);
-                                excluded = (word >> ((uint32_t)(cand - 1) & 31u)) & 1u;
+                bool stop = ++spins > spin_limit;
+                if ((spins & 1023u) == 0) stop |= __shfl_sync(0xffffffffu, lane == 0 ? ld_relaxed_u32(&st->err) : 0u, 0) != 0;
+                if (stop) gave_up = true;
+                else if (nap && !prog) __nanosleep(nap);
+            }
+            if (!gave_up && npend > 0) {
+                uint32_t rk_l = (uint32_t)lane < npend ? pend[lane] : 0u;
+                bool fresh = true;  // try a decision at once
+                for (;;) {
+                    if (npend == 1) {
+                        // one predecessor left: both outcomes are known in advance -- c1 = mex(colors
+                        // seen), or the next free color c2 if the predecessor takes c1 -- so the warp
+                        // polls that one entry alone and answers the moment its color lands (early
+                        // decisions re-tried every 64 polls)
+                        __syncwarp();
+                        const int c1 = window_mex(fb, lane, window);
+                        const int c2 = c1 > 0 ? window_mex_after(fb, lane, window, c1) : 0;
+                        const unsigned int rk0 = pend[0];
+                        unsigned int cc = 0;
+                        for (;;) {  // lane 0 reads, the warp follows its values
+                            cc = __shfl_sync(0xffffffffu, lane == 0 ? core_ld(replica + rk0) : 0u, 0);
+                            if (cc) break;
+                            bool stop = ++spins > spin_limit;
+                            if ((spins & 1023u) == 0) stop |= __shfl_sync(0xffffffffu, lane == 0 ? ld_relaxed_u32(&st->err) : 0u, 0) != 0;
+                            if (stop) {
+                                gave_up = true;
+                                break;
                             }
-                            undecided = !excluded;
+                            if (publish && c1 > 0 && (spins & 63u) == 1u) {
+                                bool excluded = (unsigned int)cpc[rk0] + 1u < (unsigned int)c1;
+                                if (!excluded && c1 <= 32 * CORE_PUB) {
+                                    const unsigned int owner = (rk0 / B) % C;
+                                    const uint32_t li = (rk0 / (B * C)) * B + rk0 % B;
+                                    const uint32_t word = __shfl_sync(
+                                        0xffffffffu,
+                                        lane == 0 ? core_ld_remote(pub + (size_t)li * CORE_PUB + ((uint32_t)(c1 - 1) >> 5), owner)
+                                                  : 0u,
+                                        0);
+                                    excluded = (word >> ((uint32_t)(c1 - 1) & 31u)) & 1u;
+                                }
+                                if (excluded) {
+                                    result = c1;
+                                    break;
+                                }
+                            }
+                            if (nap) __nanosleep(nap);
                         }
-                        if (!__any_sync(0xffffffffu, undecided)) {
-                            result = cand;
+                        if (gave_up || result > 0) break;
+                        if (c1 > 0 && (cc != (unsigned int)c1 || c2 > 0)) {
+                            result = cc == (unsigned int)c1 ? c2 : c1;
                             break;
                         }
+                        // the window holds no answer: record the color and go on to the next window
+                        if (lane == 0) core_mark(fb, cc, window);
+                        npend = 0;
+                        __syncwarp();
+                        break;
                     }
+                    const unsigned int cc = (uint32_t)lane < npend ? core_ld(replica + rk_l) : 0u;
+                    if (__ballot_sync(0xffffffffu, cc != 0u)) {
+                        if (cc) core_mark(fb, cc, window);
+                        const bool keep = (uint32_t)lane < npend && cc == 0u;
+                        const unsigned int remain = __ballot_sync(0xffffffffu, keep);
+                        if (keep) pend[__popc(remain & ((1u << lane) - 1u))] = (unsigned short)rk_l;
+                        npend = (uint32_t)__popc(remain);
+                        __syncwarp();  // marks and the compacted list are visible
+                        rk_l = (uint32_t)lane < npend ? pend[lane] : 0u;
+                        if (publish && lane < CORE_PUB) core_st_local(mypub + lane, fb[lane]);
+                        if (npend == 0) break;
+                        fresh = true;
+                        continue;
+                    }
+                    if (publish && (fresh || (spins & 63u) == 0u)) {
+                        fresh = false;
+                        const int cand = window_mex(fb, lane, 0);
+                        if (cand > 0) {
+                            bool undecided = false;
+                            if ((uint32_t)lane < npend) {
+                                bool excluded = (unsigned int)cpc[rk_l] + 1u < (unsigned int)cand;
+                                if (!excluded && cand <= 32 * CORE_PUB) {
+                                    const unsigned int owner = (rk_l / B) % C;
+                                    const uint32_t li = (rk_l / (B * C)) * B + rk_l % B;
+                                    const uint32_t word =
+                                        core_ld_remote(pub + (size_t)li * CORE_PUB + ((uint32_t)(cand - 1) >> 5), owner);
+                                    excluded = (word >> ((uint32_t)(cand - 1) & 31u)) & 1u;
+                                }
+                                undecided = !excluded;
+                            }
+                            if (!__any_sync(0xffffffffu, undecided)) {
+                                result = cand;
+                                break;
+                            }
+                        }
+                    }
+                    bool stop = ++spins > spin_limit;
+                    if ((spins & 1023u) == 0) stop |= __shfl_sync(0xffffffffu, lane == 0 ? ld_relaxed_u32(&st->err) : 0u, 0) != 0;
+                    if (stop) {
+                        gave_up = true;
+                        break;
+                    }
+                    if (nap) __nanosleep(nap);
                 }
-                retry = !retry || prog;
-                if (++spins > spin_limit || ((spins & 1023u) == 0 && ld_relaxed_u32(&st->err))) gave_up = true;
-                if (__any_sync(0xffffffffu, gave_up)) break;
-                if (nap && !prog) __nanosleep(nap);
             }
             if (result > 0) break;  // decided early
             gave_up = __any_sync(0xffffffffu, gave_up);

@@ -200,13 +200,20 @@ __global__ void __launch_bounds__(SORT_THREADS) k_sort_hist_all(SortIn in, int p
     __syncthreads();
     const int lane = threadIdx.x & 31;
     const uint32_t n = in.N;  // the first pass's input: every vertex
-    for (uint32_t base = blockIdx.x * SORT_THREADS; base < n; base += gridDim.x * SORT_THREADS) {
-        uint32_t k, v;
-        const bool valid = sort_elem(in, base + threadIdx.x, n, k, v);
-        for (int p = 0; p < passes; p++) {
-            const uint32_t d = valid ? digit_of(k, 8 * p, mask) : 0xffffffffu;
-            const unsigned int peers = __match_any_sync(0xffffffffu, d);
-            if (valid && lane == __ffs(peers) - 1) atomicAdd(&hist[p][d], (uint32_t)__popc(peers));
+    constexpr int H = 8;      // elements per thread and round, their loads in flight together
+    for (uint32_t base = blockIdx.x * SORT_THREADS * H; base < n; base += gridDim.x * SORT_THREADS * H) {
+        uint32_t k[H], v[H], valid = 0;
+#pragma unroll
+        for (int h = 0; h < H; h++)
+            if (sort_elem(in, base + h * SORT_THREADS + threadIdx.x, n, k[h], v[h])) valid |= 1u << h;
+#pragma unroll
+        for (int h = 0; h < H; h++) {
+            for (int p = 0; p < passes; p++) {
+                const bool ok = (valid >> h) & 1u;
+                const uint32_t d = ok ? digit_of(k[h], 8 * p, mask) : 0xffffffffu;
+                const unsigned int peers = __match_any_sync(0xffffffffu, d);
+                if (ok && lane == __ffs(peers) - 1) atomicAdd(&hist[p][d], (uint32_t)__popc(peers));
+            }
         }
     }
     __syncthreads();
@@ -257,10 +264,12 @@ __global__ void __launch_bounds__(SORT_THREADS) k_sort_sweep(SortIn in, int shif
     uint32_t valid_mask = 0;
     const unsigned int lt = (1u << lane) - 1u;
 #pragma unroll
+    for (int s = 0; s < SORT_ITEMS; s++) {  // every load in flight before the ranking
+        if (sort_elem(in, wbase + s * 32 + lane, n, k[s], v[s])) valid_mask |= 1u << s;
+    }
+#pragma unroll
     for (int s = 0; s < SORT_ITEMS; s++) {
-        const uint32_t j = wbase + s * 32 + lane;
-        const bool valid = sort_elem(in, j, n, k[s], v[s]);
-        if (valid) valid_mask |= 1u << s;
+        const bool valid = (valid_mask >> s) & 1u;
         const uint32_t d = valid ? digit_of(k[s], shift, mask) : 0xffffffffu;
         const unsigned int peers = __match_any_sync(0xffffffffu, d);
         const uint32_t before = valid ? wcnt[warp][d] : 0;
