@@ -421,9 +421,10 @@ __global__ void k_jp_records(const uint32_t *__restrict__ order, const uint32_t 
 // distributed shared memory instead:
 //   - each CTA holds a replica of the K core colors (16 bits each) in its shared memory;
 //   - tickets go to the CTAs in blocks of B consecutive ones (block k to CTA k % C), so a short link
-//     of a chain often stays inside one SM; a CTA's tickets, in order, go round its W warps.  A warp
-//     takes its tickets in order, so it waits only on smaller tickets (held by other warps or done)
-//     and the oldest unfinished ticket always progresses;
+//     of a chain often stays inside one SM; a CTA hands its tickets out in order to whichever warp
+//     is free (a counter in shared memory).  A warp waits only on smaller tickets, and the oldest
+//     unfinished ticket is always held by a warp (all of its CTA's warps would otherwise hold older
+//     ones), so it always progresses;
 //   - the owner writes a color into all C replicas (lane i stores into CTA i) and to global memory;
 //     waiting warps poll their own replica;
 //   - a core vertex's predecessors are sources (color 1, known before) or inner vertices with smaller
@@ -541,6 +542,7 @@ __global__ void __launch_bounds__(CORE_WARPS * 32, 1) k_jp_core(const uint4 *__r
                                                                 uint32_t kmax, uint32_t B, unsigned int nap,
                                                                 bool decide) {
     extern __shared__ __align__(16) unsigned char core_smem[];
+    __shared__ uint32_t next_local;  // this CTA's next ticket (its index among the CTA's tickets)
     const unsigned int C = cluster_size(), me = cluster_rank();
     const uint32_t kr = (kmax + 7u) & ~7u;
     unsigned short *replica = reinterpret_cast<unsigned short *>(core_smem);  // colors, kr
@@ -555,12 +557,17 @@ __global__ void __launch_bounds__(CORE_WARPS * 32, 1) k_jp_core(const uint4 *__r
         cpc[i] = (unsigned short)(rec[i].w >> 1);
     }
     for (uint32_t i = threadIdx.x; i < npub * CORE_PUB; i += blockDim.x) pub[i] = 0;
+    if (threadIdx.x == 0) next_local = 0;
     cluster_sync_all();  // every replica is zeroed before any remote store
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     uint32_t *fb = fb_all + warp * 32;
     unsigned short *pend = pend_all + warp * CORE_PEND;
-    const uint32_t W = blockDim.x >> 5;
-    for (uint32_t i = (uint32_t)warp;; i += W) {
+    for (;;) {
+        // a free warp takes the CTA's next ticket: tickets start in order, and none waits for a
+        // particular busy warp
+        uint32_t i = 0;
+        if (lane == 0) i = atomicAdd(&next_local, 1u);
+        i = __shfl_sync(0xffffffffu, i, 0);
         const uint32_t t = ((i / B) * C + me) * B + i % B;  // this CTA's i-th ticket
         if (t >= K) break;
         uint32_t *mypub = pub + (size_t)i * CORE_PUB;  // i = the ticket's index among this CTA's
@@ -1190,7 +1197,10 @@ gc_status core_cluster_config(gc_ctx *ctx) {
     gc_status s = gc_check_cuda(ctx, cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device),
                                 "smem per block");
     if (s != GC_OK) return s;
-    const size_t smem = (size_t)optin;
+    cudaFuncAttributes fa{};
+    s = gc_check_cuda(ctx, cudaFuncGetAttributes(&fa, k_jp_core), "core attributes");
+    if (s != GC_OK) return s;
+    const size_t smem = (size_t)optin - fa.sharedSizeBytes;  // the dynamic part: the rest is static
     ctx->jp_core_smem = smem;
     s = gc_check_cuda(ctx, cudaFuncSetAttribute(k_jp_core, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
                                 "core smem");

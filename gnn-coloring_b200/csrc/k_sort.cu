@@ -208,11 +208,20 @@ __global__ void __launch_bounds__(SORT_THREADS) k_sort_hist_all(SortIn in, int p
             if (sort_elem(in, base + h * SORT_THREADS + threadIdx.x, n, k[h], v[h])) valid |= 1u << h;
 #pragma unroll
         for (int h = 0; h < H; h++) {
+            const bool ok = (valid >> h) & 1u;
+            const unsigned int okm = __ballot_sync(0xffffffffu, ok);
+            if (!okm) continue;
+            const int leader = __ffs(okm) - 1;
             for (int p = 0; p < passes; p++) {
-                const bool ok = (valid >> h) & 1u;
-                const uint32_t d = ok ? digit_of(k[h], 8 * p, mask) : 0xffffffffu;
-                const unsigned int peers = __match_any_sync(0xffffffffu, d);
-                if (ok && lane == __ffs(peers) - 1) atomicAdd(&hist[p][d], (uint32_t)__popc(peers));
+                // one atomic for the warp when its valid elements share the digit (the high digits of
+                // clustered keys), else one per element (spread digits rarely collide)
+                const uint32_t d = ok ? digit_of(k[h], 8 * p, mask) : 0u;
+                const uint32_t d0 = __shfl_sync(0xffffffffu, d, leader);
+                if (__all_sync(0xffffffffu, !ok || d == d0)) {
+                    if (lane == leader) atomicAdd(&hist[p][d0], (uint32_t)__popc(okm));
+                } else if (ok) {
+                    atomicAdd(&hist[p][d], 1u);
+                }
             }
         }
     }
