@@ -21,6 +21,10 @@ struct gc_prof_rec {
 // sums are evaluated exactly by whole warps before each layer); above GC_GNN_WARP_DEGREE the split
 // gives it a warp.
 constexpr uint32_t GC_GNN_HUB_DEGREE = 16384;
+// Giant hubs (GNN): at least this many neighbours, and a third of the largest degree; their staged
+// rows take at most GC_GIANT_MAX_ROWS padded rows (16 floats each).
+constexpr uint32_t GC_GIANT_MIN_DEGREE = 32768;
+constexpr uint64_t GC_GIANT_MAX_ROWS = 1ull << 24;
 constexpr uint32_t GC_GNN_WARP_DEGREE = 256;
 // The GNN layers' own warp tier (degree schedule): a warp stages 32 rows through shared memory, which
 // costs about 2.5 L1 wavefronts per row against 1 for the four-lane tier, so only vertices whose lists
@@ -34,8 +38,8 @@ struct gc_ctx {
     cudaStream_t hub_stream = nullptr;   // GNN: the hubs' kernel beside the layer kernel (high priority)
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     bool gnn_hub_side = false;           // GNN: hubs beside the layer kernel (GC_GNN_HUB_SIDE=1), else before it
-    uint32_t gnn_hub_ctas_per_sm = 2;    // GNN: persistent hub CTAs per SM (GC_GNN_HUB_CTAS)
-    bool hub_smem_set[3] = {false, false, false};  // hub kernels' shared-memory limit raised
+    uint32_t gnn_hub_ctas_per_sm = 0;    // GNN: persistent hub CTAs per SM at most (0: as many as fit; GC_GNN_HUB_CTAS)
+    int hub_blocks_per_sm[3] = {0, 0, 0};  // resident CTAs of each hub kernel
     cudaStream_t copy_stream = nullptr;  // host copies that overlap work on `stream` (created on first use)
     cudaEvent_t ev_copy_fence = nullptr, ev_copy_done = nullptr;
     int color_blocks_per_sm = 0;         // resident CTAs of the coloring kernel (occupancy query)
@@ -127,6 +131,11 @@ struct gc_graph {
     uint32_t n_hubs = 0;
     uint32_t *hub_aux = nullptr;     // GNN: per hub 16 feature sums, then one completion counter each
     size_t hub_aux_cap = 0;
+    uint32_t n_giant = 0;            // the leading hubs whose rows the GNN stages (see k_hub_stage)
+    uint32_t giant_rows = 0;         // their degrees, each padded to a multiple of 1,024
+    uint32_t *giant_off = nullptr;   // n_giant + 1 first padded rows
+    float *hub_stage = nullptr;      // GNN: 16 x giant_rows staged feature values
+    size_t hub_stage_cap = 0;
     uint32_t *gnn_ctr = nullptr;     // GNN: 8 work counters (bulk hand-out)
     uint32_t *vorder = nullptr;      // the other vertices by descending degree (GNN schedule)
     uint32_t n_vorder = 0;

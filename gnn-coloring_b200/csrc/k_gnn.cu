@@ -585,20 +585,30 @@ __device__ __forceinline__ Xd xd_after(const Xd &f, const Xd &g) {  // f, then g
     return h;
 }
 
-// Value r of a column sits at hx_pos(r): lane l's 32 values (r = 32l + k) fill the 32-word block l,
-// their 16-byte chunk k >> 2 at chunk (k >> 2) ^ (l & 7).  A lane reads its block as 8 float4s, and
-// the 8 lanes of each quarter warp then touch 8 distinct chunks (no bank conflict); the producer's
-// stores of 32 consecutive rows (one block) hit 32 distinct banks.
-__device__ __forceinline__ uint32_t hx_pos(uint32_t r) {
-    return (r & ~31u) | (((((r >> 2) ^ (r >> 5)) & 7u)) << 2) | (r & 3u);
+// A step's column holds VPL values per lane (32 for a 1,024-value step, 16 for 512): value r = VPL*l + k
+// of lane l sits in the lane's VPL-word block, its 16-byte chunk k >> 2 at chunk (k >> 2) ^ sw(l), with
+// sw(l) = l & 7 for VPL 32 and (l >> 1) & 3 for VPL 16.  A lane reads its block as float4s, and the
+// 8 lanes of each quarter warp then touch 8 distinct 16-byte bank groups (no conflict); the
+// producer's stores of 32 consecutive rows hit 32 distinct banks.
+template <int VPL>
+__device__ __forceinline__ uint32_t hx_sw(uint32_t l) {
+    return VPL == 32 ? (l & 7u) : ((l >> 1) & 3u);
 }
-__device__ __forceinline__ uint32_t hx_slot(uint32_t k, uint32_t l) { return ((((k >> 2) ^ l) & 7u) << 2) | (k & 3u); }
+template <int VPL>
+__device__ __forceinline__ uint32_t hx_slot(uint32_t k, uint32_t l) {
+    return ((((k >> 2) ^ hx_sw<VPL>(l)) & (VPL / 4 - 1)) << 2) | (k & 3u);
+}
+template <int VPL>
+__device__ __forceinline__ uint32_t hx_pos(uint32_t r) {
+    return (r & ~(uint32_t)(VPL - 1)) | hx_slot<VPL>(r & (VPL - 1), r / VPL);
+}
 
-// The 32 values of lane c added to s with FP32 adds, in order (every lane reads them: broadcasts).
+// The VPL values of lane c added to s with FP32 adds, in order (every lane reads them: broadcasts).
+template <int VPL>
 __device__ __forceinline__ void serial_lane(float &s, const float *col, uint32_t c) {
-    const float *cp = col + 32u * c;
+    const float *cp = col + (uint32_t)VPL * c;
 #pragma unroll 8
-    for (uint32_t k = 0; k < 32; k++) s = __fadd_rn(s, cp[hx_slot(k, c)]);
+    for (uint32_t k = 0; k < VPL; k++) s = __fadd_rn(s, cp[hx_slot<VPL>(k, c)]);
 }
 
 // Parity (0/1) of the increments at the positions of mask m.
@@ -612,9 +622,9 @@ __device__ __forceinline__ uint32_t grid_increment(float xv, bool &tie) {
     return __float2uint_rz(qf) + (r > 0.5f ? 1u : 0u);
 }
 
-// Adds one step of 1,024 values to s, bit-identical to the serial chain.  col is the step's column
-// in shared memory, value r at col[hx_pos(r)], +0 past the column's end; lane l takes values
-// 32l .. 32l+31.
+// Adds one step of 32 * VPL values to s, bit-identical to the serial chain.  col is the step's column
+// in shared memory, value r at col[hx_pos<VPL>(r)], +0 past the column's end; lane l takes values
+// VPL*l .. VPL*l + VPL-1.
 //
 // A lane's transducer: without ties it adds the total t of its increments (rounded to nearest) and
 // flips the parity by t's.  With ties at k_1 < ... < k_n, built from two bit masks, pm (increment odd)
@@ -624,29 +634,31 @@ __device__ __forceinline__ uint32_t grid_increment(float xv, bool &tie) {
 // one.  The masks are only built (a second pass over the lane's values) when a tie was seen.  Values
 // with a/u >= 2^24, negative ones (-0 included), Inf and NaN all have float bits >= those of 2^24 once
 // scaled, so one unsigned maximum flags them, and their lane is added serially.
+template <int VPL>
 __device__ __forceinline__ void exact_step(float &s, const float *col, int lane) {
+    constexpr uint32_t CH = VPL / 4;  // float4 chunks per lane
     uint32_t start = 0;  // lanes [0, start) are in s (warp-uniform)
-    const float4 *colp = reinterpret_cast<const float4 *>(col + 32u * (uint32_t)lane);
-    const uint32_t sw = (uint32_t)lane & 7u;
+    const float4 *colp = reinterpret_cast<const float4 *>(col + (uint32_t)VPL * (uint32_t)lane);
+    const uint32_t sw = hx_sw<VPL>((uint32_t)lane);
     while (start < 32) {
         const bool act = (uint32_t)lane >= start;
         if (s == 0.0f) {
             bool nz = false;
 #pragma unroll
-            for (uint32_t j = 0; j < 8; j++) {
+            for (uint32_t j = 0; j < CH; j++) {
                 const float4 v = colp[j ^ sw];
                 nz |= (v.x != 0.0f) | (v.y != 0.0f) | (v.z != 0.0f) | (v.w != 0.0f);
             }
             const unsigned int nzm = __ballot_sync(FULL, act && nz);
             if (!nzm) return;
             const uint32_t c = (uint32_t)(__ffs(nzm) - 1);
-            serial_lane(s, col, c);
+            serial_lane<VPL>(s, col, c);
             start = c + 1u;
             continue;
         }
         const uint32_t be = (__float_as_uint(s) >> 23) & 0xffu;
         if (be < 24u || be == 255u) {
-            serial_lane(s, col, start);
+            serial_lane<VPL>(s, col, start);
             start++;
             continue;
         }
@@ -658,7 +670,7 @@ __device__ __forceinline__ void exact_step(float &s, const float *col, int lane)
             uint32_t ta = 0, tb = 0, umax = 0;  // two partial sums in flight
             bool anytie = false;
 #pragma unroll
-            for (uint32_t j = 0; j < 8; j++) {
+            for (uint32_t j = 0; j < CH; j++) {
                 const float4 v = colp[j ^ sw];
                 const float xs[4] = {__fmul_rn(v.x, scale), __fmul_rn(v.y, scale), __fmul_rn(v.z, scale),
                                      __fmul_rn(v.w, scale)};
@@ -673,7 +685,7 @@ __device__ __forceinline__ void exact_step(float &s, const float *col, int lane)
                 }
             }
             bad = umax >= 0x4B800000u;               // 2^24
-            const uint32_t t = min(ta + tb, EXACT_SAT);  // without bad values at most 32 (2^24 - 1)
+            const uint32_t t = min(ta + tb, EXACT_SAT);  // without bad values at most VPL (2^24 - 1)
             if (!anytie || bad) {
                 x.t0 = x.t1 = t;
                 x.p0 = t & 1u;
@@ -681,7 +693,7 @@ __device__ __forceinline__ void exact_step(float &s, const float *col, int lane)
             } else {
                 uint32_t pm = 0, tm = 0;
 #pragma unroll
-                for (uint32_t j = 0; j < 8; j++) {
+                for (uint32_t j = 0; j < CH; j++) {
                     const float4 v = colp[j ^ sw];
                     const float xs[4] = {__fmul_rn(v.x, scale), __fmul_rn(v.y, scale), __fmul_rn(v.z, scale),
                                          __fmul_rn(v.w, scale)};
@@ -726,18 +738,40 @@ __device__ __forceinline__ void exact_step(float &s, const float *col, int lane)
         const uint32_t c = (uint32_t)(__ffs(cm) - 1);
         const uint32_t before = __shfl_sync(FULL, I, c > 0 ? (int)c - 1 : 0);
         if (c > start) s = __fmul_rn(__uint2float_rn(m + before), unscale);
-        serial_lane(s, col, c);
+        serial_lane<VPL>(s, col, c);
         start = c + 1u;
     }
 }
 
-// Hub items share one layout: per step, the group pieces of 1,024 neighbour rows (a float4 of four
-// features, or the float2 of the layer-0 inputs) become a feature-major tile in shared memory,
-// XOR-swizzled (hx_pos) so that both the producer's stores of 32 consecutive rows and each feature
-// warp's reads of its contiguous per-lane runs hit 32 distinct banks.
-
-constexpr int HX_STAGE = 3;  // staging ring: steps of rows in flight (cp.async)
-constexpr int HX_TILES = 3;  // column tiles ready or being summed: how far the feature warps may drift
+// Hub work comes in two kinds of item, both evaluated with exact_step on feature-major column tiles
+// in shared memory (the swizzled layout of hx_pos):
+//   - a hub item (kind A): one hub, all its features at once.  Producer warps copy each step's
+//     neighbour rows whole -- one 64-byte request per row (the float2 of layer-0 inputs in the input
+//     layer) -- by cp.async into a staging ring, and transpose them into the column tiles; one feature
+//     warp per feature sums its column.  One request per row, not one per feature group: a single
+//     SM issues about one miss request per two cycles, which bounds any per-SM gather of scattered
+//     rows;
+//   - a staged item (kind B): a giant hub's group of features (4; in the input layer 1).  Before the
+//     layer, k_hub_stage gathers the giant hubs' rows with the whole GPU into a feature-major buffer
+//     already in the tiles' layout, so a staged item's producer moves each step's columns with one
+//     bulk copy per feature, and the giant hub's chain runs on several SMs at its arithmetic speed.
+// The hub's last item to finish (a counter per hub) runs the dense part.
+template <int MODE>
+struct HubCfg {
+    static constexpr int NWA = MODE == MODE_INPUT ? 2 : FEAT;  // hub items: feature warps (all features)
+    static constexpr int VPLA = MODE == MODE_INPUT ? 32 : 16;  // hub items: values per lane and step
+    static constexpr int STEPA = 32 * VPLA;                    // rows per step
+    static constexpr int NP = MODE == MODE_INPUT ? 1 : 2;      // producer warps
+    static constexpr int ROWB = MODE == MODE_INPUT ? 8 : 64;   // bytes of a staged row
+    static constexpr int STA = 2;                              // staging ring depth (steps of rows)
+    static constexpr int NWB = MODE == MODE_INPUT ? 1 : 4;     // staged items: features per item
+    static constexpr int NGB = (MODE == MODE_INPUT ? 2 : FEAT) / NWB;  // staged items per giant hub
+    static constexpr int THREADS = 32 * (NWA + NP);
+    static constexpr size_t SMEM_A = sizeof(float) * 3 * NWA * STEPA + (size_t)STA * STEPA * ROWB;
+    static constexpr size_t SMEM_B = sizeof(float) * 3 * NWB * HX_TILE;
+    static constexpr size_t SMEM = SMEM_A > SMEM_B ? SMEM_A : SMEM_B;
+};
+constexpr int HX_TILES = 3;                       // column tiles ready or being summed
 constexpr unsigned int HX_WAIT_LIMIT = 1u << 22;  // polls of one mbarrier phase
 
 __device__ __forceinline__ void cp_async_16(void *smem, const void *gmem) {
@@ -762,6 +796,20 @@ __device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned int count) {
 __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
     asm volatile("{\n .reg .b64 st;\n mbarrier.arrive.shared::cta.b64 st, [%0];\n}" ::"r"(smem_u32(bar)) : "memory");
 }
+// One arrival that also announces `bytes` of bulk copies completing on the same phase.
+__device__ __forceinline__ void mbar_arrive_tx(uint64_t *bar, unsigned int bytes) {
+    asm volatile("{\n .reg .b64 st;\n mbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n}" ::"r"(smem_u32(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+// Bulk copy of `bytes` (a multiple of 16, both addresses 16-byte aligned) from global to this CTA's
+// shared memory, completing on mbarrier `bar`.
+__device__ __forceinline__ void bulk_load(void *smem, const void *gmem, unsigned int bytes, uint64_t *bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(smem)),
+                 "l"(gmem), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
 __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned int parity) {
     unsigned int ok;
     asm volatile(
@@ -782,86 +830,149 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned int parity, De
     return false;
 }
 
-// One (hub, feature group) item, warp-specialized.  The producer (the CTA's last warp) copies each
-// step's rows -- their group piece -- by cp.async into a staging ring of HX_STAGE steps (ids read a
-// step ahead), waits for its own copies, writes them as swizzled feature columns into the tile ring
-// slot released by the feature warps (mbarrier `empty`, one arrival per feature warp), and marks it
-// full (mbarrier `full`).  Each feature warp sums its column step by step on its own, so a slow
-// feature (a tie, a change of binade) does not hold the others back by more than the ring's depth.
-// T counts the CTA's steps over all its items, so the barriers' phases continue from item to item.
-template <int MODE, int NG, int NW>
-__device__ __forceinline__ bool hubx_item(uint32_t h, uint32_t g, uint32_t &T, const uint32_t *__restrict__ V,
-                                          const uint32_t *__restrict__ E, const uint32_t *__restrict__ hubs,
-                                          const float2 *__restrict__ t01, const float *__restrict__ x,
-                                          float *__restrict__ sums, unsigned char *smem, uint64_t *full,
-                                          uint64_t *empty, DevState *st) {
-    constexpr int PER = (int)HX_TILE / 32;                // rows per producer lane per step
-    constexpr int PIECE = (MODE == MODE_INPUT) ? 8 : 16;  // bytes of a row's group piece
-    float *tiles = reinterpret_cast<float *>(smem);                                     // HX_TILES x NW x HX_TILE
-    unsigned char *ring = smem + sizeof(float) * HX_TILES * NW * HX_TILE;               // HX_STAGE x HX_TILE pieces
+// Giant hubs' rows, feature-major: feature f of a giant hub's row r sits at
+// stage[f * R + off + (r & ~1023) + hx_pos<32>(r & 1023)], off its first padded row (a multiple of
+// 1,024; rows past the degree are +0) and R all giant hubs' padded rows.  One warp per 32 rows: four
+// lanes read a row's four 16-byte pieces together (one request per row), and each store instruction
+// fills four features' 8-row runs.
+template <int MODE>
+__global__ void __launch_bounds__(256) k_hub_stage(const uint32_t *__restrict__ V, const uint32_t *__restrict__ E,
+                                                   const uint32_t *__restrict__ hubs, const uint32_t *__restrict__ off,
+                                                   uint32_t n_giant, uint32_t R, const float2 *__restrict__ t01,
+                                                   const float *__restrict__ x, float *__restrict__ stage) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t nchunks = R / 32;
+    for (uint32_t c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < nchunks; c += (gridDim.x * blockDim.x) >> 5) {
+        const uint32_t p0 = 32 * c;  // first padded position of the chunk
+        uint32_t h = 0;
+        while (h + 1 < n_giant && off[h + 1] <= p0) h++;
+        const uint32_t u = hubs[h], beg = V[u], d = V[u + 1] - beg;
+        const uint32_t r0 = p0 - off[h];  // the chunk's first row (a multiple of 32)
+        const uint32_t base = off[h] + (r0 & ~1023u);
+        const uint32_t myid = r0 + lane < d ? __ldg(E + beg + r0 + lane) : 0u;
+        if (MODE == MODE_INPUT) {
+            const uint32_t r = r0 + lane, pos = base + hx_pos<32>(r & 1023u);
+            const float2 v = r < d ? __ldg(t01 + myid) : make_float2(0.0f, 0.0f);
+            stage[pos] = v.x;
+            stage[R + pos] = v.y;
+        } else {
+            const int q = lane & 3;
+            float4 a[4];
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                const uint32_t m = 8 * i + (lane >> 2);  // the row of this lane's piece
+                const uint32_t v = __shfl_sync(0xffffffffu, myid, (int)m);
+                a[i] = r0 + m < d ? __ldg(reinterpret_cast<const float4 *>(x) + (size_t)v * 4 + q)
+                                  : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            }
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                const uint32_t m = 8 * i + (lane >> 2);
+                const size_t pos = base + hx_pos<32>((r0 + m) & 1023u);
+                stage[(size_t)(4 * q + 0) * R + pos] = a[i].x;
+                stage[(size_t)(4 * q + 1) * R + pos] = a[i].y;
+                stage[(size_t)(4 * q + 2) * R + pos] = a[i].z;
+                stage[(size_t)(4 * q + 3) * R + pos] = a[i].w;
+            }
+        }
+    }
+}
+
+// A hub item (kind A): hub h, all features.  Producer warp p copies rows [p, p+1) * STEP/NP of each
+// step -- four lanes per 64-byte row, one 16-byte piece each, stored at a piece slot XOR-rotated by
+// the row so the transpose's loads of 8 consecutive rows hit 8 distinct bank groups -- into a staging
+// ring of STA steps (ids read a step ahead), waits for its own copies, writes them as swizzled
+// feature columns into the tile ring slot the feature warps released (mbarrier `empty`), and marks
+// it full (mbarrier `full`, one arrival per producer warp).  T counts the CTA's kind-A steps over
+// all its items, so the barriers' phases continue from item to item.
+template <int MODE>
+__device__ __forceinline__ bool hub_item(uint32_t h, uint32_t &T, const uint32_t *__restrict__ V,
+                                         const uint32_t *__restrict__ E, const uint32_t *__restrict__ hubs,
+                                         const float2 *__restrict__ t01, const float *__restrict__ x,
+                                         float *__restrict__ sums, unsigned char *smem, uint64_t *full, uint64_t *empty,
+                                         DevState *st) {
+    using Cfg = HubCfg<MODE>;
+    constexpr int NW = Cfg::NWA, VPL = Cfg::VPLA, STEP = Cfg::STEPA, NP = Cfg::NP, ROWB = Cfg::ROWB, STA = Cfg::STA;
+    constexpr int LPR = ROWB >= 16 ? ROWB / 16 : 1;  // lanes per row
+    constexpr int RPP = STEP / NP;                   // rows per producer warp and step
+    constexpr int NI = RPP * LPR / 32;               // copies per lane and step
+    constexpr int NID = RPP / 32;                    // row ids per lane and step (lane l: rows l + 32 j)
+    float *tiles = reinterpret_cast<float *>(smem);                                 // HX_TILES x NW x STEP
+    unsigned char *ring = smem + sizeof(float) * HX_TILES * NW * STEP;               // STA x STEP x ROWB
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const uint32_t u = hubs[h], beg = V[u], d = V[u + 1] - beg;
-    const uint32_t nsteps = (d + HX_TILE - 1) / HX_TILE;
+    const uint32_t nsteps = (d + STEP - 1) / STEP;
     bool ok = true;
-    if (w == NW) {  // producer
-        uint32_t ids[PER];
+    if (w >= NW) {  // producer
+        const uint32_t p = (uint32_t)(w - NW), row0 = p * RPP;
+        uint32_t ids[NID];
         auto load_ids = [&](uint32_t t) {
 #pragma unroll
-            for (int i = 0; i < PER; i++) {
-                const uint32_t r = t * HX_TILE + 32u * i + lane;
-                ids[i] = r < d ? ld_stream(E + beg + r) : 0xffffffffu;
+            for (int j = 0; j < NID; j++) {
+                const uint32_t r = t * STEP + row0 + 32u * j + (uint32_t)lane;
+                ids[j] = r < d ? ld_stream(E + beg + r) : 0xffffffffu;
             }
         };
         auto issue = [&](uint32_t t) {  // step t's copies: one commit group, possibly empty
             if (t < nsteps) {
-                unsigned char *slot = ring + (size_t)(t % HX_STAGE) * HX_TILE * PIECE;
+                unsigned char *slot = ring + (size_t)(t % STA) * STEP * ROWB;
 #pragma unroll
-                for (int i = 0; i < PER; i++) {
-                    const uint32_t r = 32u * i + lane;
-                    if (ids[i] != 0xffffffffu) {
-                        if (MODE == MODE_INPUT) cp_async_8(slot + (size_t)r * PIECE, t01 + ids[i]);
-                        else cp_async_16(slot + (size_t)r * PIECE, x + (size_t)ids[i] * FEAT + 4u * g);
+                for (int i = 0; i < NI; i++) {
+                    const uint32_t rel = (uint32_t)(i * 32 + lane) / LPR;  // this lane's row of copy i
+                    // its id: held by lane rel % 32 as ids[rel / 32] (rel / 32 is the same in every lane)
+                    const uint32_t id = LPR == 1 ? ids[i] : __shfl_sync(0xffffffffu, ids[(i * 32) / LPR / 32], (int)(rel & 31u));
+                    const uint32_t row = row0 + rel;
+                    if (id != 0xffffffffu) {
+                        if (ROWB == 8) {
+                            cp_async_8(slot + (size_t)row * 8, t01 + id);
+                        } else {
+                            const uint32_t q = (uint32_t)lane % LPR, sq = q ^ ((row >> 1) & 3u);
+                            cp_async_16(slot + (size_t)row * 64 + 16 * sq, x + (size_t)id * FEAT + 4 * q);
+                        }
                     }
                 }
             }
             cp_async_commit();
         };
-        for (uint32_t t = 0; t + 1 < HX_STAGE; t++) {
+        for (uint32_t t = 0; t + 1 < STA; t++) {
             if (t < nsteps) load_ids(t);
             issue(t);
         }
-        if (HX_STAGE - 1 < nsteps) load_ids(HX_STAGE - 1);
+        if (STA - 1 < nsteps) load_ids(STA - 1);
         for (uint32_t t = 0; t < nsteps; t++, T++) {
-            cp_async_wait<HX_STAGE - 2>();  // step t's copies (this warp's only) have landed
+            cp_async_wait<STA - 2>();  // step t's copies (this warp's only) have landed
             __syncwarp();
             const uint32_t slot_t = T % HX_TILES;
             if (T >= HX_TILES && !mbar_wait(&empty[slot_t], ((T / HX_TILES) - 1u) & 1u, st)) {
                 ok = false;
                 break;
             }
-            const unsigned char *stg = ring + (size_t)(t % HX_STAGE) * HX_TILE * PIECE;
-            float *tile = tiles + (size_t)slot_t * NW * HX_TILE;
-#pragma unroll 4
-            for (int i = 0; i < PER; i++) {  // staged rows -> swizzled columns (rows past the end: +0)
-                const uint32_t r = 32u * i + lane;
-                const bool in = t * HX_TILE + r < d;
-                const uint32_t p = hx_pos(r);
-                if (MODE == MODE_INPUT) {
-                    const float2 v = in ? *reinterpret_cast<const float2 *>(stg + (size_t)r * PIECE) : make_float2(0.0f, 0.0f);
-                    tile[p] = v.x;
-                    tile[HX_TILE + p] = v.y;
+            const unsigned char *stg = ring + (size_t)(t % STA) * STEP * ROWB;
+            float *tile = tiles + (size_t)slot_t * NW * STEP;
+#pragma unroll 2
+            for (int i = 0; i < RPP / 32; i++) {  // staged rows -> swizzled columns (rows past the end: +0)
+                const uint32_t row = row0 + 32u * i + lane;
+                const bool in = t * STEP + row < d;
+                const uint32_t pos = hx_pos<VPL>(row);
+                if (ROWB == 8) {
+                    const float2 v = in ? *reinterpret_cast<const float2 *>(stg + (size_t)row * 8) : make_float2(0.0f, 0.0f);
+                    tile[pos] = v.x;
+                    tile[STEP + pos] = v.y;
                 } else {
-                    const float4 v = in ? *reinterpret_cast<const float4 *>(stg + (size_t)r * PIECE)
-                                        : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-                    tile[p] = v.x;
-                    tile[HX_TILE + p] = v.y;
-                    tile[(NW > 2 ? 2 : 0) * HX_TILE + p] = v.z;
-                    tile[(NW > 3 ? 3 : 0) * HX_TILE + p] = v.w;
+#pragma unroll
+                    for (uint32_t q = 0; q < 4; q++) {
+                        const float4 v = in ? *reinterpret_cast<const float4 *>(stg + (size_t)row * 64 + 16 * (q ^ ((row >> 1) & 3u)))
+                                            : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                        tile[(4 * q + 0) * STEP + pos] = v.x;
+                        tile[(4 * q + 1) * STEP + pos] = v.y;
+                        tile[(4 * q + 2) * STEP + pos] = v.z;
+                        tile[(4 * q + 3) * STEP + pos] = v.w;
+                    }
                 }
             }
             __syncwarp();  // the staging slot is read and the tile written by every lane
             if (lane == 0) mbar_arrive(&full[slot_t]);
-            const uint32_t tn = t + HX_STAGE - 1;
+            const uint32_t tn = t + STA - 1;
             issue(tn);
             if (tn + 1 < nsteps) load_ids(tn + 1);
         }
@@ -875,7 +986,68 @@ __device__ __forceinline__ bool hubx_item(uint32_t h, uint32_t g, uint32_t &T, c
                 ok = false;
                 break;
             }
-            exact_step(s, tiles + ((size_t)slot_t * NW + w) * HX_TILE, lane);
+            exact_step<VPL>(s, tiles + ((size_t)slot_t * NW + w) * STEP, lane);
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&empty[slot_t]);
+        }
+        if (ok && lane == 0) sums[h * FEAT + (uint32_t)w] = s;
+    }
+    return ok;
+}
+
+// A staged item (kind B): giant hub h, features g*NWB .. g*NWB+NWB-1, from the staging buffer.  Lane 0
+// of the first producer warp moves each step's columns with one bulk copy per feature into the tile
+// ring (mbarrier `full` carries the byte count); feature warps 0..NWB-1 sum them.  Other warps sit
+// the item out.  Before the item ends the producer waits for its copies in flight, so no bulk copy
+// outlives the item.  T counts the CTA's kind-B steps (in the warps that take part).
+template <int MODE>
+__device__ __forceinline__ bool staged_item(uint32_t h, uint32_t g, uint32_t &T, const uint32_t *__restrict__ V,
+                                            const uint32_t *__restrict__ hubs, const float *__restrict__ stage,
+                                            uint32_t off, uint32_t R, float *__restrict__ sums, unsigned char *smem,
+                                            uint64_t *full, uint64_t *empty, DevState *st) {
+    using Cfg = HubCfg<MODE>;
+    constexpr int NW = Cfg::NWB, NWA = Cfg::NWA;
+    constexpr unsigned int COL = sizeof(float) * HX_TILE;
+    float *tiles = reinterpret_cast<float *>(smem);  // HX_TILES x NW x HX_TILE
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const uint32_t u = hubs[h], d = V[u + 1] - V[u];
+    const uint32_t nsteps = (d + HX_TILE - 1) / HX_TILE;
+    bool ok = true;
+    if (w == NWA) {  // the first producer warp
+        // the tiles may last have been written through ordinary stores (a hub item): order those
+        // before the bulk copies that overwrite them
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        uint32_t t = 0;
+        for (; t < nsteps; t++, T++) {
+            const uint32_t slot_t = T % HX_TILES;
+            if (T >= HX_TILES && !mbar_wait(&empty[slot_t], ((T / HX_TILES) - 1u) & 1u, st)) {
+                ok = false;
+                break;
+            }
+            if (lane == 0) {
+                mbar_arrive_tx(&full[slot_t], NW * COL);
+#pragma unroll
+                for (int c = 0; c < NW; c++)
+                    bulk_load(tiles + ((size_t)slot_t * NW + c) * HX_TILE,
+                              stage + (size_t)(g * NW + c) * R + off + (size_t)t * HX_TILE, COL, &full[slot_t]);
+            }
+            __syncwarp();
+        }
+        // the copies of the last (up to HX_TILES) steps issued may still be in flight: wait for them
+        for (uint32_t k = 0; k < HX_TILES && k < t; k++) {
+            const uint32_t Tk = T - 1u - k;
+            mbar_wait(&full[Tk % HX_TILES], (Tk / HX_TILES) & 1u, st);
+        }
+        __syncwarp();
+    } else if (w < NW) {  // feature warp w
+        float s = 0.0f;
+        for (uint32_t t = 0; t < nsteps; t++, T++) {
+            const uint32_t slot_t = T % HX_TILES;
+            if (!mbar_wait(&full[slot_t], (T / HX_TILES) & 1u, st)) {
+                ok = false;
+                break;
+            }
+            exact_step<32>(s, tiles + ((size_t)slot_t * NW + w) * HX_TILE, lane);
             __syncwarp();
             if (lane == 0) mbar_arrive(&empty[slot_t]);
         }
@@ -931,42 +1103,56 @@ __device__ __forceinline__ void hub_dense(uint32_t h, const uint32_t *__restrict
     }
 }
 
-// Hubs (more than the hub degree), before each layer kernel: persistent CTAs take (hub, group of 4
-// features) items from a counter, heaviest hub first (the input layer: one item per hub, its two
-// layer-0 inputs); NW feature warps and one producer warp each (hubx_item).  The hub's last item to
-// finish (a counter per hub, zeroed before the layer) runs the dense part: mean, 32 x 16 FMA chain
-// in order, ReLU, and in the output layer the reference's fixed-tree sum into the key.
+// Hubs (more than the hub degree), before each layer kernel: persistent CTAs take items from a
+// counter -- the giant hubs' staged items first (heaviest first), then one hub item per other hub,
+// by descending degree.  The hub's last item to finish (a counter per hub, zeroed before the layer)
+// runs the dense part: mean, 32 x 16 FMA chain in order, ReLU, and in the output layer the
+// reference's fixed-tree sum into the key.
 template <int MODE>
-__global__ void __launch_bounds__(160) k_gnn_hubx(const uint32_t *__restrict__ V, const uint32_t *__restrict__ E,
-                                                  const uint32_t *__restrict__ hubs, const float2 *__restrict__ t01,
-                                                  const float *__restrict__ x, float *__restrict__ y,
-                                                  uint32_t *__restrict__ key, const float *__restrict__ Wb,
-                                                  float *__restrict__ sums, uint32_t *__restrict__ done,
-                                                  uint32_t *__restrict__ items, uint32_t n_hubs, DevState *st) {
-    constexpr int NG = (MODE == MODE_INPUT) ? 1 : 4;  // items (feature groups) per hub
-    constexpr int NW = (MODE == MODE_INPUT) ? 2 : 4;  // feature warps per CTA
+__global__ void __launch_bounds__(HubCfg<MODE>::THREADS) k_gnn_hubx(
+    const uint32_t *__restrict__ V, const uint32_t *__restrict__ E, const uint32_t *__restrict__ hubs,
+    const float2 *__restrict__ t01, const float *__restrict__ x, float *__restrict__ y, uint32_t *__restrict__ key,
+    const float *__restrict__ Wb, float *__restrict__ sums, uint32_t *__restrict__ done, uint32_t *__restrict__ items,
+    uint32_t n_hubs, uint32_t n_giant, const float *__restrict__ stage, const uint32_t *__restrict__ stage_off,
+    uint32_t R, DevState *st) {
+    using Cfg = HubCfg<MODE>;
     extern __shared__ __align__(16) unsigned char hx_smem[];
-    __shared__ __align__(8) uint64_t full[HX_TILES], empty[HX_TILES];
+    __shared__ __align__(8) uint64_t full_a[HX_TILES], empty_a[HX_TILES], full_b[HX_TILES], empty_b[HX_TILES];
     __shared__ uint32_t item_s, last_s;
     if (threadIdx.x == 0) {
         for (int i = 0; i < HX_TILES; i++) {
-            mbar_init(&full[i], 1);
-            mbar_init(&empty[i], NW);
+            mbar_init(&full_a[i], Cfg::NP);
+            mbar_init(&empty_a[i], Cfg::NWA);
+            mbar_init(&full_b[i], 1);
+            mbar_init(&empty_b[i], Cfg::NWB);
         }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
-    uint32_t T = 0;  // this thread's count of the CTA's steps (the same in every warp)
+    uint32_t Ta = 0, Tb = 0;  // this thread's count of the CTA's steps of each kind
+    const uint32_t n_staged = n_giant * Cfg::NGB;
+    const uint32_t n_items = n_staged + (n_hubs - n_giant);
     for (;;) {
         if (threadIdx.x == 0) item_s = atomicAdd(items, 1u);
         __syncthreads();
         const uint32_t it = item_s;
-        if (it >= n_hubs * NG) return;
-        const uint32_t h = it / NG, g = it % NG;
-        const bool ok = hubx_item<MODE, NG, NW>(h, g, T, V, E, hubs, t01, x, sums, hx_smem, full, empty, st);
+        if (it >= n_items) return;
+        uint32_t h, parts;
+        bool ok;
+        if (it < n_staged) {
+            h = it / Cfg::NGB;
+            parts = Cfg::NGB;
+            ok = staged_item<MODE>(h, it % Cfg::NGB, Tb, V, hubs, stage, stage_off[h], R, sums, hx_smem, full_b,
+                                   empty_b, st);
+        } else {
+            h = n_giant + (it - n_staged);
+            parts = 1;
+            ok = hub_item<MODE>(h, Ta, V, E, hubs, t01, x, sums, hx_smem, full_a, empty_a, st);
+        }
         if (__syncthreads_or(!ok)) return;  // a wait gave up: the error is raised
         if (threadIdx.x == 0) {
             __threadfence();
-            last_s = atomicAdd(done + h, 1u) == NG - 1;
+            last_s = atomicAdd(done + h, 1u) == parts - 1;
         }
         __syncthreads();
         if (last_s && threadIdx.x < 32) {
@@ -976,7 +1162,6 @@ __global__ void __launch_bounds__(160) k_gnn_hubx(const uint32_t *__restrict__ V
     }
 }
 
-// n_iso: trailing vertices of the degree order without neighbours that k_gnn_isolated has done.
 template <int MODE>
 gc_status launch_layer(gc_graph *g, const float *Wb, const float *x, float *y, uint32_t n_iso) {
     gc_ctx *ctx = g->ctx;
@@ -990,8 +1175,7 @@ gc_status launch_layer(gc_graph *g, const float *Wb, const float *x, float *y, u
     // hubs: persistent CTAs before the layer kernel, on the library's stream (GC_GNN_HUB_SIDE=1 puts
     // them on a high-priority side stream beside it, the layer grid then leaving one CTA per SM)
     if (g->n_hubs) {
-        constexpr uint32_t NG = (MODE == MODE_INPUT) ? 1 : 4;
-        constexpr uint32_t NW = (MODE == MODE_INPUT) ? 2 : 4;
+        using Cfg = HubCfg<MODE>;
         float *sums = reinterpret_cast<float *>(g->hub_aux);
         uint32_t *done = g->hub_aux + (size_t)FEAT * g->n_hubs;  // n_hubs counters, then the item counter
         if ((s = gc_check_cuda(ctx, cudaMemsetAsync(done, 0, sizeof(uint32_t) * (g->n_hubs + 1), ctx->stream),
@@ -1004,21 +1188,31 @@ gc_status launch_layer(gc_graph *g, const float *Wb, const float *x, float *y, u
         }
         ProfScope ph(ctx, MODE == MODE_INPUT ? "gnn_hub_input" : (MODE == MODE_HIDDEN ? "gnn_hub_hidden" : "gnn_hub_output"),
                      side);
-        // CTAs per SM (GC_GNN_HUB_CTAS, default 1): the heaviest hubs' items go first, each warp then
-        // has a scheduler of its own, and those chains bound the kernel
-        const uint32_t per_sm = ctx->gnn_hub_ctas_per_sm;
-        const uint32_t grid = std::min<uint32_t>((uint32_t)ctx->num_sms * per_sm, g->n_hubs * NG);
-        const size_t hsmem =
-            sizeof(float) * HX_TILES * NW * HX_TILE + (size_t)HX_STAGE * HX_TILE * (MODE == MODE_INPUT ? 8 : 16);
-        if (!ctx->hub_smem_set[MODE]) {  // once per context: keeps the call out of captured sequences
+        if (g->n_giant) {  // the giant hubs' rows, staged by the whole GPU
+            k_hub_stage<MODE><<<ctx->num_sms * 8, 256, 0, side>>>(g->V, g->E, g->hubs, g->giant_off, g->n_giant,
+                                                                  g->giant_rows, g->t01, x, g->hub_stage);
+            ctx->launches++;
+        }
+        int &occ = ctx->hub_blocks_per_sm[MODE];
+        if (!occ) {  // once per context: keeps these calls out of captured sequences
             if ((s = gc_check_cuda(ctx, cudaFuncSetAttribute(k_gnn_hubx<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                             (int)hsmem),
+                                                             (int)Cfg::SMEM),
                                    "hub smem")) != GC_OK)
                 return s;
-            ctx->hub_smem_set[MODE] = true;
+            if ((s = gc_check_cuda(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_gnn_hubx<MODE>, Cfg::THREADS,
+                                                                                      Cfg::SMEM),
+                                   "hub occupancy")) != GC_OK)
+                return s;
+            if (occ < 1) occ = 1;
         }
-        k_gnn_hubx<MODE><<<grid, (NW + 1) * 32, hsmem, side>>>(g->V, g->E, g->hubs, g->t01, x, y, g->key, Wb, sums,
-                                                               done, done + g->n_hubs, g->n_hubs, ctx->dstate);
+        // CTAs per SM: as many as fit, at most GC_GNN_HUB_CTAS when set
+        const uint32_t per_sm = ctx->gnn_hub_ctas_per_sm ? std::min<uint32_t>(ctx->gnn_hub_ctas_per_sm, (uint32_t)occ)
+                                                         : (uint32_t)occ;
+        const uint32_t n_items = g->n_giant * Cfg::NGB + (g->n_hubs - g->n_giant);
+        const uint32_t grid = std::min<uint32_t>((uint32_t)ctx->num_sms * per_sm, n_items);
+        k_gnn_hubx<MODE><<<grid, Cfg::THREADS, Cfg::SMEM, side>>>(g->V, g->E, g->hubs, g->t01, x, y, g->key, Wb, sums,
+                                                                 done, done + g->n_hubs, g->n_hubs, g->n_giant,
+                                                                 g->hub_stage, g->giant_off, g->giant_rows, ctx->dstate);
         ctx->launches++;
         if ((s = gc_check_launch(ctx, "gnn hubs")) != GC_OK) return s;
     }
@@ -1075,6 +1269,12 @@ gc_status gc_priority_gnn(gc_graph *g, const gc_model *m) {
         g->hub_aux = nullptr;
         if ((s = gc_alloc(ctx, &g->hub_aux, (size_t)(FEAT + 1) * g->n_hubs + 1, "hub sums")) != GC_OK) return s;
         g->hub_aux_cap = (size_t)(FEAT + 1) * g->n_hubs + 1;
+    }
+    if (g->n_giant && g->hub_stage_cap < (size_t)FEAT * g->giant_rows) {  // staged rows of the giant hubs
+        gc_dev_free(ctx, g->hub_stage);
+        g->hub_stage = nullptr;
+        if ((s = gc_alloc(ctx, &g->hub_stage, (size_t)FEAT * g->giant_rows, "giant hub rows")) != GC_OK) return s;
+        g->hub_stage_cap = (size_t)FEAT * g->giant_rows;
     }
     if (g->n_hubs && ctx->gnn_hub_side && !ctx->hub_stream) {
         int lo = 0, hi = 0;

@@ -92,6 +92,8 @@ gc_status gc_graph_prepare(gc_graph *g) {
         g->max_deg = 0;
         g->n_big_tasks = 0;
         g->n_hubs = 0;
+        g->n_giant = 0;
+        g->giant_rows = 0;
         g->n_vorder = 0;
         g->n_thin = 0;
         g->n_iso = 0;
@@ -156,7 +158,34 @@ gc_status gc_graph_prepare(gc_graph *g) {
         if ((s = gc_check_cuda(ctx, cudaMemcpyAsync(g->hubs, h.data(), 4 * (size_t)n_hubs,
                                                     cudaMemcpyHostToDevice, ctx->stream), "hub list")) != GC_OK)
             return s;
+        // giant hubs: at least GC_GIANT_MIN_DEGREE neighbours and a third of the largest degree.  Their
+        // rows are staged by the whole GPU before each GNN layer, and their features split over
+        // several SMs (k_hub_stage, k_gnn_hubx)
+        const uint32_t top = hp[2 * idx[0] + 1];
+        const uint32_t giant_deg = std::max<uint32_t>(GC_GIANT_MIN_DEGREE, top / 3);
+        std::vector<uint32_t> off(1, 0);
+        uint64_t rows = 0;
+        for (uint32_t i = 0; i < n_hubs && hp[2 * idx[i] + 1] >= giant_deg; i++) {
+            const uint64_t padded = ((uint64_t)hp[2 * idx[i] + 1] + 1023u) & ~(uint64_t)1023u;
+            if (rows + padded > GC_GIANT_MAX_ROWS) break;
+            rows += padded;
+            off.push_back((uint32_t)rows);
+        }
+        g->n_giant = (uint32_t)off.size() - 1;
+        g->giant_rows = (uint32_t)rows;
+        gc_dev_free(ctx, g->giant_off);
+        g->giant_off = nullptr;
+        if (g->n_giant) {
+            if ((s = gc_alloc(ctx, &g->giant_off, off.size(), "giant hub offsets")) != GC_OK) return s;
+            if ((s = gc_check_cuda(ctx, cudaMemcpyAsync(g->giant_off, off.data(), 4 * off.size(), cudaMemcpyHostToDevice,
+                                                        ctx->stream),
+                                   "giant hub offsets")) != GC_OK)
+                return s;
+        }
         if ((s = gc_check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "hub list")) != GC_OK) return s;
+    } else {
+        g->n_giant = 0;
+        g->giant_rows = 0;
     }
     // GNN schedule.  By degree: every non-hub vertex by descending degree (ties by id), so that the
     // vertices a warp handles together have nearly equal neighbour counts.  Graph-major (segmented
