@@ -564,7 +564,7 @@ __global__ void __launch_bounds__(THIN_THREADS, 3) k_gnn_thin(const uint32_t *__
 //     and transducers compose associatively.
 // Lane l holds values 32l .. 32l+31 of the step and builds its transducer over them for both start
 // parities; a 5-round warp scan composes the lanes in order.  The first lane whose run would carry s
-// out of the binade, or that holds a value with a/u >= 2^24 (or Inf/NaN), is added with plain FP32
+// out of the binade, or that holds a value with a/u >= 2^23 (or Inf/NaN), is added with plain FP32
 // adds in order (shuffles broadcast its values; every lane adds them, so s stays warp-uniform), and
 // the step resumes after it in the new binade.  +0 plus zeros stays +0, and a sum below 2^-103 (grid
 // or its inverse not a normal float) is also added lane by lane with FP32 adds.
@@ -572,18 +572,17 @@ constexpr uint32_t EXACT_TOP = 1u << 24;
 constexpr uint32_t EXACT_SAT = 1u << 25;  // transducer totals are clamped here: >= 2^24 means "leaves"
 constexpr uint32_t HX_TILE = 1024;        // values per step
 
+// A transducer as two words, one per start parity P: bits 0..30 the total added, bit 31 the end
+// parity (totals are clamped at EXACT_SAT < 2^31).
+constexpr uint32_t XD_P = 1u << 31, XD_T = XD_P - 1u;
 struct Xd {
-    uint32_t t0, t1;  // total added for start parity 0 / 1
-    uint32_t p0, p1;  // end parity for start parity 0 / 1
+    uint32_t w0, w1;  // start parity 0 / 1
 };
-__device__ __forceinline__ Xd xd_after(const Xd &f, const Xd &g) {  // f, then g
-    Xd h;
-    h.t0 = min(f.t0 + (f.p0 ? g.t1 : g.t0), EXACT_SAT);
-    h.t1 = min(f.t1 + (f.p1 ? g.t1 : g.t0), EXACT_SAT);
-    h.p0 = f.p0 ? g.p1 : g.p0;
-    h.p1 = f.p1 ? g.p1 : g.p0;
-    return h;
+__device__ __forceinline__ uint32_t xd_then(uint32_t f, const Xd &g) {  // f's total, then g from f's end parity
+    const uint32_t gs = (f & XD_P) ? g.w1 : g.w0;
+    return min((f & XD_T) + (gs & XD_T), EXACT_SAT) | (gs & XD_P);
 }
+__device__ __forceinline__ Xd xd_after(const Xd &f, const Xd &g) { return {xd_then(f.w0, g), xd_then(f.w1, g)}; }
 
 // A step's column holds VPL values per lane (32 for a 1,024-value step, 16 for 512): value r = VPL*l + k
 // of lane l sits in the lane's VPL-word block, its 16-byte chunk k >> 2 at chunk (k >> 2) ^ sw(l), with
@@ -631,9 +630,7 @@ __device__ __forceinline__ uint32_t grid_increment(float xv, bool &tie) {
 // and tm (value k is a tie, counted as q): the first tie adds one more when P + (increments up to and
 // including k_1) is odd (P = the start parity), each later tie k_j adds one when the increments in
 // (k_{j-1}, k_j] have odd sum, and after a tie the parity is that of the increments after the last
-// one.  The masks are only built (a second pass over the lane's values) when a tie was seen.  Values
-// with a/u >= 2^24, negative ones (-0 included), Inf and NaN all have float bits >= those of 2^24 once
-// scaled, so one unsigned maximum flags them, and their lane is added serially.
+// one.  The masks are only built (a second pass over the lane's values) when a tie was seen.
 template <int VPL>
 __device__ __forceinline__ void exact_step(float &s, const float *col, int lane) {
     constexpr uint32_t CH = VPL / 4;  // float4 chunks per lane
@@ -664,9 +661,14 @@ __device__ __forceinline__ void exact_step(float &s, const float *col, int lane)
         }
         const float scale = __uint_as_float((277u - be) << 23);  // 1/u = 2^(23-e), e = be - 127
         const uint32_t m = __float2uint_rz(__fmul_rn(s, scale));
-        Xd x = {0u, 0u, 0u, 1u};
+        Xd x = {0u, XD_P};  // identity: nothing added, parity kept
         bool bad = false;
         if (act) {
+            // Increments rounded to nearest even through the adder, 2^23 + xs: exact for 0 <= xs < 2^23
+            // (larger, negative -- -0 included --, Inf and NaN values all have float bits >= those of
+            // 2^23 once scaled, so one unsigned maximum flags them, and their lane is added serially).
+            // The bits of 2^23 + xs are summed mod 2^32, VPL offsets of 0x4B000000 removed at the end.
+            // A tie (xs - RNE(xs) = +-1/2, both exact) sends the lane to the second pass below.
             uint32_t ta = 0, tb = 0, umax = 0;  // two partial sums in flight
             bool anytie = false;
 #pragma unroll
@@ -677,21 +679,20 @@ __device__ __forceinline__ void exact_step(float &s, const float *col, int lane)
 #pragma unroll
                 for (int i = 0; i < 4; i++) {
                     umax = max(umax, __float_as_uint(xs[i]));
-                    bool tie;
-                    const uint32_t nt = grid_increment(xs[i], tie);
-                    anytie |= tie;
-                    if (i & 1) tb += nt;
-                    else ta += nt;
+                    const float yv = __fadd_rn(xs[i], 8388608.0f);
+                    if (i & 1) tb += __float_as_uint(yv);
+                    else ta += __float_as_uint(yv);
+                    anytie |= fabsf(__fsub_rn(xs[i], __fsub_rn(yv, 8388608.0f))) == 0.5f;
                 }
             }
-            bad = umax >= 0x4B800000u;               // 2^24
-            const uint32_t t = min(ta + tb, EXACT_SAT);  // without bad values at most VPL (2^24 - 1)
+            bad = umax >= 0x4B000000u;  // 2^23
             if (!anytie || bad) {
-                x.t0 = x.t1 = t;
-                x.p0 = t & 1u;
-                x.p1 = x.p0 ^ 1u;
+                const uint32_t t = min(ta + tb - (uint32_t)VPL * 0x4B000000u, EXACT_SAT);
+                x.w0 = t | ((t & 1u) << 31);
+                x.w1 = t | ((~t & 1u) << 31);
             } else {
-                uint32_t pm = 0, tm = 0;
+                // ties counted as q: totals and the masks pm (increment odd), tm (value k a tie)
+                uint32_t tq = 0, pm = 0, tm = 0;
 #pragma unroll
                 for (uint32_t j = 0; j < CH; j++) {
                     const float4 v = colp[j ^ sw];
@@ -701,10 +702,12 @@ __device__ __forceinline__ void exact_step(float &s, const float *col, int lane)
                     for (int i = 0; i < 4; i++) {
                         bool tie;
                         const uint32_t nt = grid_increment(xs[i], tie);
+                        tq += nt;
                         pm |= (nt & 1u) << (4 * j + i);
                         tm |= (tie ? 1u : 0u) << (4 * j + i);
                     }
                 }
+                const uint32_t t = min(tq, EXACT_SAT);
                 const int k1 = __ffs(tm) - 1;
                 const uint32_t first = par(pm, 0xffffffffu >> (31 - k1));  // increments 0 .. k1
                 uint32_t extra = 0, rest = tm & (tm - 1u), prev = (uint32_t)k1;
@@ -714,21 +717,19 @@ __device__ __forceinline__ void exact_step(float &s, const float *col, int lane)
                     prev = k;
                     rest &= rest - 1u;
                 }
-                x.t0 = min(t + extra + first, EXACT_SAT);          // P = 0: the first tie adds one when odd
-                x.t1 = min(t + extra + (first ^ 1u), EXACT_SAT);   // P = 1
-                x.p0 = x.p1 = prev == 31u ? 0u : par(pm, 0xffffffffu << (prev + 1u));
+                const uint32_t pe = prev == 31u ? 0u : par(pm, 0xffffffffu << (prev + 1u));  // end parity
+                x.w0 = min(t + extra + first, EXACT_SAT) | (pe << 31);          // P = 0: the first tie adds one when odd
+                x.w1 = min(t + extra + (first ^ 1u), EXACT_SAT) | (pe << 31);   // P = 1
             }
         }
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {  // inclusive composition over the lanes, in order
             Xd f;
-            f.t0 = __shfl_up_sync(FULL, x.t0, o);
-            f.t1 = __shfl_up_sync(FULL, x.t1, o);
-            f.p0 = __shfl_up_sync(FULL, x.p0, o);
-            f.p1 = __shfl_up_sync(FULL, x.p1, o);
+            f.w0 = __shfl_up_sync(FULL, x.w0, o);
+            f.w1 = __shfl_up_sync(FULL, x.w1, o);
             if (lane >= o) x = xd_after(f, x);
         }
-        const uint32_t I = (m & 1u) ? x.t1 : x.t0;  // added through this lane
+        const uint32_t I = ((m & 1u) ? x.w1 : x.w0) & XD_T;  // added through this lane
         const unsigned int cm = __ballot_sync(FULL, act && (bad || m + I >= EXACT_TOP));
         const float unscale = __uint_as_float((be - 23u) << 23);
         if (!cm) {
