@@ -764,7 +764,7 @@ struct HubCfg {
     static constexpr int STEPA = 32 * VPLA;                    // rows per step
     static constexpr int NP = MODE == MODE_INPUT ? 1 : 2;      // producer warps
     static constexpr int ROWB = MODE == MODE_INPUT ? 8 : 64;   // bytes of a staged row
-    static constexpr int STA = 2;                              // staging ring depth (steps of rows)
+    static constexpr int STA = 3;                              // staging ring depth: 2 steps of rows in flight
     static constexpr int NWB = MODE == MODE_INPUT ? 1 : 4;     // staged items: features per item
     static constexpr int NGB = (MODE == MODE_INPUT ? 2 : FEAT) / NWB;  // staged items per giant hub
     static constexpr int THREADS = 32 * (NWA + NP);
