@@ -762,7 +762,7 @@ struct HubCfg {
     static constexpr int NWA = MODE == MODE_INPUT ? 2 : FEAT;  // hub items: feature warps (all features)
     static constexpr int VPLA = MODE == MODE_INPUT ? 32 : 16;  // hub items: values per lane and step
     static constexpr int STEPA = 32 * VPLA;                    // rows per step
-    static constexpr int NP = MODE == MODE_INPUT ? 1 : 2;      // producer warps
+    static constexpr int NP = MODE == MODE_INPUT ? 1 : 4;      // producer warps
     static constexpr int ROWB = MODE == MODE_INPUT ? 8 : 64;   // bytes of a staged row
     static constexpr int STA = 3;                              // staging ring depth: 2 steps of rows in flight
     static constexpr int NWB = MODE == MODE_INPUT ? 1 : 4;     // staged items: features per item
