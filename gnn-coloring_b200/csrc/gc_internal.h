@@ -37,7 +37,7 @@ struct gc_ctx {
     cudaStream_t stream = nullptr;
     cudaStream_t hub_stream = nullptr;   // GNN: the hubs' kernel beside the layer kernel (high priority)
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
-    bool gnn_hub_side = false;           // GNN: hubs beside the layer kernel (GC_GNN_HUB_SIDE=1), else before it
+    bool gnn_hub_side = true;            // GNN: hubs on a high-priority stream beside the layer kernel (GC_GNN_HUB_SIDE=0: before it)
     uint32_t gnn_hub_ctas_per_sm = 0;    // GNN: persistent hub CTAs per SM at most (0: as many as fit; GC_GNN_HUB_CTAS)
     int hub_blocks_per_sm[3] = {0, 0, 0};  // resident CTAs of each hub kernel
     cudaStream_t copy_stream = nullptr;  // host copies that overlap work on `stream` (created on first use)

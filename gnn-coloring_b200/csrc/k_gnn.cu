@@ -1173,8 +1173,8 @@ gc_status launch_layer(gc_graph *g, const float *Wb, const float *x, float *y, u
     if ((s = gc_check_cuda(ctx, cudaMemsetAsync(ctr, 0, 8 * sizeof(uint32_t), ctx->stream), "gnn work counters")) !=
         GC_OK)
         return s;
-    // hubs: persistent CTAs before the layer kernel, on the library's stream (GC_GNN_HUB_SIDE=1 puts
-    // them on a high-priority side stream beside it, the layer grid then leaving one CTA per SM)
+    // hubs: persistent CTAs on a high-priority side stream beside the layer kernel, whose grid then
+    // leaves one CTA per SM (GC_GNN_HUB_SIDE=0: before it, on the library's stream)
     if (g->n_hubs) {
         using Cfg = HubCfg<MODE>;
         float *sums = reinterpret_cast<float *>(g->hub_aux);
