@@ -120,7 +120,8 @@ void gc_graph_free_buffers(gc_graph *g) {
                     g->big,       g->hubs,   g->x,        g->y,        g->t01,      g->deg_rem,  g->frontier,
                     g->frontier2, g->removed, g->leaf_list, g->vorder, g->rank,     g->p64,      g->seg_voff,
                     g->seg_stat,  g->fmask,    g->jprec, g->class_first,
-                    g->gnn_ctr,   g->hub_aux, g->jpsplit, g->part_tiles, g->giant_off, g->hub_stage};
+                    g->gnn_ctr,   g->hub_aux, g->jpsplit, g->part_tiles, g->giant_off, g->hub_stage,
+                    g->row_of,    g->Er,      g->vrow};
     for (void *p : bufs) gc_dev_free(ctx, p);
 }
 

@@ -390,12 +390,13 @@ void gc_tuning_default(gc_tuning *t) {
 
 uint64_t gc_batch_device_bytes(uint32_t G, uint32_t N, uint32_t M, gc_heuristic h) {
     // CSR, keys, colors, hub list, degree order, sort buffers, predecessor lists and counts, ticket
-    // order, leaf list, staged offsets, published forbidden colors, ticket records; GNN feature planes and input
-    // table; segment arrays; the
+    // order, leaf list, staged offsets, published forbidden colors, ticket records; GNN feature planes, input
+    // table, feature-row map and the neighbour ids as rows; segment arrays; the
     // split task list and sort histogram; allocation granularity.
     uint64_t per_vertex = 4 + 4 + 4 + 4 + 4 + 16 + 4 + 4 + 4 + 4 + 8 * GC_JP_MASK_WORDS + 16;
-    if (h == GC_GNN) per_vertex += 64 + 64 + 8;
-    uint64_t bytes = 8ull * M + per_vertex * N + 4ull * G + 20ull * G + 64;
+    uint64_t per_edge = 8;
+    if (h == GC_GNN) per_vertex += 64 + 64 + 8 + 4 + 8, per_edge += 4;
+    uint64_t bytes = per_edge * M + per_vertex * N + 4ull * G + 20ull * G + 64;
     bytes += 8ull * (M / GC_SPLIT_CHUNK + 1) + 4ull * (256ull * (N / 8192 + 1) + 2048);
     bytes += 24ull * (2u << 20);
     return bytes;

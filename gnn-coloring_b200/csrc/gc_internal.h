@@ -145,9 +145,15 @@ struct gc_graph {
     uint32_t n_thin = 0;             // trailing vorder entries with at most ctx->gnn_thin_deg neighbours
     uint32_t n_iso = 0;              // of those, the trailing entries without neighbours (degree schedule only)
                                      // (degree schedule only; 0 with the graph-major schedule)
-    // GNN scratch (allocated on first use)
+    // GNN scratch (allocated on first use).  Feature rows (x, y, t01) are stored in degree order:
+    // the hubs take rows 0 .. n_hubs-1 in hub order, vorder[i] takes row n_hubs + i, so rows that
+    // many lists gather share cache lines, and a warp's own rows are consecutive.
     float *x = nullptr, *y = nullptr;
     float2 *t01 = nullptr;
+    uint32_t *row_of = nullptr;  // feature row of each vertex
+    uint2 *vrow = nullptr;       // per feature row: (first CSR entry, degree) of its vertex
+    uint32_t *Er = nullptr;      // E with every neighbour id replaced by its feature row (same positions)
+    bool rows_ready = false;     // row_of and Er describe the current CSR (cleared by gc_graph_prepare)
     // SL/SLL scratch (allocated on first use)
     uint32_t *deg_rem = nullptr, *frontier = nullptr, *frontier2 = nullptr, *removed = nullptr;
     // tier thresholds and vertex schedule of the split and GNN kernels (gc_graph_prepare applies them)

@@ -22,6 +22,12 @@
 //     features) gathers the neighbour rows in steps of 1,024 into shared memory, and one warp per
 //     feature evaluates the reference's sequential FP32 chain exactly, a step at a time
 //     (exact_step below); the hub's last CTA runs its dense part.
+// Feature rows (x, y and the layer-0 table) are stored in degree order: hub h at row h, vorder[i] at
+// row n_hubs + i.  The neighbour lists are read from Er, the CSR with each id replaced by its row
+// (entry for entry, so every sum keeps the reference's order), and each row's first CSR entry and
+// degree from vrow.  The rows most lists gather then share cache lines, and a warp's own rows,
+// offsets and outputs are consecutive: on R-MAT 22 (GNN3) the three layers took 2.97 ms per job
+// against 3.33 ms with rows by vertex id.
 // Neighbour rows are read with __ldg: a layer never writes the features it reads.  In an A/B on
 // R-MAT 22 (GNN3) the explicit read-only load made the bulk hidden and output layers about 6 %
 // faster than the plain loads the compiler emits here.
@@ -37,9 +43,10 @@ using namespace gc;
 
 enum : int { MODE_INPUT = 0, MODE_HIDDEN = 1, MODE_OUTPUT = 2 };
 
-// In a segmented CSR the id feature is (local id) / (the graph's own N).
+// In a segmented CSR the id feature is (local id) / (the graph's own N).  Written at the vertex's
+// feature row.
 __global__ void k_gnn_table0(const uint32_t *__restrict__ V, uint32_t N, float fmd, const uint32_t *__restrict__ voff,
-                             uint32_t nseg, float2 *__restrict__ t01) {
+                             uint32_t nseg, const uint32_t *__restrict__ row_of, float2 *__restrict__ t01) {
     for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < N; u += gridDim.x * blockDim.x) {
         uint32_t d = V[u + 1] - V[u];
         uint32_t base = 0, n = N;
@@ -50,8 +57,30 @@ __global__ void k_gnn_table0(const uint32_t *__restrict__ V, uint32_t N, float f
         }
         float deg_feat = __fdiv_rn(__uint2float_rn(d), fmd);
         float id_feat = __double2float_rn(__ddiv_rn((double)(u - base), (double)n));
-        t01[u] = make_float2(deg_feat, id_feat);
+        t01[row_of[u]] = make_float2(deg_feat, id_feat);
     }
+}
+
+// Feature rows in degree order: hub h takes row h, vorder[i] row n_hubs + i.  Each row also gets
+// its vertex's first CSR entry and degree, so the bulk kernels read them in row order.
+__global__ void k_gnn_rows(const uint32_t *__restrict__ V, const uint32_t *__restrict__ hubs, uint32_t n_hubs,
+                           const uint32_t *__restrict__ vorder, uint32_t n_vorder, uint32_t *__restrict__ row_of,
+                           uint2 *__restrict__ vrow) {
+    const uint32_t n = n_hubs + n_vorder;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t u = i < n_hubs ? hubs[i] : vorder[i - n_hubs];
+        const uint32_t beg = V[u];
+        row_of[u] = i;
+        vrow[i] = make_uint2(beg, V[u + 1] - beg);
+    }
+}
+
+// The CSR's neighbour ids as feature rows, entry for entry: the lists keep their order, so every
+// neighbour sum still runs in the reference's CSR order.
+__global__ void k_gnn_row_ids(const uint32_t *__restrict__ E, uint32_t M, const uint32_t *__restrict__ row_of,
+                              uint32_t *__restrict__ Er) {
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < M; j += gridDim.x * blockDim.x)
+        Er[j] = __ldg(row_of + ld_stream(E + j));
 }
 
 // ---- shared pieces: four lanes per vertex, lane q owns features 4q..4q+3 ---------------------
@@ -118,11 +147,12 @@ constexpr int GNN_THREADS = 256;
 // neighbour rows per step (one id each, then one float4 per lane for 8 rows at a time), stage
 // them in the warp's shared-memory slab, and lanes 0..15 add them in CSR order, one feature each.
 template <int MODE>
-__device__ __forceinline__ void warp_vertex(uint32_t u, const uint32_t *__restrict__ V, const uint32_t *__restrict__ E,
+__device__ __forceinline__ void warp_vertex(uint32_t u, uint32_t r, const uint2 *__restrict__ vrow, const uint32_t *__restrict__ E,
                                             const float2 *__restrict__ t01, const float *__restrict__ x, float *__restrict__ y,
                                             uint32_t *__restrict__ key, const float4 *W4, const float *sW, float *slab,
                                             int lane) {
-    const uint32_t beg = V[u], d = V[u + 1] - beg;
+    const uint2 bd = vrow[r];
+    const uint32_t beg = bd.x, d = bd.y;
     const float fd = __uint2float_rn(d);
     const int q = lane & 3;
     const float4 zero4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
@@ -183,27 +213,27 @@ __device__ __forceinline__ void warp_vertex(uint32_t u, const uint32_t *__restri
             s0 = __fdiv_rn(s0, fd);
             sid = __fdiv_rn(sid, fd);
         }
-        const float2 self = t01[u];
+        const float2 self = t01[r];
         out = dense_quad<MODE_INPUT>(W4, b4, q, 0, mask, zero4, zero4, s0, sid, self.x, self.y);
     } else {
         if (fd > 0.0f) nb = make_float4(__fdiv_rn(nb.x, fd), __fdiv_rn(nb.y, fd), __fdiv_rn(nb.z, fd), __fdiv_rn(nb.w, fd));
-        const float4 self = reinterpret_cast<const float4 *>(x)[(size_t)u * 4 + q];
+        const float4 self = reinterpret_cast<const float4 *>(x)[(size_t)r * 4 + q];
         out = dense_quad<MODE>(W4, b4, q, 0, mask, nb, self, 0.0f, 0.0f, 0.0f, 0.0f);
     }
     if (MODE == MODE_OUTPUT) {
         const float sum = output_sum(out, mask);
         if (q == 0) key[u] = __float_as_uint(sum);
     } else {
-        reinterpret_cast<float4 *>(y)[(size_t)u * 4 + q] = out;
+        reinterpret_cast<float4 *>(y)[(size_t)r * 4 + q] = out;
     }
 }
 
 // Work items, heaviest first: the degree order in two tiers, its first n_wide vertices (more than the
 // GNN warp degree) one per warp, the rest eight per warp (four lanes each).  Handed out by counters
-// (work_ctr).
+// (work_ctr).  E holds the neighbours' feature rows; vorder[i]'s own row is row0 + i.
 template <int MODE>
-__global__ void __launch_bounds__(GNN_THREADS, 4) k_gnn_layer(const uint32_t *__restrict__ V, const uint32_t *__restrict__ E,
-                                                              const uint32_t *__restrict__ vorder, uint32_t n_wide,
+__global__ void __launch_bounds__(GNN_THREADS, 4) k_gnn_layer(const uint2 *__restrict__ vrow, const uint32_t *__restrict__ E,
+                                                              const uint32_t *__restrict__ vorder, uint32_t row0, uint32_t n_wide,
                                                               uint32_t n_vorder, const float2 *__restrict__ t01,
                                                               const float *__restrict__ x, float *__restrict__ y,
                                                               uint32_t *__restrict__ key, const float *__restrict__ Wb,
@@ -225,16 +255,18 @@ __global__ void __launch_bounds__(GNN_THREADS, 4) k_gnn_layer(const uint32_t *__
 
     auto item = [&](uint32_t it) {
         if (it < n_wide) {
-            warp_vertex<MODE>(vorder[it], V, E, t01, x, y, key, W4, sW, slab, lane);
+            warp_vertex<MODE>(MODE == MODE_OUTPUT ? vorder[it] : 0u, row0 + it, vrow, E, t01, x, y, key, W4, sW, slab,
+                              lane);
             __syncwarp();
             return;
         }
         const uint32_t g0 = n_wide + (it - n_wide) * 8;
         const uint32_t slot = g0 + (lane >> 2);
         const bool valid = slot < n_vorder;
-        const uint32_t u = valid ? vorder[slot] : 0u;
-        const uint32_t beg = valid ? V[u] : 0u;
-        const uint32_t d = valid ? V[u + 1] - beg : 0u;
+        const uint32_t u = valid && MODE == MODE_OUTPUT ? vorder[slot] : 0u;  // the vertex (for its key)
+        const uint32_t r = row0 + slot;                                       // its feature row
+        const uint2 bd = valid ? vrow[r] : make_uint2(0u, 0u);
+        const uint32_t beg = bd.x, d = bd.y;
         const uint32_t dmax = __reduce_max_sync(FULL, d);  // loop bounds stay warp-uniform
         const float fd = __uint2float_rn(d);
         float4 out;
@@ -257,7 +289,7 @@ __global__ void __launch_bounds__(GNN_THREADS, 4) k_gnn_layer(const uint32_t *__
                 s0 = __fdiv_rn(s0, fd);
                 s1 = __fdiv_rn(s1, fd);
             }
-            const float2 self = valid ? t01[u] : make_float2(0.0f, 0.0f);
+            const float2 self = valid ? t01[r] : make_float2(0.0f, 0.0f);
             out = dense_quad<MODE_INPUT>(W4, b4, q, qbase, FULL, zero4, zero4, s0, s1, self.x, self.y);
         } else {
             float4 s = zero4;
@@ -280,14 +312,14 @@ __global__ void __launch_bounds__(GNN_THREADS, 4) k_gnn_layer(const uint32_t *__
                     if (c + k < d) s = add4(s, r[k]);
             }
             if (fd > 0.0f) s = make_float4(__fdiv_rn(s.x, fd), __fdiv_rn(s.y, fd), __fdiv_rn(s.z, fd), __fdiv_rn(s.w, fd));
-            const float4 self = valid ? __ldg(X4 + (size_t)u * 4 + q) : zero4;
+            const float4 self = valid ? __ldg(X4 + (size_t)r * 4 + q) : zero4;
             out = dense_quad<MODE>(W4, b4, q, qbase, FULL, s, self, 0.0f, 0.0f, 0.0f, 0.0f);
         }
         if (MODE == MODE_OUTPUT) {
             const float sum = output_sum(out, FULL);
             if (valid && q == 0) key[u] = __float_as_uint(sum);
         } else if (valid) {
-            Y4[(size_t)u * 4 + q] = out;
+            Y4[(size_t)r * 4 + q] = out;
         }
     };
     // Dynamic hand-out (work_ctr): items are sorted heaviest first, so the warp-tier vertices
@@ -334,11 +366,11 @@ __global__ void __launch_bounds__(GNN_THREADS, 4) k_gnn_layer(const uint32_t *__
 // chain runs over the inputs in the reference's order; the leading inputs are the same for every
 // such vertex (the +0 means, and in layer 0 also deg/md = 0/md), so that prefix of each chain is
 // evaluated once per CTA, with the same operations, and each vertex continues from it.  These
-// vertices are the tail vorder[first, n) of the degree order.
+// vertices are the tail vorder[first, n) of the degree order; vorder[i]'s input row is row0 + i.
 constexpr int ISO_THREADS = 256;
 constexpr int ISO_MAX_LAYERS = 16;
 
-__global__ void __launch_bounds__(ISO_THREADS) k_gnn_isolated(const uint32_t *__restrict__ vorder, uint32_t first,
+__global__ void __launch_bounds__(ISO_THREADS) k_gnn_isolated(const uint32_t *__restrict__ vorder, uint32_t row0, uint32_t first,
                                                              uint32_t n, const float2 *__restrict__ t01,
                                                              uint32_t *__restrict__ key, const float *__restrict__ params,
                                                              int layers) {
@@ -351,7 +383,7 @@ __global__ void __launch_bounds__(ISO_THREADS) k_gnn_isolated(const uint32_t *__
         const float *W = sP + l * LAYER_PARAMS;
         float c = W[2 * FEAT * FEAT + j];
         if (l == 0) {
-            const float deg0 = t01[vorder[first]].x;  // 0 / md, the same for every vertex here
+            const float deg0 = t01[row0 + first].x;  // 0 / md, the same for every vertex here
             for (int i = 0; i < 24; i++) c = __fmaf_rn(W[i * FEAT + j], i < 16 ? 0.0f : deg0, c);
         } else {
             for (int i = 0; i < FEAT; i++) c = __fmaf_rn(W[i * FEAT + j], 0.0f, c);
@@ -361,7 +393,7 @@ __global__ void __launch_bounds__(ISO_THREADS) k_gnn_isolated(const uint32_t *__
     __syncthreads();
     for (uint32_t slot = first + blockIdx.x * blockDim.x + threadIdx.x; slot < n; slot += gridDim.x * blockDim.x) {
         const uint32_t u = vorder[slot];
-        const float id = t01[u].y;
+        const float id = t01[row0 + slot].y;
         float h[FEAT];
         for (int l = 0; l < layers; l++) {
             const float4 *W4 = reinterpret_cast<const float4 *>(sP + l * LAYER_PARAMS);
@@ -397,14 +429,15 @@ __global__ void __launch_bounds__(ISO_THREADS) k_gnn_isolated(const uint32_t *__
 
 // Vertices with at most ctx->gnn_thin_deg neighbours (the tail of the degree order, vorder[first,
 // n_vorder)): one per lane, 32 per warp, whose degrees are nearly equal because the order is sorted.
+// E holds the neighbours' feature rows; vorder[i]'s own row is row0 + i.
 // Each lane adds its vertex's neighbour rows in CSR order (the next row's loads in flight while the
 // current one is added; the 16 feature chains interleave) and runs the 32 x 16 dense part alone:
 // no lane sits idle on a short neighbour list, and no shuffles are needed.
 constexpr int THIN_THREADS = 256;
 
 template <int MODE>
-__global__ void __launch_bounds__(THIN_THREADS, 3) k_gnn_thin(const uint32_t *__restrict__ V, const uint32_t *__restrict__ E,
-                                                              const uint32_t *__restrict__ vorder, uint32_t first,
+__global__ void __launch_bounds__(THIN_THREADS, 3) k_gnn_thin(const uint2 *__restrict__ vrow, const uint32_t *__restrict__ E,
+                                                              const uint32_t *__restrict__ vorder, uint32_t row0, uint32_t first,
                                                               uint32_t n_vorder, const float2 *__restrict__ t01,
                                                               const float *__restrict__ x, float *__restrict__ y,
                                                               uint32_t *__restrict__ key, const float *__restrict__ Wb,
@@ -419,8 +452,10 @@ __global__ void __launch_bounds__(THIN_THREADS, 3) k_gnn_thin(const uint32_t *__
     auto group = [&](uint32_t base) {  // the 32 vertices vorder[base, base + 32), one per lane
         const uint32_t slot = base + lane;
         const bool valid = slot < n_vorder;
-        const uint32_t u = valid ? vorder[slot] : 0u;
-        const uint32_t beg = valid ? V[u] : 0u, d = valid ? V[u + 1] - beg : 0u;
+        const uint32_t u = valid && MODE == MODE_OUTPUT ? vorder[slot] : 0u;  // the vertex (for its key)
+        const uint32_t r = row0 + slot;                                       // its feature row
+        const uint2 bd = valid ? vrow[r] : make_uint2(0u, 0u);
+        const uint32_t beg = bd.x, d = bd.y;
         const uint32_t dmax = __reduce_max_sync(FULL, d);
         const float fd = __uint2float_rn(d);
         float c[FEAT];
@@ -441,7 +476,7 @@ __global__ void __launch_bounds__(THIN_THREADS, 3) k_gnn_thin(const uint32_t *__
                 s0 = __fdiv_rn(s0, fd);
                 s1 = __fdiv_rn(s1, fd);
             }
-            const float2 self = valid ? t01[u] : make_float2(0.0f, 0.0f);
+            const float2 self = valid ? t01[r] : make_float2(0.0f, 0.0f);
 #pragma unroll
             for (int i = 0; i < 32; i++) {
                 const float a = i < 8 ? s0 : (i < 16 ? s1 : (i < 24 ? self.x : self.y));
@@ -493,7 +528,7 @@ __global__ void __launch_bounds__(THIN_THREADS, 3) k_gnn_thin(const uint32_t *__
             float self[FEAT];
 #pragma unroll
             for (int p = 0; p < 4; p++) {
-                const float4 s4 = valid ? __ldg(X4 + (size_t)u * 4 + p) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                const float4 s4 = valid ? __ldg(X4 + (size_t)r * 4 + p) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
                 self[4 * p + 0] = s4.x;
                 self[4 * p + 1] = s4.y;
                 self[4 * p + 2] = s4.z;
@@ -524,7 +559,7 @@ __global__ void __launch_bounds__(THIN_THREADS, 3) k_gnn_thin(const uint32_t *__
                                         __fadd_rn(__fadd_rn(t[4], t[5]), __fadd_rn(t[6], t[7])));
             key[u] = __float_as_uint(sum);
         } else {
-            float4 *Y4 = reinterpret_cast<float4 *>(y) + (size_t)u * 4;
+            float4 *Y4 = reinterpret_cast<float4 *>(y) + (size_t)r * 4;
 #pragma unroll
             for (int p = 0; p < 4; p++) Y4[p] = make_float4(c[4 * p], c[4 * p + 1], c[4 * p + 2], c[4 * p + 3]);
         }
@@ -1073,7 +1108,7 @@ __device__ __forceinline__ void hub_dense(uint32_t h, const uint32_t *__restrict
             s0 = __fdiv_rn(s0, fd);
             s1 = __fdiv_rn(s1, fd);
         }
-        const float2 self = t01[u];
+        const float2 self = t01[h];  // hub h's feature row is h
 #pragma unroll
         for (int i = 0; i < 32; i++) {
             const float a = i < 8 ? s0 : (i < 16 ? s1 : (i < 24 ? self.x : self.y));
@@ -1082,7 +1117,7 @@ __device__ __forceinline__ void hub_dense(uint32_t h, const uint32_t *__restrict
     } else {
         float nb = __ldcg(sums + h * FEAT + j);
         if (fd > 0.0f) nb = __fdiv_rn(nb, fd);
-        const float self = x[(size_t)u * FEAT + j];
+        const float self = x[(size_t)h * FEAT + j];
 #pragma unroll
         for (int i = 0; i < 32; i++) {
             const float a = __shfl_sync(FULL, i < FEAT ? nb : self, i & 15);
@@ -1100,7 +1135,7 @@ __device__ __forceinline__ void hub_dense(uint32_t h, const uint32_t *__restrict
                                   __fadd_rn(__fadd_rn(tk[4], tk[5]), __fadd_rn(tk[6], tk[7])));
         if (lane == 0) key[u] = __float_as_uint(p);
     } else if (lane < FEAT) {
-        y[(size_t)u * FEAT + lane] = o;
+        y[(size_t)h * FEAT + lane] = o;
     }
 }
 
@@ -1190,7 +1225,7 @@ gc_status launch_layer(gc_graph *g, const float *Wb, const float *x, float *y, u
         ProfScope ph(ctx, MODE == MODE_INPUT ? "gnn_hub_input" : (MODE == MODE_HIDDEN ? "gnn_hub_hidden" : "gnn_hub_output"),
                      side);
         if (g->n_giant) {  // the giant hubs' rows, staged by the whole GPU
-            k_hub_stage<MODE><<<ctx->num_sms * 8, 256, 0, side>>>(g->V, g->E, g->hubs, g->giant_off, g->n_giant,
+            k_hub_stage<MODE><<<ctx->num_sms * 8, 256, 0, side>>>(g->V, g->Er, g->hubs, g->giant_off, g->n_giant,
                                                                   g->giant_rows, g->t01, x, g->hub_stage);
             ctx->launches++;
         }
@@ -1211,7 +1246,7 @@ gc_status launch_layer(gc_graph *g, const float *Wb, const float *x, float *y, u
                                                          : (uint32_t)occ;
         const uint32_t n_items = g->n_giant * Cfg::NGB + (g->n_hubs - g->n_giant);
         const uint32_t grid = std::min<uint32_t>((uint32_t)ctx->num_sms * per_sm, n_items);
-        k_gnn_hubx<MODE><<<grid, Cfg::THREADS, Cfg::SMEM, side>>>(g->V, g->E, g->hubs, g->t01, x, y, g->key, Wb, sums,
+        k_gnn_hubx<MODE><<<grid, Cfg::THREADS, Cfg::SMEM, side>>>(g->V, g->Er, g->hubs, g->t01, x, y, g->key, Wb, sums,
                                                                  done, done + g->n_hubs, g->n_hubs, g->n_giant,
                                                                  g->hub_stage, g->giant_off, g->giant_rows, ctx->dstate);
         ctx->launches++;
@@ -1232,16 +1267,17 @@ gc_status launch_layer(gc_graph *g, const float *Wb, const float *x, float *y, u
         const int bb = g->n_hubs && ctx->hub_stream && blocks > 1 ? blocks - 1 : blocks;
         if (first_thin) {
             k_gnn_layer<MODE><<<ctx->num_sms * bb, GNN_THREADS, 0, ctx->stream>>>(
-                g->V, g->E, g->vorder, g->n_wide_gnn, first_thin, g->t01, x, y, g->key, Wb, ctr, ctx->gnn_grab,
-                ctx->gnn_heavy);
+                g->vrow, g->Er, g->vorder, g->n_hubs, g->n_wide_gnn, first_thin, g->t01, x, y, g->key, Wb, ctr,
+                ctx->gnn_grab, ctx->gnn_heavy);
             ctx->launches++;
         }
         const uint32_t end_thin = g->n_vorder - n_iso;
         if (end_thin > first_thin) {
             const uint32_t grid = std::min<uint32_t>((uint32_t)ctx->num_sms * 3,
                                                      (end_thin - first_thin + THIN_THREADS - 1) / THIN_THREADS);
-            k_gnn_thin<MODE><<<grid, THIN_THREADS, 0, ctx->stream>>>(g->V, g->E, g->vorder, first_thin, end_thin,
-                                                                     g->t01, x, y, g->key, Wb, ctr + 5, ctx->gnn_grab);
+            k_gnn_thin<MODE><<<grid, THIN_THREADS, 0, ctx->stream>>>(g->vrow, g->Er, g->vorder, g->n_hubs, first_thin,
+                                                                     end_thin, g->t01, x, y, g->key, Wb, ctr + 5,
+                                                                     ctx->gnn_grab);
             ctx->launches++;
         }
     }
@@ -1289,10 +1325,25 @@ gc_status gc_priority_gnn(gc_graph *g, const gc_model *m) {
             return s;
     }
     if ((s = gc_alloc(ctx, &g->gnn_ctr, 8, "gnn work counters")) != GC_OK) return s;
+    if (!g->rows_ready) {  // once per upload: the feature-row order and the neighbour ids as rows
+        if ((s = gc_alloc(ctx, &g->row_of, rows, "feature rows")) != GC_OK) return s;
+        if ((s = gc_alloc(ctx, &g->Er, (size_t)g->cap_M, "neighbour rows")) != GC_OK) return s;
+        if ((s = gc_alloc(ctx, &g->vrow, rows, "row offsets")) != GC_OK) return s;
+        ProfScope ps(ctx, "gnn_rows", ctx->stream);
+        k_gnn_rows<<<ctx->num_sms * 4, 256, 0, ctx->stream>>>(g->V, g->hubs, g->n_hubs, g->vorder, g->n_vorder,
+                                                               g->row_of, g->vrow);
+        ctx->launches++;
+        if (g->M) {
+            k_gnn_row_ids<<<ctx->num_sms * 8, 256, 0, ctx->stream>>>(g->E, g->M, g->row_of, g->Er);
+            ctx->launches++;
+        }
+        if ((s = gc_check_launch(ctx, "gnn feature rows")) != GC_OK) return s;
+        g->rows_ready = true;
+    }
     {
         ProfScope ps(ctx, "gnn_table0", ctx->stream);
         k_gnn_table0<<<ctx->num_sms * 4, 256, 0, ctx->stream>>>(g->V, g->N, (float)m->md, g->seg_voff, g->n_seg,
-                                                                 g->t01);
+                                                                 g->row_of, g->t01);
     }
     ctx->launches++;
     if ((s = gc_check_launch(ctx, "gnn input table")) != GC_OK) return s;
@@ -1303,8 +1354,8 @@ gc_status gc_priority_gnn(gc_graph *g, const gc_model *m) {
         const uint32_t first = g->n_vorder - g->n_iso;
         const uint32_t grid = std::min<uint32_t>((uint32_t)ctx->num_sms * 4, (g->n_iso + ISO_THREADS - 1) / ISO_THREADS);
         const size_t smem = sizeof(float) * LAYER_PARAMS * (size_t)L;
-        k_gnn_isolated<<<grid, ISO_THREADS, smem, ctx->stream>>>(g->vorder, first, g->n_vorder, g->t01, g->key,
-                                                                 m->d_param, L);
+        k_gnn_isolated<<<grid, ISO_THREADS, smem, ctx->stream>>>(g->vorder, g->n_hubs, first, g->n_vorder, g->t01,
+                                                                 g->key, m->d_param, L);
         ctx->launches++;
         if ((s = gc_check_launch(ctx, "gnn isolated vertices")) != GC_OK) return s;
     }

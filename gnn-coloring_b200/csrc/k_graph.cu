@@ -88,6 +88,7 @@ __global__ void k_hub_degrees(const uint32_t *__restrict__ V, const uint32_t *__
 gc_status gc_graph_prepare(gc_graph *g) {
     gc_ctx *ctx = g->ctx;
     gc_status s;
+    g->rows_ready = false;  // the GNN's feature-row order follows the hub list and the degree order
     if (g->N == 0) {
         g->max_deg = 0;
         g->n_big_tasks = 0;
