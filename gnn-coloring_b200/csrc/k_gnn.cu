@@ -35,6 +35,7 @@
 // Compiled without fast-math; every add, divide and FMA is an explicit round-to-nearest
 // intrinsic so the compiler cannot contract or reassociate them.
 #include <algorithm>
+#include <cstring>
 
 #include "gc_internal.h"
 
@@ -400,9 +401,9 @@ __global__ void __launch_bounds__(ISO_THREADS) k_gnn_isolated(const uint32_t *__
             float c[FEAT];
 #pragma unroll
             for (int j = 0; j < FEAT; j++) c[j] = c0[l][j];
-            const int i0 = l == 0 ? 24 : FEAT;
-            for (int i = i0; i < 32; i++) {
-                const float a = l == 0 ? id : h[i - FEAT];
+            // the inputs after the common prefix: layer 0 the id feature (inputs 24..31), later layers
+            // the vertex's own previous outputs (inputs 16..31); unrolled so h stays in registers
+            auto fma_in = [&](int i, float a) {
 #pragma unroll
                 for (int jq = 0; jq < 4; jq++) {
                     const float4 w = W4[i * 4 + jq];
@@ -411,6 +412,13 @@ __global__ void __launch_bounds__(ISO_THREADS) k_gnn_isolated(const uint32_t *__
                     c[4 * jq + 2] = __fmaf_rn(w.z, a, c[4 * jq + 2]);
                     c[4 * jq + 3] = __fmaf_rn(w.w, a, c[4 * jq + 3]);
                 }
+            };
+            if (l == 0) {
+#pragma unroll
+                for (int i = 24; i < 32; i++) fma_in(i, id);
+            } else {
+#pragma unroll
+                for (int i = FEAT; i < 32; i++) fma_in(i, h[i - FEAT]);
             }
 #pragma unroll
             for (int j = 0; j < FEAT; j++) h[j] = relu(c[j]);
@@ -435,17 +443,22 @@ __global__ void __launch_bounds__(ISO_THREADS) k_gnn_isolated(const uint32_t *__
 // no lane sits idle on a short neighbour list, and no shuffles are needed.
 constexpr int THIN_THREADS = 256;
 
+// One layer's 32 x 16 weights and 16 biases as a kernel parameter.  Every lane of the thin tier reads
+// the same weight at the same time, with compile-time indices, so each one is a constant-bank
+// operand of its FMA: no load through the L1 data pipe, which bounds this kernel (weights in shared
+// memory cost it 15 M of 53 M wavefronts per hidden layer on R-MAT 22).
+struct LayerArg {
+    float w[LAYER_PARAMS];
+};
+
 template <int MODE>
 __global__ void __launch_bounds__(THIN_THREADS, 3) k_gnn_thin(const uint2 *__restrict__ vrow, const uint32_t *__restrict__ E,
                                                               const uint32_t *__restrict__ vorder, uint32_t row0, uint32_t first,
                                                               uint32_t n_vorder, const float2 *__restrict__ t01,
                                                               const float *__restrict__ x, float *__restrict__ y,
-                                                              uint32_t *__restrict__ key, const float *__restrict__ Wb,
+                                                              uint32_t *__restrict__ key, const __grid_constant__ LayerArg P,
                                                               uint32_t *work_ctr, uint32_t grab) {
-    __shared__ __align__(16) float sW[LAYER_PARAMS];
-    for (int i = threadIdx.x; i < LAYER_PARAMS; i += blockDim.x) sW[i] = Wb[i];
-    __syncthreads();
-    const float4 *W4 = reinterpret_cast<const float4 *>(sW);
+    const float *W = P.w;  // row i of the weights: W[16 i .. 16 i + 15], biases W[512 ..]
     const float4 *X4 = reinterpret_cast<const float4 *>(x);
     const int lane = threadIdx.x & 31;
     const uint32_t stride = gridDim.x * blockDim.x;
@@ -460,7 +473,7 @@ __global__ void __launch_bounds__(THIN_THREADS, 3) k_gnn_thin(const uint2 *__res
         const float fd = __uint2float_rn(d);
         float c[FEAT];
 #pragma unroll
-        for (int j = 0; j < FEAT; j++) c[j] = sW[2 * FEAT * FEAT + j];
+        for (int j = 0; j < FEAT; j++) c[j] = W[2 * FEAT * FEAT + j];
         if (MODE == MODE_INPUT) {
             float s0 = 0.0f, s1 = 0.0f;
             float2 tn = d ? __ldg(t01 + __ldg(E + beg)) : make_float2(0.0f, 0.0f);
@@ -481,13 +494,7 @@ __global__ void __launch_bounds__(THIN_THREADS, 3) k_gnn_thin(const uint2 *__res
             for (int i = 0; i < 32; i++) {
                 const float a = i < 8 ? s0 : (i < 16 ? s1 : (i < 24 ? self.x : self.y));
 #pragma unroll
-                for (int jq = 0; jq < 4; jq++) {
-                    const float4 w = W4[i * 4 + jq];
-                    c[4 * jq + 0] = __fmaf_rn(w.x, a, c[4 * jq + 0]);
-                    c[4 * jq + 1] = __fmaf_rn(w.y, a, c[4 * jq + 1]);
-                    c[4 * jq + 2] = __fmaf_rn(w.z, a, c[4 * jq + 2]);
-                    c[4 * jq + 3] = __fmaf_rn(w.w, a, c[4 * jq + 3]);
-                }
+                for (int j = 0; j < FEAT; j++) c[j] = __fmaf_rn(W[i * FEAT + j], a, c[j]);
             }
         } else {
             float acc[FEAT];
@@ -538,13 +545,7 @@ __global__ void __launch_bounds__(THIN_THREADS, 3) k_gnn_thin(const uint2 *__res
             for (int i = 0; i < 32; i++) {
                 const float a = i < FEAT ? acc[i] : self[i - FEAT];
 #pragma unroll
-                for (int jq = 0; jq < 4; jq++) {
-                    const float4 w = W4[i * 4 + jq];
-                    c[4 * jq + 0] = __fmaf_rn(w.x, a, c[4 * jq + 0]);
-                    c[4 * jq + 1] = __fmaf_rn(w.y, a, c[4 * jq + 1]);
-                    c[4 * jq + 2] = __fmaf_rn(w.z, a, c[4 * jq + 2]);
-                    c[4 * jq + 3] = __fmaf_rn(w.w, a, c[4 * jq + 3]);
-                }
+                for (int j = 0; j < FEAT; j++) c[j] = __fmaf_rn(W[i * FEAT + j], a, c[j]);
             }
         }
 #pragma unroll
@@ -1199,7 +1200,7 @@ __global__ void __launch_bounds__(HubCfg<MODE>::THREADS) k_gnn_hubx(
 }
 
 template <int MODE>
-gc_status launch_layer(gc_graph *g, const float *Wb, const float *x, float *y, uint32_t n_iso) {
+gc_status launch_layer(gc_graph *g, const float *Wb, const float *Wh, const float *x, float *y, uint32_t n_iso) {
     gc_ctx *ctx = g->ctx;
     gc_status s;
     // counters, zeroed for each layer: warp-tier vertices (0), leading four-lane items (1), the rest
@@ -1275,8 +1276,10 @@ gc_status launch_layer(gc_graph *g, const float *Wb, const float *x, float *y, u
         if (end_thin > first_thin) {
             const uint32_t grid = std::min<uint32_t>((uint32_t)ctx->num_sms * 3,
                                                      (end_thin - first_thin + THIN_THREADS - 1) / THIN_THREADS);
+            LayerArg la;
+            memcpy(la.w, Wh, sizeof(la.w));
             k_gnn_thin<MODE><<<grid, THIN_THREADS, 0, ctx->stream>>>(g->vrow, g->Er, g->vorder, g->n_hubs, first_thin,
-                                                                     end_thin, g->t01, x, y, g->key, Wb, ctr + 5,
+                                                                     end_thin, g->t01, x, y, g->key, la, ctr + 5,
                                                                      ctx->gnn_grab);
             ctx->launches++;
         }
@@ -1361,13 +1364,13 @@ gc_status gc_priority_gnn(gc_graph *g, const gc_model *m) {
     }
     float *x = g->x, *y = g->y;
     for (int l = 0; l < L; l++) {
-        const float *Wb = m->d_param + (size_t)l * LAYER_PARAMS;
+        const float *Wb = m->d_param + (size_t)l * LAYER_PARAMS, *Wh = m->h_param + (size_t)l * LAYER_PARAMS;
         if (l == 0)
-            s = launch_layer<MODE_INPUT>(g, Wb, nullptr, y, n_iso);
+            s = launch_layer<MODE_INPUT>(g, Wb, Wh, nullptr, y, n_iso);
         else if (l < L - 1)
-            s = launch_layer<MODE_HIDDEN>(g, Wb, x, y, n_iso);
+            s = launch_layer<MODE_HIDDEN>(g, Wb, Wh, x, y, n_iso);
         else
-            s = launch_layer<MODE_OUTPUT>(g, Wb, x, nullptr, n_iso);
+            s = launch_layer<MODE_OUTPUT>(g, Wb, Wh, x, nullptr, n_iso);
         if (s != GC_OK) return s;
         float *t = x;
         x = y;
