@@ -66,6 +66,20 @@ __device__ __forceinline__ void st_relaxed_u64(unsigned long long *p, unsigned l
 // Streaming load (evict-first): CSR edge arrays are read once per pass.
 __device__ __forceinline__ uint32_t ld_stream(const uint32_t *p) { return __ldcs(p); }
 
+// An L2 policy that keeps the lines it loads (evict-last), for small arrays gathered at random
+// beside a large stream (an instruction hint: no device setting changes).
+__device__ __forceinline__ uint64_t l2_keep_policy() {
+    uint64_t pol;
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
+// Read-only load under that policy.
+__device__ __forceinline__ uint32_t ld_keep(const uint32_t *p, uint64_t pol) {
+    uint32_t v;
+    asm("ld.global.nc.L2::cache_hint.b32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(pol));
+    return v;
+}
+
 __device__ __forceinline__ void raise_error(DevState *st, unsigned int code, unsigned int info) {
     if (atomicOr(&st->err, code) == 0) st->err_info = info;
 }

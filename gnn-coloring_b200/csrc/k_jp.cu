@@ -52,6 +52,7 @@ __global__ void __launch_bounds__(256) k_jp_split(const uint32_t *__restrict__ V
     const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
     const uint32_t n_items = n_wide + (n_vorder - n_wide + 7) / 8;
+    const uint64_t keep = l2_keep_policy();  // the keys (4N bytes) stay in L2 while E streams past
     for (uint32_t it = warp; it < n_items; it += nwarps) {
         if (it < n_wide) {
             const uint32_t u = vorder[it];
@@ -66,7 +67,7 @@ __global__ void __launch_bounds__(256) k_jp_split(const uint32_t *__restrict__ V
                     v[k] = i < d ? ld_stream(E + beg + i) : 0u;
                 }
 #pragma unroll
-                for (int k = 0; k < SPLIT_LOADS; k++) kv[k] = c + 32 * k + lane < d ? __ldg(key + v[k]) : 0u;
+                for (int k = 0; k < SPLIT_LOADS; k++) kv[k] = c + 32 * k + lane < d ? ld_keep(key + v[k], keep) : 0u;
 #pragma unroll
                 for (int k = 0; k < SPLIT_LOADS; k++) {
                     const bool pk = c + 32 * k + lane < d && precedes(kv[k], v[k], ku, u);
@@ -95,7 +96,7 @@ __global__ void __launch_bounds__(256) k_jp_split(const uint32_t *__restrict__ V
                 v[k] = i < d ? ld_stream(E + beg + i) : 0u;
             }
 #pragma unroll
-            for (int k = 0; k < SPLIT_LOADS; k++) kv[k] = c + 4 * k + q < d ? __ldg(key + v[k]) : 0u;
+            for (int k = 0; k < SPLIT_LOADS; k++) kv[k] = c + 4 * k + q < d ? ld_keep(key + v[k], keep) : 0u;
 #pragma unroll
             for (int k = 0; k < SPLIT_LOADS; k++) {
                 const bool pk = c + 4 * k + q < d && precedes(kv[k], v[k], ku, u);
