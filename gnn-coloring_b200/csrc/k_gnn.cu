@@ -18,10 +18,11 @@
 //   - quad tier: four lanes per vertex, a float4 of the row each, eight vertices per warp;
 //   - warp tier (more than GC_GNN_WIDE_DEGREE neighbours): a warp per vertex, rows staged in
 //     shared memory;
-//   - hubs (more than GC_GNN_HUB_DEGREE): before the layer kernel, one CTA per (hub, group of four
-//     features) gathers the neighbour rows in steps of 1,024 into shared memory, and one warp per
-//     feature evaluates the reference's sequential FP32 chain exactly, a step at a time
-//     (exact_step below); the hub's last CTA runs its dense part.
+//   - hubs (more than GC_GNN_HUB_DEGREE): a persistent kernel on a high-priority side stream; one
+//     item per hub gathers its neighbour rows into shared memory, 512 or 1,024 at a time, and one
+//     warp per feature evaluates the reference's sequential FP32 chain exactly, a step at a time
+//     (exact_step below); the rows of the largest hubs are staged feature-major by the whole GPU
+//     first and split into (hub, 4 features) items; the hub's last item runs its dense part.
 // Feature rows (x, y and the layer-0 table) are stored in degree order: hub h at row h, vorder[i] at
 // row n_hubs + i.  The neighbour lists are read from Er, the CSR with each id replaced by its row
 // (entry for entry, so every sum keeps the reference's order), and each row's first CSR entry and
