@@ -347,6 +347,20 @@ def prep_time_ms(ctx, N, V, E, reps: int = 5):
     return float(statistics.median(ts)), float(min(ts))
 
 
+def rows_time_ms(ctx, model, N, V, E):
+    """The GNN's feature-row order (k_gnn_rows, k_gnn_row_ids), built by the first GNN call after an
+    upload: timed with the library's event pairs on a second upload of the same graph, so that the
+    kernels' first-launch loading is not counted.  Once per upload; not part of `value`."""
+    import gnn_coloring as gcn
+    g2 = gcn.Graph(ctx, N, V, E)
+    gcn.lib.gc_prof_enable(ctx.h, 1)
+    g2.priority("GNN", model)
+    ms = prof_totals(gcn, ctx).get("gnn_rows", {}).get("ms_per_step")
+    gcn.lib.gc_prof_enable(ctx.h, 0)
+    g2.close()
+    return ms
+
+
 def prof_totals(gcn, ctx, steps: int = 1):
     """The library's per-kernel event timings since gc_prof_enable, per step."""
     names = (C.c_char_p * 64)()
@@ -393,13 +407,7 @@ def run_ours(args):
         g.priority("GNN", model)
         g.color(count=False)
 
-    # the first GNN call after the upload also builds the feature-row order (once per upload, like
-    # the preparation that prep_ms times): timed here with the library's event pairs
-    gcn.lib.gc_prof_enable(ctx.h, 1)
-    step()
-    rows_ms = prof_totals(gcn, ctx).get("gnn_rows", {}).get("ms_per_step")
-    gcn.lib.gc_prof_enable(ctx.h, 0)
-    for _ in range(max(3, args.warmup) - 1):
+    for _ in range(max(3, args.warmup)):
         step()
     colors_used = g.validate()
     assert colors_used > 0, "invalid coloring"
@@ -460,6 +468,7 @@ def run_ours(args):
     step_roof = {"algorithmic_bytes": job_bytes, "achieved_gbs": job_bytes / (ms_per_step / 1e3) / 1e9,
                  "frac": job_bytes / (ms_per_step / 1e3) / 1e9 / hbm_peak}
     prep_ms, prep_min_ms = prep_time_ms(ctx, N, V, E) if world == 1 else (None, None)
+    rows_ms = rows_time_ms(ctx, model, N, V, E) if world == 1 else None
 
     # e2e through the reference-facing entry point with host buffers
     e2e = None
