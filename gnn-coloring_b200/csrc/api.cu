@@ -9,6 +9,7 @@
 
 #include "gc_internal.h"
 #include "host_graph.h"
+#include "overlap.h"
 
 
 // ---- errors ------------------------------------------------------------------------------------
@@ -171,7 +172,13 @@ gc_status gc_copy_stream(gc_ctx *ctx) {
         s = gc_check_cuda(ctx, cudaEventCreateWithFlags(&ctx->ev_copy_fence, cudaEventDisableTiming), "copy events");
     if (s == GC_OK)
         s = gc_check_cuda(ctx, cudaEventCreateWithFlags(&ctx->ev_copy_done, cudaEventDisableTiming), "copy events");
+    for (int k = 0; k < GC_UPLOAD_CHUNKS && s == GC_OK; k++)
+        s = gc_check_cuda(ctx, cudaEventCreateWithFlags(&ctx->ev_chunk[k], cudaEventDisableTiming), "copy events");
     return s;
+}
+
+void gc_graph_gnn_hint(gc_graph *g, int on) {
+    if (g) g->gnn_hint = on != 0;
 }
 
 bool gc_is_pinned(const void *host_ptr) {
@@ -187,21 +194,33 @@ namespace {
 
 // Upload of a CSR whose E is page-locked host memory: E goes up on the copy stream while V is
 // checked and the graph prepared on the context's stream (preparation reads V only); E is checked
-// once it has arrived.  Returns only after the copy has finished, so the caller may reuse E.
+// once it has arrived.  When GNN priorities follow (gnn_hint), E goes up in GC_UPLOAD_CHUNKS pieces
+// and, once the graph is prepared, each piece is converted to feature rows (which checks its ids)
+// as soon as it has arrived, beside the rest of the copy.  Returns only after the copy has
+// finished, so the caller may reuse E.
 gc_status reupload_overlapped(gc_ctx *ctx, gc_graph *g, const uint32_t *V, const uint32_t *E) {
     const uint32_t N = g->N, M = g->M;
     gc_status s = gc_copy_stream(ctx);
     if (s != GC_OK) return s;
     g->has_keys = g->has_colors = false;
     g->key_kind = -1;
+    const bool rows = g->gnn_hint;
+    const uint32_t piece = (M + GC_UPLOAD_CHUNKS - 1) / GC_UPLOAD_CHUNKS;
     // E may still be read by earlier work on the context's stream
     if ((s = gc_check_cuda(ctx, cudaEventRecord(ctx->ev_copy_fence, ctx->stream), "upload E")) != GC_OK) return s;
     if ((s = gc_check_cuda(ctx, cudaStreamWaitEvent(ctx->copy_stream, ctx->ev_copy_fence, 0), "upload E")) != GC_OK)
         return s;
-    if ((s = gc_check_cuda(ctx, cudaMemcpyAsync(g->E, E, sizeof(uint32_t) * (size_t)M, cudaMemcpyHostToDevice,
-                                                ctx->copy_stream), "upload E")) != GC_OK)
-        return s;
-    if ((s = gc_check_cuda(ctx, cudaEventRecord(ctx->ev_copy_done, ctx->copy_stream), "upload E")) != GC_OK) {
+    for (int k = 0; k < (rows ? GC_UPLOAD_CHUNKS : 1) && s == GC_OK; k++) {
+        const uint32_t first = rows ? std::min<uint32_t>(M, (uint32_t)k * piece) : 0u;
+        const uint32_t count = rows ? std::min<uint32_t>(M - first, piece) : M;
+        if (count)
+            s = gc_check_cuda(ctx, cudaMemcpyAsync(g->E + first, E + first, sizeof(uint32_t) * (size_t)count,
+                                                   cudaMemcpyHostToDevice, ctx->copy_stream), "upload E");
+        if (s == GC_OK && rows)
+            s = gc_check_cuda(ctx, cudaEventRecord(ctx->ev_chunk[k], ctx->copy_stream), "upload E");
+    }
+    if (s == GC_OK) s = gc_check_cuda(ctx, cudaEventRecord(ctx->ev_copy_done, ctx->copy_stream), "upload E");
+    if (s != GC_OK) {
         cudaStreamSynchronize(ctx->copy_stream);
         return s;
     }
@@ -216,6 +235,20 @@ gc_status reupload_overlapped(gc_ctx *ctx, gc_graph *g, const uint32_t *V, const
     if (s == GC_OK && (s = gc_read_state(ctx)) == GC_ERR_DEVICE)
         s = gc_fail(ctx, GC_ERR_INVALID, "malformed CSR: V not monotone or E out of range");
     if (s == GC_OK) s = gc_graph_prepare(g);
+    // GNN priorities follow: the feature-row order now, then each piece of E as rows once it has
+    // arrived (the conversion checks the piece's ids)
+    bool rows_queued = false;
+    if (s == GC_OK && rows) {
+        s = gc_reset_state(ctx);
+        if (s == GC_OK) s = gc_gnn_rows_begin(g);
+        for (int k = 0; k < GC_UPLOAD_CHUNKS && s == GC_OK; k++) {
+            const uint32_t first = std::min<uint32_t>(M, (uint32_t)k * piece);
+            const uint32_t count = std::min<uint32_t>(M - first, piece);
+            s = gc_check_cuda(ctx, cudaStreamWaitEvent(ctx->stream, ctx->ev_chunk[k], 0), "upload E");
+            if (s == GC_OK) s = gc_gnn_row_ids(g, first, count);
+        }
+        rows_queued = s == GC_OK;
+    }
     // from here on the context's stream follows the copy
     const gc_status w = gc_check_cuda(ctx, cudaStreamWaitEvent(ctx->stream, ctx->ev_copy_done, 0), "upload E");
     if (w != GC_OK) {
@@ -226,17 +259,20 @@ gc_status reupload_overlapped(gc_ctx *ctx, gc_graph *g, const uint32_t *V, const
         cudaStreamSynchronize(ctx->copy_stream);
         return s;
     }
-    if ((s = gc_reset_state(ctx)) == GC_OK) {
-        k_check_ids<<<ctx->num_sms * 4, 256, 0, ctx->stream>>>(g->E, N, M, ctx->dstate);
-        ctx->launches++;
-        s = gc_check_launch(ctx, "csr check");
-    }
-    if (s != GC_OK) {
-        cudaStreamSynchronize(ctx->copy_stream);
-        return s;
+    if (!rows_queued) {
+        if ((s = gc_reset_state(ctx)) == GC_OK) {
+            k_check_ids<<<ctx->num_sms * 4, 256, 0, ctx->stream>>>(g->E, N, M, ctx->dstate);
+            ctx->launches++;
+            s = gc_check_launch(ctx, "csr check");
+        }
+        if (s != GC_OK) {
+            cudaStreamSynchronize(ctx->copy_stream);
+            return s;
+        }
     }
     if ((s = gc_read_state(ctx)) != GC_OK)
         return s == GC_ERR_DEVICE ? gc_fail(ctx, GC_ERR_INVALID, "malformed CSR: V not monotone or E out of range") : s;
+    g->rows_ready = rows_queued;
     return GC_OK;
 }
 
@@ -340,6 +376,8 @@ static void ctx_release(gc_ctx *ctx) {
     if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
     if (ctx->ev_copy_fence) cudaEventDestroy(ctx->ev_copy_fence);
     if (ctx->ev_copy_done) cudaEventDestroy(ctx->ev_copy_done);
+    for (auto e : ctx->ev_chunk)
+        if (e) cudaEventDestroy(e);
     if (ctx->dstate) cudaFree(ctx->dstate);
     if (ctx->hstate) cudaFreeHost(ctx->hstate);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);

@@ -20,6 +20,7 @@ struct gc_prof_rec {
 // Degree tiers: above GC_GNN_HUB_DEGREE a vertex is a hub (JP split tasks; in the GNN its neighbour
 // sums are evaluated exactly by whole warps before each layer); above GC_GNN_WARP_DEGREE the split
 // gives it a warp.
+constexpr int GC_UPLOAD_CHUNKS = 8;  // pieces of a page-locked E converted to GNN rows as they arrive
 constexpr uint32_t GC_GNN_HUB_DEGREE = 16384;
 // Giant hubs (GNN): at least this many neighbours, and a third of the largest degree; their staged
 // rows take at most GC_GIANT_MAX_ROWS padded rows (16 floats each).
@@ -42,6 +43,7 @@ struct gc_ctx {
     int hub_blocks_per_sm[3] = {0, 0, 0};  // resident CTAs of each hub kernel
     cudaStream_t copy_stream = nullptr;  // host copies that overlap work on `stream` (created on first use)
     cudaEvent_t ev_copy_fence = nullptr, ev_copy_done = nullptr;
+    cudaEvent_t ev_chunk[GC_UPLOAD_CHUNKS] = {};  // pieces of a page-locked E that have arrived
     int color_blocks_per_sm = 0;         // resident CTAs of the coloring kernel (occupancy query)
     int jp_ctas_per_sm = 2;              // CTAs per SM of the coloring kernel: fewer pollers beat more lookahead (measured)
     unsigned int jp_tight = 32;          // coloring: unproductive polling rounds before sleeping
@@ -154,6 +156,8 @@ struct gc_graph {
     uint2 *vrow = nullptr;       // per feature row: (first CSR entry, degree) of its vertex
     uint32_t *Er = nullptr;      // E with every neighbour id replaced by its feature row (same positions)
     bool rows_ready = false;     // row_of and Er describe the current CSR (cleared by gc_graph_prepare)
+    bool gnn_hint = false;       // GNN priorities follow the next upload: a page-locked E is converted to
+                                 // rows piece by piece while it arrives (set by the reference-named calls)
     // SL/SLL scratch (allocated on first use)
     uint32_t *deg_rem = nullptr, *frontier = nullptr, *frontier2 = nullptr, *removed = nullptr;
     // tier thresholds and vertex schedule of the split and GNN kernels (gc_graph_prepare applies them)
@@ -225,6 +229,11 @@ gc_status gc_graph_prepare(gc_graph *g);  // degree classes, max degree (k_graph
 gc_status gc_priority_simple(gc_graph *g, gc_heuristic h);         // FF / LF / LLF (k_priority.cu)
 gc_status gc_priority_peel(gc_graph *g, bool log_thresholds);      // SL / SLL (k_priority.cu)
 gc_status gc_priority_gnn(gc_graph *g, const gc_model *m);         // GraphSAGE (k_gnn.cu)
+// The GNN's feature-row order (k_gnn.cu): row_of and vrow from the hub list and the degree order,
+// then E's entries [first, first + count) as rows into Er.  The conversion checks every id against
+// N (ERR_BOUND, reported by the next gc_read_state) and writes row 0 for one that is out of range.
+gc_status gc_gnn_rows_begin(gc_graph *g);
+gc_status gc_gnn_row_ids(gc_graph *g, uint32_t first, uint32_t count);
 gc_status gc_jp_color(gc_graph *g);                                // JP by current keys (k_jp.cu)
 gc_status gc_keys_from_colors(gc_graph *g);                        // Culberson step (k_jp.cu)
 gc_status gc_validate_device(gc_graph *g, int *max_color);         // (k_jp.cu)

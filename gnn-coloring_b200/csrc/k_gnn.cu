@@ -78,11 +78,20 @@ __global__ void k_gnn_rows(const uint32_t *__restrict__ V, const uint32_t *__res
 }
 
 // The CSR's neighbour ids as feature rows, entry for entry: the lists keep their order, so every
-// neighbour sum still runs in the reference's CSR order.
-__global__ void k_gnn_row_ids(const uint32_t *__restrict__ E, uint32_t M, const uint32_t *__restrict__ row_of,
-                              uint32_t *__restrict__ Er) {
-    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < M; j += gridDim.x * blockDim.x)
-        Er[j] = __ldg(row_of + ld_stream(E + j));
+// neighbour sum still runs in the reference's CSR order.  Entries [first, first + count); an id of N
+// or more (a malformed CSR, when this runs before the upload's own check) raises ERR_BOUND and
+// becomes row 0, so nothing is read out of bounds.
+__global__ void k_gnn_row_ids(const uint32_t *__restrict__ E, uint32_t first, uint32_t count, uint32_t N,
+                              const uint32_t *__restrict__ row_of, uint32_t *__restrict__ Er, DevState *st) {
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x) {
+        const uint32_t j = first + k, v = ld_stream(E + j);
+        if (v < N) {
+            Er[j] = __ldg(row_of + v);
+        } else {
+            Er[j] = 0u;
+            raise_error(st, ERR_BOUND, j);
+        }
+    }
 }
 
 // ---- shared pieces: four lanes per vertex, lane q owns features 4q..4q+3 ---------------------
@@ -1295,6 +1304,29 @@ gc_status launch_layer(gc_graph *g, const float *Wb, const float *Wh, const floa
 
 }  // namespace
 
+gc_status gc_gnn_rows_begin(gc_graph *g) {
+    gc_ctx *ctx = g->ctx;
+    gc_status s;
+    const size_t rows = (size_t)g->cap_N;
+    if ((s = gc_alloc(ctx, &g->row_of, rows, "feature rows")) != GC_OK) return s;
+    if ((s = gc_alloc(ctx, &g->Er, (size_t)g->cap_M, "neighbour rows")) != GC_OK) return s;
+    if ((s = gc_alloc(ctx, &g->vrow, rows, "row offsets")) != GC_OK) return s;
+    if (g->N == 0) return GC_OK;
+    k_gnn_rows<<<ctx->num_sms * 4, 256, 0, ctx->stream>>>(g->V, g->hubs, g->n_hubs, g->vorder, g->n_vorder, g->row_of,
+                                                           g->vrow);
+    ctx->launches++;
+    return gc_check_launch(ctx, "gnn feature rows");
+}
+
+gc_status gc_gnn_row_ids(gc_graph *g, uint32_t first, uint32_t count) {
+    gc_ctx *ctx = g->ctx;
+    if (!count) return GC_OK;
+    const uint32_t grid = std::min<uint32_t>((uint32_t)ctx->num_sms * 8, (count + 255) / 256);
+    k_gnn_row_ids<<<grid, 256, 0, ctx->stream>>>(g->E, first, count, g->N, g->row_of, g->Er, ctx->dstate);
+    ctx->launches++;
+    return gc_check_launch(ctx, "gnn neighbour rows");
+}
+
 gc_status gc_priority_gnn(gc_graph *g, const gc_model *m) {
     gc_ctx *ctx = g->ctx;
     gc_status s;
@@ -1330,18 +1362,9 @@ gc_status gc_priority_gnn(gc_graph *g, const gc_model *m) {
     }
     if ((s = gc_alloc(ctx, &g->gnn_ctr, 8, "gnn work counters")) != GC_OK) return s;
     if (!g->rows_ready) {  // once per upload: the feature-row order and the neighbour ids as rows
-        if ((s = gc_alloc(ctx, &g->row_of, rows, "feature rows")) != GC_OK) return s;
-        if ((s = gc_alloc(ctx, &g->Er, (size_t)g->cap_M, "neighbour rows")) != GC_OK) return s;
-        if ((s = gc_alloc(ctx, &g->vrow, rows, "row offsets")) != GC_OK) return s;
         ProfScope ps(ctx, "gnn_rows", ctx->stream);
-        k_gnn_rows<<<ctx->num_sms * 4, 256, 0, ctx->stream>>>(g->V, g->hubs, g->n_hubs, g->vorder, g->n_vorder,
-                                                               g->row_of, g->vrow);
-        ctx->launches++;
-        if (g->M) {
-            k_gnn_row_ids<<<ctx->num_sms * 8, 256, 0, ctx->stream>>>(g->E, g->M, g->row_of, g->Er);
-            ctx->launches++;
-        }
-        if ((s = gc_check_launch(ctx, "gnn feature rows")) != GC_OK) return s;
+        if ((s = gc_gnn_rows_begin(g)) != GC_OK) return s;
+        if ((s = gc_gnn_row_ids(g, 0, g->M)) != GC_OK) return s;
         g->rows_ready = true;
     }
     {

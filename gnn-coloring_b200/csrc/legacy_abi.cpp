@@ -81,7 +81,7 @@ void free_color_state(ColorState *cs) {
 }
 
 // Puts (N, V, E) into the state's device graph, growing it when needed.
-void load_graph(ColorState *cs, uint32_t N, const uint32_t *V, const uint32_t *E) {
+void load_graph(ColorState *cs, uint32_t N, const uint32_t *V, const uint32_t *E, bool gnn = false) {
     if (cs->bind && cs->bound_V == V && cs->bound_E == E && cs->bound_N == N) return;
     std::vector<uint32_t> zeros;
     if (!V) {  // orderings that ignore the graph may be called without one
@@ -96,6 +96,7 @@ void load_graph(ColorState *cs, uint32_t N, const uint32_t *V, const uint32_t *E
         cs->cap_M = M > cs->cap_M ? M : cs->cap_M;
         check(gc_graph_create(ctx(), cs->cap_N, cs->cap_M, &cs->g), "device allocation");
     }
+    gc_graph_gnn_hint(cs->g, gnn);  // GNN priorities follow: E becomes feature rows while it arrives
     check(gc_graph_reupload(ctx(), cs->g, N, V, E), "graph upload");
     if (cs->bind && V != zeros.data()) {
         cs->bound_V = V;
@@ -132,7 +133,7 @@ gc_model *load_model_or_die(int l) {
 
 void priority_into(ColorState *cs, uint32_t N, const uint32_t *V, const uint32_t *E, gc_heuristic h,
                    const gc_model *m, double *p) {
-    load_graph(cs, N, V, E);
+    load_graph(cs, N, V, E, h == GC_GNN);
     check(gc_priority(ctx(), cs->g, h, m), "priority");
     if (p) check(gc_download_priority(ctx(), cs->g, p), "priority download");
 }

@@ -14,6 +14,11 @@ extern "C" {
 gc_status gc_download_priority_begin(gc_ctx *ctx, gc_graph *g, double *p, int *pending);
 gc_status gc_download_priority_wait(gc_ctx *ctx);
 
+/* Announces that GNN priorities follow g's next upload.  With a page-locked E that upload then
+ * converts E to the GNN's feature rows piece by piece as it arrives, beside the copy, instead of in
+ * the first GNN call; the id check is part of that conversion. */
+void gc_graph_gnn_hint(gc_graph *g, int on);
+
 #ifdef __cplusplus
 }
 #endif

@@ -102,3 +102,43 @@ def test_legacy_internal_par_from_pinned_buffers(golden, tmp_path, monkeypatch):
             assert np.array_equal(tc.numpy(), golden.get(name, "GNN3", "color")), name
         lib.gnn_cleanup(ad)
         lib.jones_plassmann_cleanup(jp)
+
+
+def test_gnn_rows_built_while_pinned_e_arrives(gpu_ctx, golden):
+    """With GNN priorities announced (gc_graph_gnn_hint, what the reference-named GNN calls do), a
+    page-locked E goes up in pieces and each piece is turned into feature rows as it arrives; that
+    conversion also checks the ids.  An id outside the graph in the first, a middle or the last piece
+    is refused, the graph then takes a good upload, and GNN3 priorities, LF colors and Culberson
+    rounds equal those of a plain upload."""
+    lib = gcn.lib
+    lib.gc_graph_gnn_hint.argtypes = [C.c_void_p, C.c_int]
+    lib.gc_graph_gnn_hint.restype = None
+    model = gcn.Model(gpu_ctx, *golden.model(3))
+    for name in ("rmat11", "er1500"):
+        N, V, E = golden.graph(name)
+        M = len(E)
+        h = C.c_void_p()
+        gpu_ctx.check(lib.gc_graph_create(gpu_ctx.h, N, M, C.byref(h)), "create")
+        lib.gc_graph_gnn_hint(h, 1)
+        keep_v, pV = pinned_copy(V, np.uint32)
+        keep_e, pE = pinned_copy(E, np.uint32)
+        vp_, ep_ = pV.ctypes.data_as(C.POINTER(C.c_uint32)), pE.ctypes.data_as(C.POINTER(C.c_uint32))
+        for bad in (3, M // 2, M - 1):
+            pE[bad] = N + 7
+            assert lib.gc_graph_reupload(gpu_ctx.h, h, N, vp_, ep_) == 1, (name, bad)  # GC_ERR_INVALID
+            pE[bad] = E[bad]
+        assert lib.gc_graph_reupload(gpu_ctx.h, h, N, vp_, ep_) == 0, name
+        ref = gcn.Graph(gpu_ctx, N, V, E)
+        assert lib.gc_priority(gpu_ctx.h, h, gcn.GC_GNN, model.h) == 0
+        p = np.empty(N, np.float64)
+        assert lib.gc_download_priority(gpu_ctx.h, h, p.ctypes.data_as(C.POINTER(C.c_double))) == 0
+        assert np.array_equal(p, golden.get(name, "GNN3", "p")), name
+        # the rows built at upload do not disturb the other heuristics
+        assert lib.gc_priority(gpu_ctx.h, h, gcn.GC_LF, None) == 0
+        ref.priority("LF")
+        used = C.c_int()
+        assert lib.gc_color(gpu_ctx.h, h, 1, C.byref(used)) == 0
+        assert used.value == ref.color(recolor=1), name
+        ref.close()
+        lib.gc_graph_free(h)
+        del keep_v, keep_e
