@@ -349,10 +349,16 @@ def prep_time_ms(ctx, N, V, E, reps: int = 5):
 
 def rows_time_ms(ctx, model, N, V, E):
     """The GNN's feature-row order (k_gnn_rows, k_gnn_row_ids), built by the first GNN call after an
-    upload: timed with the library's event pairs on a second upload of the same graph, so that the
-    kernels' first-launch loading is not counted.  Once per upload; not part of `value`."""
+    upload: timed with the library's event pairs on a second graph, after one call has loaded the
+    kernels and allocated the buffers and a re-upload of the same CSR has dropped the order.  Once
+    per upload; not part of `value`."""
     import gnn_coloring as gcn
     g2 = gcn.Graph(ctx, N, V, E)
+    g2.priority("GNN", model)  # allocates the graph's GNN buffers
+    # the same CSR again: its preparation drops the row order, the buffers stay
+    Vc, Ec = np.ascontiguousarray(V, np.uint32), np.ascontiguousarray(E, np.uint32)
+    ctx.check(gcn.lib.gc_graph_reupload(ctx.h, g2.h, N, Vc.ctypes.data_as(C.POINTER(C.c_uint32)),
+                                        Ec.ctypes.data_as(C.POINTER(C.c_uint32))), "re-upload")
     gcn.lib.gc_prof_enable(ctx.h, 1)
     g2.priority("GNN", model)
     ms = prof_totals(gcn, ctx).get("gnn_rows", {}).get("ms_per_step")
@@ -719,7 +725,9 @@ def run_batched(args, device):
         ea, ez = int(V[a]), int(V[z])
         graphs.append(gcn.Graph(ctx, z - a, (V[a:z + 1] - V[a]).astype(np.uint32), E[ea:ez]))
     for name, h, m in heurs:
-        for gr in graphs[:16]:
+        # one untimed call per graph first: each graph's lazily allocated buffers (and, for the GNN,
+        # its feature-row order) exist before the timed pass, so that pass times launches and work
+        for gr in graphs:
             gr.priority(h, m)
             gr.color()
         ctx.sync()
