@@ -461,8 +461,9 @@ def run_ours(args):
     dominant = max(byte_bound, key=lambda k: kernels[k]["ms_per_step"]) if byte_bound else None
     other_bounds = {k: {"ms_per_step": v["ms_per_step"], "share": v["ms_per_step"] / ms_per_step,
                         "bound": "dependency chain (latency)" if k.startswith("jp_core") else
-                        "FP32 add arithmetic (exact sums); on a side stream beside the layer kernels, so its "
-                        "time overlaps theirs" if k.startswith("gnn_hub") else "launch/latency"}
+                        "FP32 add arithmetic (exact sums); the span from the layer's start on a high-priority "
+                        "side stream, whose CTAs take SMs as the layer kernel's leave them, so it overlaps the "
+                        "layer kernels' time" if k.startswith("gnn_hub") else "launch/latency"}
                     for k, v in kernels.items() if k not in byte_bound and v["ms_per_step"] > 0.05 * ms_per_step}
     roofline = None
     if dominant:
