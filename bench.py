@@ -224,7 +224,7 @@ def dist_setup(n_gpus: int, backend: str = "nccl"):
             torch.cuda.set_device(local)
             dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
         else:
-            dist.init_process_group(backend, timeout=timedelta(seconds=60))
+            dist.init_process_group(backend, timeout=timedelta(seconds=300))
     return world, rank, local
 
 
